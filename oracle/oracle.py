@@ -1,0 +1,322 @@
+"""ORACLE — test infrastructure only.
+
+ctypes bindings of ``oracle/_build/liboracle.so``, the CPU restatement of the
+reference's element routines (see ``oracle_core.hpp``). Only the tests, the
+smoke check and bench.py's CPU-baseline leg import this module; the product
+never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+NF = 39  # per-point state layout: ep 6, beta 6, alpha 4x6, eqps, thick, loading
+
+_lib = None
+
+
+def build() -> str:
+    """Compile the oracle (make in oracle/)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+_d = ctypes.POINTER(ctypes.c_double)
+_i = ctypes.POINTER(ctypes.c_int)
+_c = ctypes.POINTER(ctypes.c_char)
+_ll = ctypes.c_longlong
+
+
+def _declare(L):
+    L.orc_rule_size.argtypes = [ctypes.c_int] * 3
+    L.orc_rule.argtypes = [ctypes.c_int] * 3 + [_d]
+    L.orc_yield_matrix.argtypes = [_d, _d]
+    L.orc_return.argtypes = [_d, _d, _d, ctypes.c_int, _d, _d, _d, _d, _i]
+    L.orc_log_strain.argtypes = [_d, _d, _d, _d, _d, _d]
+    L.orc_elements.argtypes = ([_d] + [ctypes.c_int] * 4 + [_ll, _d, _d, _d, _d, ctypes.c_int, ctypes.c_int]
+                               + [_d, _d, _d, _d, _d, _i, _i, _i])
+    L.orc_count_flops.restype = _ll
+    L.orc_count_flops.argtypes = [_d] + [ctypes.c_int] * 4 + [_ll, _d, _d, _d, _d, ctypes.c_int]
+    L.orc_pattern_nnz.restype = _ll
+    L.orc_pattern_nnz.argtypes = [ctypes.c_int, ctypes.c_int, _i]
+    L.orc_build_pattern.argtypes = [ctypes.c_int, ctypes.c_int, _i, _i, _i, _i]
+    L.orc_scatter.argtypes = [ctypes.c_int, ctypes.c_int, _i, _i, _i, _d, _d, _ll]
+    L.orc_system_evaluate.argtypes = ([_d] + [ctypes.c_int] * 6 + [_d, _i, _d, _d, _d, ctypes.c_int, ctypes.c_int,
+                                      _i, _i, _ll, _d, _d, _d, _i, _d, _d, _d, _i])
+    L.orc_add_node_blocks.argtypes = [_i, _i, _d, ctypes.c_int, _i, _d]
+    L.orc_contact_create.restype = ctypes.c_void_p
+    L.orc_contact_create.argtypes = [ctypes.c_int, _d, ctypes.c_int, _d, _d, _d, ctypes.c_int]
+    L.orc_contact_destroy.argtypes = [ctypes.c_void_p]
+    L.orc_contact_begin.argtypes = [ctypes.c_void_p, _d, ctypes.c_double, ctypes.c_double, _c, ctypes.c_double, _i]
+    L.orc_contact_evaluate.argtypes = [ctypes.c_void_p, _d, ctypes.c_double, ctypes.c_int, _d, ctypes.c_int, _i,
+                                       _d, _d, _d]
+    L.orc_contact_anticipate.argtypes = [ctypes.c_void_p, _d, _d, ctypes.c_double, _d, ctypes.c_int, _i, _d]
+    L.orc_contact_commit.argtypes = [ctypes.c_void_p]
+    L.orc_contact_history.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _d]
+
+
+def _p(a, kind=_d):
+    if a is None:
+        return None
+    return a.ctypes.data_as(kind)
+
+
+def material_record(m: dict) -> np.ndarray:
+    """The oracle's flat material layout from a material dict (keys as in
+    the product's Material: youngs_modulus, poisson_ratio, yield_stress,
+    hardening_modulus, kinematic_hardening_modulus, saturation_stress,
+    saturation_rate, criterion ('von_mises'|'hill48'), backstresses
+    [(C, gamma)...], kinematic_integration ('exponential'|'backward_euler'),
+    r0, r45, r90, shear_l, shear_m, rolling_direction, sheet_normal)."""
+    r = np.zeros(32)
+    r[0] = m["youngs_modulus"]
+    r[1] = m["poisson_ratio"]
+    r[2] = m.get("yield_stress", 0.0)
+    r[3] = m.get("hardening_modulus", 0.0)
+    r[4] = m.get("kinematic_hardening_modulus", 0.0)
+    r[5] = m.get("saturation_stress", 0.0)
+    r[6] = m.get("saturation_rate", 0.0)
+    r[7] = 1.0 if m.get("criterion", "von_mises") == "hill48" else 0.0
+    back = m.get("backstresses", [])
+    r[8] = len(back)
+    r[9] = 1.0 if m.get("kinematic_integration", "exponential") == "backward_euler" else 0.0
+    for i, (c, g) in enumerate(back):
+        r[10 + i] = c
+        r[14 + i] = g
+    r[18] = m.get("r0", 1.0)
+    r[19] = m.get("r45", 1.0)
+    r[20] = m.get("r90", 1.0)
+    r[21] = m.get("shear_l", 1.5)
+    r[22] = m.get("shear_m", 1.5)
+    r[23:26] = m.get("rolling_direction", (1.0, 0.0, 0.0))
+    r[26:29] = m.get("sheet_normal", (0.0, 0.0, 1.0))
+    return r
+
+
+KIN = {"small": 0, "finite": 1, "logarithmic": 2}
+
+
+def rule(in_plane=2, thickness=0, axis=2) -> np.ndarray:
+    n = lib().orc_rule_size(in_plane, thickness, axis)
+    out = np.zeros((n, 4))
+    lib().orc_rule(in_plane, thickness, axis, _p(out))
+    return out
+
+
+def yield_matrix(m: dict) -> np.ndarray:
+    rec = material_record(m)
+    p = np.zeros(36)
+    if lib().orc_yield_matrix(_p(rec), _p(p)) != 0:
+        raise ValueError("invalid material")
+    return p.reshape(6, 6)
+
+
+def plastic_return(m: dict, strain, committed=None, want_tangent=True):
+    rec = material_record(m)
+    strain = np.ascontiguousarray(strain, dtype=np.float64)
+    committed = np.zeros(NF) if committed is None else np.ascontiguousarray(committed, dtype=np.float64)
+    stress, tangent, trial, energy = np.zeros(6), np.zeros(36), np.zeros(NF), np.zeros(1)
+    y = ctypes.c_int(0)
+    code = lib().orc_return(_p(rec), _p(strain), _p(committed), int(want_tangent), _p(stress), _p(tangent),
+                            _p(trial), _p(energy), ctypes.byref(y))
+    return dict(code=code, stress=stress, tangent=tangent.reshape(6, 6), state=trial, energy=energy[0],
+                yielding=bool(y.value))
+
+
+def log_strain(green, t=None):
+    green = np.ascontiguousarray(green, dtype=np.float64)
+    t = np.zeros(6) if t is None else np.ascontiguousarray(t, dtype=np.float64)
+    s, p, c, st = np.zeros(6), np.zeros(36), np.zeros(36), np.zeros(6)
+    code = lib().orc_log_strain(_p(green), _p(t), _p(s), _p(p), _p(c), _p(st))
+    return dict(code=code, strain=s, projection=p.reshape(6, 6), curvature=c.reshape(6, 6), stress=st)
+
+
+def elements(m: dict, X, ue, committed=None, alpha_n=None, kinematics="logarithmic", in_plane=2, thickness=0,
+             axis=2, want_tangent=True, threads=0):
+    """Evaluate a batch of independent IM Hex8 elements. X, ue: (ne, 24)
+    node-major; committed: (ne, nq, 39) or None (virgin); alpha_n: (ne, 9)."""
+    rec = material_record(m)
+    X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 24)
+    ne = X.shape[0]
+    ue = np.ascontiguousarray(ue, dtype=np.float64).reshape(ne, 24)
+    nq = lib().orc_rule_size(in_plane, thickness, axis)
+    committed = (np.zeros((ne, nq, NF)) if committed is None
+                 else np.ascontiguousarray(committed, dtype=np.float64).reshape(ne, nq, NF))
+    alpha_n = (np.zeros((ne, 9)) if alpha_n is None
+               else np.ascontiguousarray(alpha_n, dtype=np.float64).reshape(ne, 9))
+    f = np.zeros((ne, 24))
+    K = np.zeros((ne, 24, 24)) if want_tangent else None
+    energy = np.zeros(ne)
+    trial = np.zeros((ne, nq, NF))
+    alpha = np.zeros((ne, 9))
+    y = np.zeros(ne, dtype=np.int32)
+    it = np.zeros(ne, dtype=np.int32)
+    st = np.zeros(ne, dtype=np.int32)
+    lib().orc_elements(_p(rec), in_plane, thickness, axis, KIN[kinematics], ne, _p(X), _p(ue), _p(committed),
+                       _p(alpha_n), int(want_tangent), threads, _p(f), _p(K), _p(energy), _p(trial), _p(alpha),
+                       _p(y, _i), _p(it, _i), _p(st, _i))
+    return dict(force=f, tangent=K, energy=energy, states=trial, alpha=alpha, yielding=y, iterations=it, status=st)
+
+
+def count_flops(m: dict, X, ue, committed=None, alpha_n=None, kinematics="logarithmic", in_plane=2, thickness=0,
+                axis=2, want_tangent=True) -> int:
+    rec = material_record(m)
+    X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 24)
+    ne = X.shape[0]
+    ue = np.ascontiguousarray(ue, dtype=np.float64).reshape(ne, 24)
+    nq = lib().orc_rule_size(in_plane, thickness, axis)
+    committed = (np.zeros((ne, nq, NF)) if committed is None
+                 else np.ascontiguousarray(committed, dtype=np.float64).reshape(ne, nq, NF))
+    alpha_n = (np.zeros((ne, 9)) if alpha_n is None
+               else np.ascontiguousarray(alpha_n, dtype=np.float64).reshape(ne, 9))
+    return int(lib().orc_count_flops(_p(rec), in_plane, thickness, axis, KIN[kinematics], ne, _p(X), _p(ue),
+                                     _p(committed), _p(alpha_n), int(want_tangent)))
+
+
+def pattern(nn: int, conn) -> dict:
+    conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1, 8)
+    ne = conn.shape[0]
+    nnz = lib().orc_pattern_nnz(nn, ne, _p(conn, _i))
+    outer = np.zeros(3 * nn + 1, dtype=np.int32)
+    inner = np.zeros(nnz, dtype=np.int32)
+    bo = np.zeros(ne * 64, dtype=np.int32)
+    lib().orc_build_pattern(nn, ne, _p(conn, _i), _p(outer, _i), _p(inner, _i), _p(bo, _i))
+    return dict(outer=outer, inner=inner, block_offset=bo, nnz=nnz)
+
+
+def scatter(nn: int, conn, pat: dict, K) -> np.ndarray:
+    conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1, 8)
+    K = np.ascontiguousarray(K, dtype=np.float64)
+    values = np.zeros(pat["nnz"])
+    lib().orc_scatter(nn, conn.shape[0], _p(conn, _i), _p(pat["outer"], _i), _p(pat["block_offset"], _i), _p(K),
+                      _p(values), pat["nnz"])
+    return values
+
+
+def system_evaluate(m: dict, coords, conn, u, committed=None, alpha_n=None, kinematics="logarithmic", in_plane=2,
+                    thickness=0, axis=2, want_tangent=True, threads=0, pat=None):
+    rec = material_record(m)
+    coords = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+    conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1, 8)
+    nn, ne = coords.shape[0], conn.shape[0]
+    u = np.ascontiguousarray(u, dtype=np.float64).reshape(nn * 3)
+    nq = lib().orc_rule_size(in_plane, thickness, axis)
+    committed = (np.zeros((ne, nq, NF)) if committed is None
+                 else np.ascontiguousarray(committed, dtype=np.float64).reshape(ne, nq, NF))
+    alpha_n = (np.zeros((ne, 9)) if alpha_n is None
+               else np.ascontiguousarray(alpha_n, dtype=np.float64).reshape(ne, 9))
+    if pat is None:
+        pat = pattern(nn, conn)
+    internal = np.zeros(nn * 3)
+    gross, energy = np.zeros(1), np.zeros(1)
+    y = ctypes.c_int(0)
+    values = np.zeros(pat["nnz"])
+    trial = np.zeros((ne, nq, NF))
+    alpha = np.zeros((ne, 9))
+    failed = ctypes.c_int(-1)
+    code = lib().orc_system_evaluate(_p(rec), in_plane, thickness, axis, KIN[kinematics], nn, ne, _p(coords),
+                                     _p(conn, _i), _p(u), _p(committed), _p(alpha_n), int(want_tangent), threads,
+                                     _p(pat["outer"], _i), _p(pat["block_offset"], _i), pat["nnz"], _p(internal),
+                                     _p(gross), _p(energy), ctypes.byref(y), _p(values), _p(trial), _p(alpha),
+                                     ctypes.byref(failed))
+    return dict(code=code, failed_element=failed.value, internal=internal, gross=gross[0], energy=energy[0],
+                yielding_points=y.value, values=values, states=trial, alpha=alpha, pattern=pat)
+
+
+def add_node_blocks(pat: dict, values, nodes, blocks) -> np.ndarray:
+    values = np.array(values, dtype=np.float64, copy=True)
+    nodes = np.ascontiguousarray(nodes, dtype=np.int32)
+    blocks = np.ascontiguousarray(blocks, dtype=np.float64).reshape(-1, 9)
+    rc = lib().orc_add_node_blocks(_p(pat["outer"], _i), _p(pat["inner"], _i), _p(values), len(nodes),
+                                   _p(nodes, _i), _p(blocks))
+    if rc:
+        raise ValueError("a node block lies outside the pattern")
+    return values
+
+
+class Contact:
+    """ToolContact restated: tools = list of dicts with shape ('sphere',
+    'plane', 'cylinder'), radius, friction, tangential_ratio, normal, axis,
+    times, points, nodes, area, kappa."""
+
+    SHAPES = {"sphere": 0, "plane": 1, "cylinder": 2}
+
+    def __init__(self, coords, tools, friction_tangent="exact"):
+        self.coords = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+        self.nn = self.coords.shape[0]
+        self.ntools = len(tools)
+        rec, knots, slaves = [], [], []
+        for t in tools:
+            rec += [self.SHAPES[t["shape"]], t.get("radius", 0.0), t.get("friction", 0.0),
+                    t.get("tangential_ratio", 1.0), *t.get("normal", (0, 0, 1)), *t.get("axis", (0, 0, 1)),
+                    len(t["times"]), len(t["nodes"])]
+            for tt, p in zip(t["times"], t["points"]):
+                knots += [tt, *p]
+            for n, a, k in zip(t["nodes"], t["area"], t["kappa"]):
+                slaves += [n, a, k]
+        self._rec = np.array(rec, dtype=np.float64)
+        self._knots = np.array(knots, dtype=np.float64)
+        self._slaves = np.array(slaves, dtype=np.float64)
+        self.max_blocks = sum(len(t["nodes"]) for t in tools)
+        self.h = lib().orc_contact_create(self.nn, _p(self.coords), self.ntools, _p(self._rec), _p(self._knots),
+                                          _p(self._slaves), 1 if friction_tangent == "symmetric" else 0)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_contact_destroy(self.h)
+            self.h = None
+
+    def begin_increment(self, u0, t0, t1, active, margin):
+        u0 = np.ascontiguousarray(u0, dtype=np.float64)
+        act = (ctypes.c_char * self.ntools)(*[bytes([1 if a else 0]) for a in active])
+        counts = np.zeros(self.ntools, dtype=np.int32)
+        lib().orc_contact_begin(self.h, _p(u0), t0, t1, act, margin, _p(counts, _i))
+        return counts
+
+    def evaluate(self, u, t, want_tangent=True):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        residual = np.zeros(self.nn * 3)
+        nodes = np.zeros(max(self.max_blocks, 1), dtype=np.int32)
+        blocks = np.zeros((max(self.max_blocks, 1), 9))
+        res = np.zeros((self.ntools, 9))
+        sc = np.zeros(4)
+        nb = lib().orc_contact_evaluate(self.h, _p(u), t, int(want_tangent), _p(residual), self.max_blocks,
+                                        _p(nodes, _i), _p(blocks), _p(res), _p(sc))
+        if nb < 0:
+            return dict(code=-1)
+        return dict(code=0, residual=residual, nodes=nodes[:nb].copy(), blocks=blocks[:nb].reshape(-1, 3, 3).copy(),
+                    tools=res, gross=sc[0], round_off=sc[1], force_norm=sc[2], symmetric=bool(sc[3]))
+
+    def anticipate(self, u, du, t, residual):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        du = np.ascontiguousarray(du, dtype=np.float64)
+        residual = np.array(residual, dtype=np.float64, copy=True)
+        nodes = np.zeros(max(self.max_blocks, 1), dtype=np.int32)
+        blocks = np.zeros((max(self.max_blocks, 1), 9))
+        n = lib().orc_contact_anticipate(self.h, _p(u), _p(du), t, _p(residual), self.max_blocks, _p(nodes, _i),
+                                         _p(blocks))
+        return residual, nodes[:n].copy(), blocks[:n].reshape(-1, 3, 3).copy()
+
+    def commit(self):
+        lib().orc_contact_commit(self.h)
+
+    def history(self, k):
+        cap = self.max_blocks + 1
+        out = np.zeros((cap, 7))
+        n = lib().orc_contact_history(self.h, k, cap, _p(out))
+        return out[:n].copy()

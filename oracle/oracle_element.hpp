@@ -1,0 +1,644 @@
+// ORACLE — test infrastructure only (see oracle_core.hpp).
+//
+// The incompatible-mode Hex8 element of the reference, restated:
+// Gauss-Legendre rules (src/elements/Quadrature.cpp:16-219), Hex8 shape
+// gradients (src/elements/Hex8.cpp:52-64), the Taylor-corrected mode
+// gradients (src/elements/Hex8Incompatible.cpp:73-83), and the local Newton
+// iteration with its condensation (src/fem/IncompatibleModes.cpp:134-600,
+// constants src/fem/IncompatibleModes.hpp:98-127).
+#pragma once
+
+#include "oracle_core.hpp"
+
+#include <vector>
+
+namespace orc {
+
+struct QPoint {
+  double xi, eta, zeta, weight;
+};
+
+/// The 1-D Gauss-Legendre rule of n <= 7 points (Quadrature.cpp:16-163).
+inline std::vector<std::pair<double, double>> line_rule(int n) {
+  std::vector<std::pair<double, double>> r;
+  if (n == 1) { r = {{0.0, 2.0}}; return r; }
+  if (n == 2) { const double a = 1.0 / std::sqrt(3.0); r = {{-a, 1.0}, {a, 1.0}}; return r; }
+  if (n == 3) {
+    const double a = std::sqrt(3.0 / 5.0);
+    r = {{-a, 5.0 / 9.0}, {0.0, 8.0 / 9.0}, {a, 5.0 / 9.0}};
+    return r;
+  }
+  if (n == 4) {
+    const double s6 = std::sqrt(6.0 / 5.0);
+    const double x1 = std::sqrt((3.0 - 2.0 * s6) / 7.0);
+    const double x2 = std::sqrt((3.0 + 2.0 * s6) / 7.0);
+    const double s = std::sqrt(30.0);
+    const double w1 = (18.0 + s) / 36.0, w2 = (18.0 - s) / 36.0;
+    r = {{-x2, w2}, {-x1, w1}, {x1, w1}, {x2, w2}};
+    return r;
+  }
+  // Newton on P_n from Tricomi's guesses (Quadrature.cpp:100-139).
+  r.assign(static_cast<std::size_t>(n), {0.0, 0.0});
+  const double pi = std::acos(-1.0);
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    double x = std::cos(pi * (i + 0.75) / (n + 0.5));
+    double derivative = 0.0;
+    for (int it = 0; it < 100; ++it) {
+      double p0 = 1.0, p1 = x;
+      for (int k = 2; k <= n; ++k) {
+        const double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+        p0 = p1;
+        p1 = p2;
+      }
+      derivative = n * (x * p1 - p0) / (x * x - 1.0);
+      const double step = p1 / derivative;
+      x -= step;
+      if (std::fabs(step) <= 1.0e-16) break;
+    }
+    if (2 * i + 1 == n) x = 0.0;
+    double p0 = 1.0, p1 = x;
+    for (int k = 2; k <= n; ++k) {
+      const double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+      p0 = p1;
+      p1 = p2;
+    }
+    derivative = n * (x * p1 - p0) / (x * x - 1.0);
+    const double weight = 2.0 / ((1.0 - x * x) * derivative * derivative);
+    r[static_cast<std::size_t>(i)] = {-x, weight};
+    r[static_cast<std::size_t>(n - 1 - i)] = {x, weight};
+  }
+  return r;
+}
+
+/// The Hex8 stiffness rule (Hex8Kernels.hpp:125-130, Quadrature.cpp:72-93,
+/// 165-219): the cube rule, or the box rule with thickness points; xi
+/// fastest, weights multiplied x * y * z.
+inline std::vector<QPoint> hex8_rule(int in_plane, int thickness, int axis) {
+  if (thickness <= 0 || thickness == in_plane) thickness = in_plane, axis = 2;
+  const auto plane = line_rule(in_plane);
+  const auto through = line_rule(thickness);
+  const auto& rx = axis == 0 ? through : plane;
+  const auto& ry = axis == 1 ? through : plane;
+  const auto& rz = axis == 2 ? through : plane;
+  std::vector<QPoint> out;
+  for (const auto& gk : rz)
+    for (const auto& gj : ry)
+      for (const auto& gi : rx) out.push_back({gi.first, gj.first, gk.first, gi.second * gj.second * gk.second});
+  return out;
+}
+
+constexpr double kCorner[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                  {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+
+/// dN/dxi, 8 x 3 (Hex8.cpp:52-64).
+inline Mat<double, 8, 3> shape_gradients(double xi, double eta, double zeta) {
+  Mat<double, 8, 3> g;
+  for (int a = 0; a < 8; ++a) {
+    const double fx = 1.0 + xi * kCorner[a][0];
+    const double fy = 1.0 + eta * kCorner[a][1];
+    const double fz = 1.0 + zeta * kCorner[a][2];
+    g(a, 0) = 0.125 * kCorner[a][0] * fy * fz;
+    g(a, 1) = 0.125 * kCorner[a][1] * fx * fz;
+    g(a, 2) = 0.125 * kCorner[a][2] * fx * fy;
+  }
+  return g;
+}
+
+enum Kinematics { kSmall = 0, kFinite = 1, kLogarithmic = 2 };
+
+constexpr int kMaxLocal = 25;
+constexpr double kFullStepReduction = 1.0 - 1.0e-4;
+constexpr int kMaxLineSearch = 8;
+constexpr double kLineSearchRatio = 0.5;
+constexpr double kLocalShift = 1.0e-3;
+constexpr double kLocalMarquardt = 1.0e-6;
+constexpr double kLocalTolerance = 1.0e-8;
+constexpr double kLocalRoundOff = 1.0e-13;
+
+template <class T>
+struct PointWork {
+  Mat<T, 3, 11> g;  // [G | G~]
+  Mat<T, 3, 3> hu;
+  T weight = T(0.0);
+  Mat<T, 3, 3> h;
+  Mat<T, 6, 33> mb;
+  Vec<T, 6> strain;
+  LogStrain<T> log;
+  Vec<T, 6> s;
+  Mat<T, 6, 6> material;
+  T energy = T(0.0);
+  State<T> state;
+  bool yielding = false;
+};
+
+template <class T>
+struct Sums {
+  Vec<T, 33> r;
+  Vec<T, 9> scale, floor;
+  Mat<T, 9, 9> kaa;
+  Mat<T, 24, 9> kua;
+  Mat<T, 9, 24> kau;
+  Mat<T, 24, 24> kuu;
+  T energy = T(0.0);
+};
+
+template <class T>
+Mat<T, 3, 3> tensor3(const Vec<T, 6>& v) {
+  Mat<T, 3, 3> t;
+  t(0, 0) = v[0]; t(0, 1) = v[3]; t(0, 2) = v[5];
+  t(1, 0) = v[3]; t(1, 1) = v[1]; t(1, 2) = v[4];
+  t(2, 0) = v[5]; t(2, 1) = v[4]; t(2, 2) = v[2];
+  return t;
+}
+
+template <class T>
+Vec<T, 6> green_lagrange_6(const Mat<T, 3, 3>& h) {
+  Mat<T, 3, 3> e;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      T s = T(0.0);
+      for (int k = 0; k < 3; ++k) s += h(k, i) * h(k, j);
+      e(i, j) = T(0.5) * (h(i, j) + h(j, i) + s);
+    }
+  Vec<T, 6> v;
+  v[0] = e(0, 0); v[1] = e(1, 1); v[2] = e(2, 2);
+  v[3] = T(2.0) * e(0, 1); v[4] = T(2.0) * e(1, 2); v[5] = T(2.0) * e(2, 0);
+  return v;
+}
+
+template <class T>
+void green_lagrange_operator_11(const Mat<T, 3, 3>& f, const Mat<T, 3, 11>& g, Mat<T, 6, 33>& b) {
+  static constexpr int kPair[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {1, 2}, {2, 0}};
+  for (int c = 0; c < 6; ++c) {
+    const int i = kPair[c][0], j = kPair[c][1];
+    for (int a = 0; a < 11; ++a)
+      for (int k = 0; k < 3; ++k)
+        b(c, 3 * a + k) = i == j ? f(k, i) * g(i, a) : f(k, i) * g(j, a) + f(k, j) * g(i, a);
+  }
+}
+
+/// One element's result (ElastoplasticElement, Elastoplastic.hpp:171-186).
+template <class T>
+struct ElementOut {
+  Vec<T, 24> force;
+  Mat<T, 24, 24> tangent;
+  T energy = T(0.0);
+  Vec<T, 9> alpha;
+  int iterations = 0;
+  int yielding = 0;
+  std::vector<State<T>> states;
+  bool symmetric = true;
+};
+
+template <class T>
+class IMElement {
+ public:
+  IMElement(const Material& mat, const std::vector<QPoint>& rule, int kinematics)
+      : mat_(mat), rule_(rule), kin_(kinematics) {}
+
+  /// incompatible_elastoplastic_element (IncompatibleModes.cpp:577-600).
+  /// Throws Failure.
+  ElementOut<T> evaluate(const double* x /*3x8 node-major: x[3a+i]*/, const T* ue,
+                         const std::vector<State<T>>& committed, const T* alpha_n,
+                         bool want_tangent) {
+    set_up(x, ue);
+    ElementOut<T> out;
+    solve_and_condense(committed, alpha_n, want_tangent, out);
+    out.symmetric = symmetric_;
+    out.states.reserve(points_.size());
+    for (const PointWork<T>& p : points_) {
+      out.states.push_back(p.state);
+      if (p.yielding) ++out.yielding;
+    }
+    return out;
+  }
+
+ private:
+  void set_up(const double* x, const T* ue) {
+    symmetric_ = mat_.symmetric();
+    for (int a = 0; a < 8; ++a)
+      for (int k = 0; k < 3; ++k) u_(k, a) = ue[3 * a + k];
+    for (int i = 0; i < 24; ++i) ue_[i] = ue[i];
+    Mat<T, 3, 8> x0;
+    for (int a = 0; a < 8; ++a)
+      for (int k = 0; k < 3; ++k) x0(k, a) = T(x[3 * a + k]);
+    auto jacobian_at = [&](const Mat<double, 8, 3>& dn) {
+      Mat<T, 3, 3> j;
+      for (int i = 0; i < 3; ++i)
+        for (int c = 0; c < 3; ++c) {
+          T s = T(0.0);
+          for (int a = 0; a < 8; ++a) s += x0(i, a) * T(dn(a, c));
+          j(i, c) = s;
+        }
+      return j;
+    };
+    const Mat<T, 3, 3> jac0 = jacobian_at(shape_gradients(0.0, 0.0, 0.0));
+    const T det0 = det3(jac0);
+    if (!(det0 > T(0.0))) throw Failure{kMeshInverted};
+    const Mat<T, 3, 3> jinv0 = inv3(jac0);
+    points_.assign(rule_.size(), PointWork<T>());
+    for (std::size_t q = 0; q < rule_.size(); ++q) {
+      const QPoint& xi = rule_[q];
+      PointWork<T>& p = points_[q];
+      const Mat<double, 8, 3> dn = shape_gradients(xi.xi, xi.eta, xi.zeta);
+      const Mat<T, 3, 3> jac = jacobian_at(dn);
+      const T det = det3(jac);
+      if (!(det > T(0.0))) throw Failure{kMeshInverted};
+      const Mat<T, 3, 3> jinv = inv3(jac);
+      for (int a = 0; a < 8; ++a)
+        for (int i = 0; i < 3; ++i) {
+          T s = T(0.0);
+          for (int c = 0; c < 3; ++c) s += T(dn(a, c)) * jinv(c, i);
+          p.g(i, a) = s;
+        }
+      // hex8_incompatible_gradients: column k = (det0/det)(-2 xi_k) row k of J0^-1.
+      const T ratio = det0 / det;
+      const double nat[3] = {xi.xi, xi.eta, xi.zeta};
+      for (int k = 0; k < 3; ++k) {
+        const T f = ratio * T(-2.0 * nat[k]);
+        for (int i = 0; i < 3; ++i) p.g(i, 8 + k) = f * jinv0(k, i);
+      }
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          T s = T(0.0);
+          for (int a = 0; a < 8; ++a) s += u_(i, a) * p.g(j, a);
+          p.hu(i, j) = s;
+        }
+      p.weight = T(xi.weight) * det;
+      if (kin_ == kSmall) {
+        Mat<T, 3, 3> id;
+        for (int i = 0; i < 3; ++i) id(i, i) = T(1.0);
+        green_lagrange_operator_11(id, p.g, p.mb);
+      }
+    }
+  }
+
+  void kinematics_at(const Vec<T, 9>& alpha) {
+    Mat<T, 3, 3> a;
+    for (int m = 0; m < 3; ++m)
+      for (int k = 0; k < 3; ++k) a(k, m) = alpha[3 * m + k];
+    for (PointWork<T>& p : points_) {
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          T s = T(0.0);
+          for (int m = 0; m < 3; ++m) s += a(i, m) * p.g(j, 8 + m);
+          p.h(i, j) = p.hu(i, j) + s;
+        }
+      if (kin_ == kSmall) {
+        for (int c = 0; c < 6; ++c) {
+          T s = T(0.0);
+          for (int j = 0; j < 24; ++j) s += p.mb(c, j) * ue_[j];
+          T t = T(0.0);
+          for (int j = 0; j < 9; ++j) t += p.mb(c, 24 + j) * alpha[j];
+          p.strain[c] = s + t;
+        }
+      } else {
+        Mat<T, 3, 3> f = p.h;
+        for (int i = 0; i < 3; ++i) f(i, i) += T(1.0);
+        if (kin_ == kLogarithmic && !(det3(f) > T(0.0))) throw Failure{kInverted};
+        green_lagrange_operator_11(f, p.g, p.mb);
+        if (kin_ == kFinite) {
+          p.strain = green_lagrange_6(p.h);
+        } else {
+          p.log = logarithmic_strain(green_lagrange_6(p.h));
+          p.strain = p.log.strain;
+        }
+      }
+    }
+  }
+
+  void respond(const std::vector<State<T>>& committed) {
+    for (std::size_t q = 0; q < points_.size(); ++q) {
+      PointWork<T>& p = points_[q];
+      const Response<T> r = plastic_return(mat_, p.strain, committed[q], true);
+      p.energy = r.energy;
+      p.state = r.state;
+      p.yielding = r.yielding;
+      if (kin_ == kLogarithmic) {
+        p.s = logarithmic_stress(p.log, r.stress);
+        const Mat<T, 6, 6> pcp = mul(mul(tr(p.log.projection), r.tangent), p.log.projection);
+        const Mat<T, 6, 6> curv = logarithmic_curvature(p.log, r.stress);
+        for (int i = 0; i < 36; ++i) p.material[i] = pcp[i] + curv[i];
+      } else {
+        p.s = r.stress;
+        p.material = r.tangent;
+      }
+    }
+  }
+
+  void accumulate_local(Sums<T>& sums) {
+    const bool geometric = kin_ != kSmall;
+    for (const PointWork<T>& p : points_) {
+      const T w = p.weight;
+      for (int j = 0; j < 33; ++j) {
+        T s = T(0.0);
+        for (int c = 0; c < 6; ++c) s += p.mb(c, j) * p.s[c];
+        sums.r[j] += w * s;
+      }
+      for (int j = 0; j < 9; ++j) {
+        T s = T(0.0);
+        for (int c = 0; c < 6; ++c) s += abs(p.mb(c, 24 + j)) * abs(p.s[c]);
+        sums.scale[j] += w * s;
+      }
+      const T h = maxabs(p.h);
+      const T f = w * maxabs(p.material) * h * (T(1.0) + h);
+      for (int j = 0; j < 9; ++j) {
+        T s = T(0.0);
+        for (int c = 0; c < 6; ++c) s += abs(p.mb(c, 24 + j));
+        sums.floor[j] += f * s;
+      }
+      sums.energy += w * p.energy;
+      Mat<T, 6, 9> mba;
+      for (int c = 0; c < 6; ++c)
+        for (int j = 0; j < 9; ++j) {
+          T s = T(0.0);
+          for (int d = 0; d < 6; ++d) s += p.material(c, d) * p.mb(d, 24 + j);
+          mba(c, j) = s;
+        }
+      for (int i = 0; i < 9; ++i)
+        for (int j = 0; j < 9; ++j) {
+          T s = T(0.0);
+          for (int c = 0; c < 6; ++c) s += p.mb(c, 24 + i) * mba(c, j);
+          sums.kaa(i, j) += w * s;
+        }
+      if (geometric) {
+        const Mat<T, 3, 3> st = tensor3(p.s);
+        for (int a = 0; a < 3; ++a)
+          for (int b = 0; b < 3; ++b) {
+            T s = T(0.0);
+            for (int i = 0; i < 3; ++i)
+              for (int j = 0; j < 3; ++j) s += p.g(i, 8 + a) * st(i, j) * p.g(j, 8 + b);
+            for (int k = 0; k < 3; ++k) sums.kaa(3 * a + k, 3 * b + k) += w * s;
+          }
+      }
+    }
+  }
+
+  void accumulate_coupling(bool full, Sums<T>& sums) {
+    const bool geometric = kin_ != kSmall;
+    for (const PointWork<T>& p : points_) {
+      const T w = p.weight;
+      // material * mb (6 x 33)
+      Mat<T, 6, 33> mb2;
+      for (int c = 0; c < 6; ++c)
+        for (int j = 0; j < 33; ++j) {
+          T s = T(0.0);
+          for (int d = 0; d < 6; ++d) s += p.material(c, d) * p.mb(d, j);
+          mb2(c, j) = s;
+        }
+      for (int i = 0; i < 24; ++i)
+        for (int j = 0; j < 9; ++j) {
+          T s = T(0.0);
+          for (int c = 0; c < 6; ++c) s += p.mb(c, i) * mb2(c, 24 + j);
+          sums.kua(i, j) += w * s;
+        }
+      if (!symmetric_) {
+        for (int i = 0; i < 9; ++i)
+          for (int j = 0; j < 24; ++j) {
+            T s = T(0.0);
+            for (int c = 0; c < 6; ++c) s += p.mb(c, 24 + i) * mb2(c, j);
+            sums.kau(i, j) += w * s;
+          }
+      }
+      if (full) {
+        for (int i = 0; i < 24; ++i)
+          for (int j = 0; j < 24; ++j) {
+            T s = T(0.0);
+            for (int c = 0; c < 6; ++c) s += p.mb(c, i) * mb2(c, j);
+            sums.kuu(i, j) += w * s;
+          }
+      }
+      if (geometric) {
+        const Mat<T, 3, 3> st = tensor3(p.s);
+        for (int a = 0; a < 8; ++a)
+          for (int b = 0; b < 11; ++b) {
+            T s = T(0.0);
+            for (int i = 0; i < 3; ++i)
+              for (int j = 0; j < 3; ++j) s += p.g(i, a) * st(i, j) * p.g(j, b);
+            const T v = w * s;
+            for (int k = 0; k < 3; ++k) {
+              if (b < 8) {
+                if (full) sums.kuu(3 * a + k, 3 * b + k) += v;
+              } else {
+                sums.kua(3 * a + k, 3 * (b - 8) + k) += v;
+                if (!symmetric_) sums.kau(3 * (b - 8) + k, 3 * a + k) += v;
+              }
+            }
+          }
+      }
+    }
+  }
+
+  static Vec<T, 9> tail9(const Vec<T, 33>& r) {
+    Vec<T, 9> t;
+    for (int i = 0; i < 9; ++i) t[i] = r[24 + i];
+    return t;
+  }
+
+  void solve_and_condense(const std::vector<State<T>>& committed, const T* start,
+                          bool want_tangent, ElementOut<T>& out) {
+    Vec<T, 9> alpha;
+    if (start != nullptr)
+      for (int i = 0; i < 9; ++i) alpha[i] = start[i];
+    Sums<T> sums;
+    FullPivLU<T, 9> lu;
+    auto pass = [&](const Vec<T, 9>& at) {
+      kinematics_at(at);
+      respond(committed);
+      sums = Sums<T>();
+      accumulate_local(sums);
+    };
+    auto try_pass = [&](const Vec<T, 9>& at) {
+      try {
+        pass(at);
+        return true;
+      } catch (const Failure&) {
+        return false;
+      }
+    };
+    auto axpy = [](const Vec<T, 9>& a, T s, const Vec<T, 9>& d) {
+      Vec<T, 9> o;
+      for (int i = 0; i < 9; ++i) o[i] = a[i] + s * d[i];
+      return o;
+    };
+    pass(alpha);
+    T residual = norm(tail9(sums.r));
+    auto search_norm = [&](const Vec<T, 9>& d, T reach) {
+      T best_step = T(0.0);
+      T best = residual;
+      bool last_is_best = false;
+      T trial_step = reach;
+      for (int search = 0; search < kMaxLineSearch; ++search, trial_step = trial_step * T(0.5)) {
+        if (!try_pass(axpy(alpha, trial_step, d))) { last_is_best = false; continue; }
+        const T n = norm(tail9(sums.r));
+        last_is_best = n < best;
+        if (last_is_best) { best = n; best_step = trial_step; }
+        if (n <= T(kFullStepReduction) * residual) break;
+      }
+      if (best_step == T(0.0)) return false;
+      if (!last_is_best) pass(axpy(alpha, best_step, d));
+      alpha = axpy(alpha, best_step, d);
+      residual = best;
+      return true;
+    };
+    auto line_search = [&](const Vec<T, 9>& d, const Vec<T, 9>& r0) {
+      const T phi0 = dot(d, r0);
+      T reach = T(1.0);
+      bool evaluated = try_pass(axpy(alpha, T(1.0), d));
+      for (int halving = 0; !evaluated && halving < kMaxLineSearch; ++halving) {
+        reach = reach * T(0.5);
+        evaluated = try_pass(axpy(alpha, reach, d));
+      }
+      if (!evaluated) return false;
+      const T full = norm(tail9(sums.r));
+      if (full <= T(kFullStepReduction) * residual ||
+          maxabs(tail9(sums.r)) <= T(kLocalTolerance) * maxabs(sums.scale) + T(kLocalRoundOff) * maxabs(sums.floor)) {
+        alpha = axpy(alpha, reach, d);
+        residual = full;
+        return true;
+      }
+      const T phi1 = dot(d, tail9(sums.r));
+      if (!(phi0 < T(0.0)) || !(phi1 > T(0.0)) || !isfinite(phi1)) return search_norm(d, T(0.5) * reach);
+      T s0 = T(0.0), f0 = phi0, s1 = reach, f1 = phi1, step = reach;
+      int side = 0;
+      for (int search = 0; search < kMaxLineSearch; ++search) {
+        const T width = s1 - s0;
+        step = tclamp((s0 * f1 - s1 * f0) / (f1 - f0), s0 + T(0.1) * width, s1 - T(0.1) * width);
+        evaluated = try_pass(axpy(alpha, step, d));
+        const T f = evaluated ? dot(d, tail9(sums.r)) : T(std::numeric_limits<double>::infinity());
+        if (evaluated && abs(f) <= T(kLineSearchRatio) * abs(phi0)) break;
+        if (!evaluated || f > T(0.0)) {
+          s1 = step;
+          f1 = evaluated ? f : T(0.5) * f1;
+          if (side == 1) f0 = f0 * T(0.5);
+          side = 1;
+        } else {
+          s0 = step;
+          f0 = f;
+          if (side == -1) f1 = f1 * T(0.5);
+          side = -1;
+        }
+      }
+      if (!evaluated) {
+        if (s0 == T(0.0)) return false;
+        step = s0;
+        pass(axpy(alpha, step, d));
+      }
+      alpha = axpy(alpha, step, d);
+      residual = norm(tail9(sums.r));
+      return true;
+    };
+    for (;;) {
+      const Vec<T, 9> ra = tail9(sums.r);
+      const T largest = maxabs(ra);
+      const T scale = maxabs(sums.scale);
+      const T floor = T(kLocalRoundOff) * maxabs(sums.floor);
+      lu.compute(sums.kaa);
+      if (!lu.invertible()) throw Failure{kLocalSingular};
+      if (largest <= T(kLocalTolerance) * scale + floor || largest == T(0.0)) break;
+      if (out.iterations == kMaxLocal || !isfinite(largest)) throw Failure{kLocalNoConverge};
+      ++out.iterations;
+      const Vec<T, 9> r0 = ra;
+      const Mat<T, 9, 9> k0 = sums.kaa;
+      Vec<T, 9> newton = lu.solve(r0);
+      for (int i = 0; i < 9; ++i) newton[i] = -newton[i];
+      Mat<T, 9, 9> sym;
+      for (int i = 0; i < 9; ++i)
+        for (int j = 0; j < 9; ++j) sym(i, j) = T(0.5) * (k0(i, j) + k0(j, i));
+      Mat<T, 9, 9> chol = sym;
+      if (llt<T, 9>(chol)) {
+        if (line_search(newton, r0)) continue;
+      } else {
+        if (try_pass(axpy(alpha, T(1.0), newton))) {
+          const T full = norm(tail9(sums.r));
+          if (full <= T(kFullStepReduction) * residual) {
+            alpha = axpy(alpha, T(1.0), newton);
+            residual = full;
+            continue;
+          }
+        }
+        Vec<T, 9> ev;
+        Mat<T, 9, 9> evec;
+        sym_eigen<T, 9>(sym, ev, evec);
+        const T top = maxabs(ev);
+        const T mu = T(kLocalShift) * top - ev[0];
+        Mat<T, 9, 9> shifted_m = k0;
+        for (int i = 0; i < 9; ++i) shifted_m(i, i) += mu;
+        int perm[9];
+        lu_partial(shifted_m, perm);
+        Vec<T, 9> shifted = lu_partial_solve(shifted_m, perm, r0);
+        for (int i = 0; i < 9; ++i) shifted[i] = -shifted[i];
+        if (line_search(shifted, r0) || search_norm(newton, T(0.5))) continue;
+      }
+      // Levenberg-Marquardt fallback (IncompatibleModes.cpp:522-545).
+      const Mat<T, 9, 9> normal = mul(tr(k0), k0);
+      Vec<T, 9> gradient;
+      for (int i = 0; i < 9; ++i) {
+        T s = T(0.0);
+        for (int j = 0; j < 9; ++j) s += k0(j, i) * r0[j];
+        gradient[i] = s;
+      }
+      T dmax = normal(0, 0);
+      for (int i = 1; i < 9; ++i) dmax = tmax(dmax, normal(i, i));
+      T mu = T(kLocalMarquardt) * dmax;
+      bool moved = false;
+      for (int search = 0; search < kMaxLineSearch && !moved; ++search, mu = mu * T(10.0)) {
+        Mat<T, 9, 9> a = normal;
+        for (int i = 0; i < 9; ++i) a(i, i) += mu;
+        if (!llt<T, 9>(a)) continue;  // (normal + mu I) is positive definite for mu > 0
+        Vec<T, 9> d = llt_solve(a, gradient);
+        for (int i = 0; i < 9; ++i) d[i] = -d[i];
+        if (!try_pass(axpy(alpha, T(1.0), d))) continue;
+        const T n = norm(tail9(sums.r));
+        if (n < residual) {
+          alpha = axpy(alpha, T(1.0), d);
+          residual = n;
+          moved = true;
+        }
+      }
+      if (!moved) throw Failure{kLocalNoDescent};
+    }
+    accumulate_coupling(want_tangent, sums);
+    const Vec<T, 9> correction = lu.solve(tail9(sums.r));
+    for (int i = 0; i < 24; ++i) {
+      T s = T(0.0);
+      for (int j = 0; j < 9; ++j) s += sums.kua(i, j) * correction[j];
+      out.force[i] = sums.r[i] - s;
+    }
+    out.energy = sums.energy;
+    if (want_tangent) {
+      Mat<T, 9, 24> coupling;
+      for (int col = 0; col < 24; ++col) {
+        Vec<T, 9> b;
+        for (int i = 0; i < 9; ++i) b[i] = symmetric_ ? sums.kua(col, i) : sums.kau(i, col);
+        const Vec<T, 9> x = lu.solve(b);
+        for (int i = 0; i < 9; ++i) coupling(i, col) = x[i];
+      }
+      Mat<T, 24, 24> k;
+      for (int i = 0; i < 24; ++i)
+        for (int j = 0; j < 24; ++j) {
+          T s = T(0.0);
+          for (int m = 0; m < 9; ++m) s += sums.kua(i, m) * coupling(m, j);
+          k(i, j) = sums.kuu(i, j) - s;
+        }
+      if (symmetric_) {
+        Mat<T, 24, 24> ks;
+        for (int i = 0; i < 24; ++i)
+          for (int j = 0; j < 24; ++j) ks(i, j) = T(0.5) * (k(i, j) + k(j, i));
+        k = ks;
+      }
+      out.tangent = k;
+    }
+    out.alpha = alpha;
+  }
+
+  const Material& mat_;
+  const std::vector<QPoint>& rule_;
+  int kin_;
+  bool symmetric_ = true;
+  Mat<T, 3, 8> u_;
+  Vec<T, 24> ue_;
+  std::vector<PointWork<T>> points_;
+};
+
+}  // namespace orc
