@@ -1,0 +1,273 @@
+/*
+ * sbk.h - C ABI of the B200 element loop of sparlab_form.
+ *
+ * The reference has no FFI for this path: its seam is the library-internal
+ * class detail::NonlinearSystem (src/fem/NonlinearSystem.hpp:85-334), whose
+ * evaluate/commit the forming driver calls every Newton iteration
+ * (src/fem/Forming.cpp:692,766-783,1202), plus ToolContact
+ * (include/sparlab/fem/RigidTool.hpp:248-320) for the penalty contact and
+ * Assembler's node-block pattern (src/fem/Assembler.cpp:86-215). Every
+ * entry point below replaces one member of those, with plain pointers and
+ * sizes: no exceptions cross it (an int status is returned), buffers named
+ * "_dev" are device pointers, everything else is host memory.
+ *
+ * Units and conventions are the reference's: SI, node-major DOFs (dof =
+ * 3 node + k), Voigt order {11, 22, 33, 12, 23, 31} with engineering shear
+ * strains and tensorial stresses, Hex8 nodes in VTK order.
+ */
+#ifndef SBK_H_
+#define SBK_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference's exceptions) ------------------------ */
+enum sbk_status {
+  SBK_OK = 0,
+  SBK_ERR_ARGUMENT = 1,    /* a null pointer, a bad size or option        */
+  SBK_ERR_CONFIG = 2,      /* ConfigError: invalid material or rule       */
+  SBK_ERR_MESH = 3,        /* MeshError: an element inverted at rest      */
+  SBK_ERR_SOLVER = 4,      /* SolverError: see the failing element's code */
+  SBK_ERR_CUDA = 5,        /* a CUDA call failed                          */
+  SBK_ERR_UNSUPPORTED = 6, /* a rule or a size this build does not take   */
+  SBK_ERR_NO_EXTENSION = 7 /* no device: the library never falls back     */
+};
+
+/* ---- per-element codes (why an element's SolverError was thrown) ------- */
+enum sbk_element_code {
+  SBK_EL_OK = 0,
+  SBK_EL_INVERTED_POINT = 1,     /* det F <= 0 (IncompatibleModes.cpp:214)         */
+  SBK_EL_RETURN_NO_CONVERGE = 2, /* Plasticity.cpp:134-139, 356-359, 423-430       */
+  SBK_EL_LOCAL_NO_CONVERGE = 3,  /* 25 local iterations (IncompatibleModes.cpp:470) */
+  SBK_EL_LOCAL_SINGULAR = 4,     /* K_aa singular (IncompatibleModes.cpp:462)      */
+  SBK_EL_LOCAL_NO_DESCENT = 5,   /* IncompatibleModes.cpp:537-545                  */
+  SBK_EL_MESH_INVERTED = 6,      /* det J <= 0 (IncompatibleModes.cpp:159,176)     */
+  SBK_EL_NONFINITE = 7,          /* LogarithmicStrain.cpp:110-112                  */
+  SBK_EL_DEGENERATE = 8          /* LogarithmicStrain.cpp:120-125                  */
+};
+
+enum sbk_kinematics { SBK_SMALL_STRAIN = 0, SBK_FINITE = 1, SBK_FINITE_LOGARITHMIC = 2 };
+enum sbk_criterion { SBK_VON_MISES = 0, SBK_HILL48 = 1 };
+enum sbk_integration { SBK_EXPONENTIAL = 0, SBK_BACKWARD_EULER = 1 };
+
+#define SBK_MAX_BACKSTRESSES 4
+#define SBK_MAX_POINTS 32
+
+/* The material block (include/sparlab/material/Material.hpp:103-257): E, nu,
+ * sigma_y(a) = sy0 + H a + Q (1 - exp(-delta a)), Prager's H_kin, Hill48 from
+ * r-values in the frame (rolling direction, sheet normal), Chaboche
+ * backstresses (C_i, gamma_i). */
+typedef struct sbk_material {
+  double youngs_modulus, poisson_ratio;
+  double yield_stress, hardening_modulus, kinematic_hardening_modulus;
+  double saturation_stress, saturation_rate;
+  int criterion;       /* sbk_criterion */
+  int num_backstresses;
+  int kinematic_integration; /* sbk_integration */
+  int reserved;
+  double backstress_modulus[SBK_MAX_BACKSTRESSES];
+  double backstress_recovery[SBK_MAX_BACKSTRESSES];
+  double r0, r45, r90, shear_l, shear_m;
+  double rolling_direction[3], sheet_normal[3];
+} sbk_material;
+
+/* The stiffness rule (include/sparlab/elements/Element.hpp:56-71):
+ * stiffness_points per direction (1..4), thickness_points (0: the cube
+ * rule; else 1..7 along thickness_axis 0/1/2). This build takes rules of at
+ * most SBK_MAX_POINTS points. */
+typedef struct sbk_rule {
+  int stiffness_points, thickness_points, thickness_axis, reserved;
+} sbk_rule;
+
+/* Number of points of a rule (0 for an invalid one). */
+int sbk_rule_size(const sbk_rule* rule);
+
+/* Doubles per integration point in the device state layout of a material:
+ * plastic strain (6), whole back stress (6), one 6-vector per kinematic term
+ * of the general return, accumulated plastic strain, loading flag (0/1). The
+ * layout is field-major: field f of point q of element e at
+ * state[f * (ne * nq) + e * nq + q]. PlasticState
+ * (include/sparlab/material/Plasticity.hpp:185-201) minus its plane-stress
+ * thickness strain. */
+int sbk_state_fields(const sbk_material* material);
+
+/* The yield matrix P (6x6, row-major, tensorial Voigt, global axes) the
+ * material's criterion gives (Material.cpp:135-217); SBK_ERR_CONFIG for an
+ * invalid material (Material::set_plasticity's checks). */
+int sbk_yield_matrix(const sbk_material* material, double* p_out);
+
+/* ---- one batch of independent elements ---------------------------------
+ * incompatible_elastoplastic_element (src/fem/IncompatibleModes.cpp:577-600)
+ * for ne elements at once, every pointer on the device:
+ *   x_dev      ne x 24   reference coordinates, node-major (x0 y0 z0 x1 ...)
+ *   u_dev      ne x 24   displacements, same order
+ *   state_dev  committed points, field-major (sbk_state_fields)
+ *   alpha_dev  ne x 9    committed mode parameters (NULL: zero)
+ * outputs:
+ *   force_dev  ne x 24   condensed force f*
+ *   tangent_dev ne x 576 condensed tangent K* in node blocks: entry
+ *              (3a+i, 3b+j) at e*576 + (8a+b)*9 + 3i + j; NULL: no tangent
+ *   energy_dev ne, trial_dev (state layout), alpha_out_dev ne x 9,
+ *   yield_dev  ne x nq (1 where the point's return was plastic),
+ *   iterations_dev ne, code_dev ne (sbk_element_code).
+ * stream: a cudaStream_t (NULL: the default stream). Returns SBK_OK or a
+ * launch error; element failures are reported per element in code_dev. */
+int sbk_element_batch(const sbk_material* material, const sbk_rule* rule, int kinematics, int64_t ne,
+                      const double* x_dev, const double* u_dev, const double* state_dev,
+                      const double* alpha_dev, double* force_dev, double* tangent_dev,
+                      double* energy_dev, double* trial_dev, double* alpha_out_dev,
+                      uint8_t* yield_dev, int32_t* iterations_dev, int32_t* code_dev, void* stream);
+
+/* ---- the system: detail::NonlinearSystem ------------------------------- */
+typedef struct sbk_system sbk_system;
+
+typedef struct sbk_mesh {
+  int32_t num_nodes, num_elements;
+  const double* coords;        /* host, 3 per node                         */
+  const int32_t* connectivity; /* host, 8 per element, VTK order           */
+} sbk_mesh;
+
+/* NonlinearSystem(model, assembler, options) (NonlinearSystem.hpp:95-101):
+ * uploads the mesh, builds the node-block pattern (Assembler::build_pattern,
+ * Assembler.cpp:86-173) and its gather maps, and starts every point virgin
+ * and every element's modes at zero (initialise_history, :273-311). */
+int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const sbk_rule* rule,
+                      int kinematics, sbk_system** out);
+int sbk_system_destroy(sbk_system* sys);
+/* All later launches go to this stream (a cudaStream_t; NULL: default). */
+int sbk_system_set_stream(sbk_system* sys, void* stream);
+
+/* Launch shape of the element kernel: elements per thread block (0: the
+ * default; the autotuner sets it). */
+int sbk_system_set_elements_per_block(sbk_system* sys, int elements_per_block);
+
+/* Sizes and the pattern (device pointers owned by the system). The values
+ * array is the reference's column-major (CSC) layout; the pattern is
+ * structurally symmetric, so the same arrays read as CSR hold K^T. */
+typedef struct sbk_pattern {
+  int64_t num_dofs, nnz;
+  const int32_t* outer_dev; /* num_dofs + 1 */
+  const int32_t* inner_dev; /* nnz          */
+} sbk_pattern;
+int sbk_system_pattern(const sbk_system* sys, sbk_pattern* out);
+
+/* Evaluation (NonlinearSystem.hpp:27-47); device arrays owned by the system,
+ * valid until the next evaluate. */
+typedef struct sbk_evaluation {
+  const double* internal_dev; /* f_int, num_dofs                          */
+  const double* residual_dev; /* f_int - lambda f_dead = f_int (dead = 0) */
+  const double* values_dev;   /* tangent CSC values, nnz (want_tangent)   */
+  double energy;
+  double gross;               /* |sum_e |f_e| per DOF|_2                   */
+  int32_t yielding_points;
+  int32_t failed_element;     /* -1, or the lowest failing element        */
+  int32_t failure_code;       /* sbk_element_code of that element         */
+  int32_t reserved;
+} sbk_evaluation;
+
+/* NonlinearSystem::evaluate(u, lambda, want_tangent)
+ * (NonlinearSystem.hpp:192-268). u_dev: num_dofs doubles on the device.
+ * Returns SBK_ERR_SOLVER (and fills failed_element, failure_code) where the
+ * reference throws SolverError. */
+int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int want_tangent,
+                        sbk_evaluation* out);
+
+/* NonlinearSystem::commit (NonlinearSystem.hpp:119-129): the trial points
+ * and modes of the last successful evaluate become the committed ones. */
+int sbk_system_commit(sbk_system* sys);
+
+/* committed_all / set_committed (NonlinearSystem.hpp:161-182) and
+ * internal_all / set_internal (:137-158) for restart and output: host
+ * buffers, state in the field-major device layout, alpha ne x 9. */
+int sbk_system_get_committed(const sbk_system* sys, double* state, double* alpha);
+int sbk_system_set_committed(sbk_system* sys, const double* state, const double* alpha);
+/* The trial state of the last evaluate (Evaluation::states / modes), and
+ * its per-point yield flags (ne x nq). */
+int sbk_system_get_trial(const sbk_system* sys, double* state, double* alpha, uint8_t* yield);
+/* Device pointers of the committed and trial buffers (owned by the system). */
+int sbk_system_buffers(const sbk_system* sys, const double** committed_state_dev,
+                       const double** committed_alpha_dev, const double** trial_state_dev,
+                       const double** trial_alpha_dev);
+/* symmetric() and plastic() (NonlinearSystem.hpp:103-105). */
+int sbk_system_symmetric(const sbk_system* sys);
+int sbk_system_plastic(const sbk_system* sys);
+
+/* add_node_block (src/fem/Forming.cpp:280-297) for n blocks (node, 3x3
+ * row-major), all device pointers, added in list order into the tangent of
+ * the last evaluate. */
+int sbk_system_add_node_blocks(sbk_system* sys, int32_t n, const int32_t* nodes_dev,
+                               const double* blocks_dev);
+
+/* ---- contact: ToolContact ---------------------------------------------- */
+typedef struct sbk_contact sbk_contact;
+
+/* One rigid tool (include/sparlab/fem/RigidTool.hpp:155-189) with its
+ * piecewise-linear trajectory and its slave nodes (ascending), their
+ * tributary areas and penalty stiffnesses kappa (ToolContact's constructor,
+ * RigidTool.cpp:275-333, computes those once from the face geometry). */
+typedef struct sbk_tool {
+  int32_t shape; /* 0 sphere, 1 plane, 2 cylinder */
+  int32_t num_knots;
+  int32_t num_slaves;
+  int32_t reserved;
+  double radius, friction, tangential_ratio;
+  double normal[3], axis[3];
+  const double* times;     /* host, num_knots           */
+  const double* points;    /* host, 3 per knot          */
+  const int32_t* nodes;    /* host, num_slaves          */
+  const double* area;      /* host                      */
+  const double* kappa;     /* host                      */
+} sbk_tool;
+
+int sbk_contact_create(const sbk_mesh* mesh, int32_t num_tools, const sbk_tool* tools,
+                       int friction_tangent /* 0 exact, 1 symmetric */, sbk_contact** out);
+int sbk_contact_destroy(sbk_contact* c);
+int sbk_contact_set_stream(sbk_contact* c, void* stream);
+
+/* ToolContact::begin_increment (RigidTool.cpp:345-393); u0_dev on the
+ * device, active one flag per tool (host). */
+int sbk_contact_begin(sbk_contact* c, const double* u0_dev, double t0, double t1,
+                      const uint8_t* active, double margin);
+
+typedef struct sbk_contact_result {
+  const double* residual_dev;  /* num_dofs: minus the contact forces          */
+  const int32_t* block_nodes_dev; /* num_blocks, in tool then slave order     */
+  const double* blocks_dev;    /* 9 per block, row-major, d(residual)/du      */
+  int32_t num_blocks;
+  int32_t symmetric;
+  double gross, round_off, force_norm;
+  int32_t failed;              /* 1: a node within half a radius (SolverError) */
+  int32_t reserved;
+} sbk_contact_result;
+
+/* Per-tool resultants after evaluate: 9 doubles per tool, centre xyz,
+ * force xyz, active nodes, slipping nodes, max penetration. */
+int sbk_contact_resultants(const sbk_contact* c, double* out);
+
+/* ToolContact::evaluate (RigidTool.cpp:398-555). */
+int sbk_contact_evaluate(sbk_contact* c, const double* u_dev, double t, int want_tangent,
+                         sbk_contact_result* out);
+/* ToolContact::anticipate (RigidTool.cpp:557-603): adds to residual_dev and
+ * appends to the block list of the last evaluate; returns the count added
+ * in *added. */
+int sbk_contact_anticipate(sbk_contact* c, const double* u_dev, const double* du_dev, double t,
+                           double* residual_dev, int32_t* added, sbk_contact_result* out);
+/* ToolContact::commit (RigidTool.cpp:605-611). */
+int sbk_contact_commit(sbk_contact* c);
+/* The committed history of tool k (host): count, then per slave node in
+ * contact (node, force xyz, relative xyz). */
+int sbk_contact_history(const sbk_contact* c, int32_t k, int32_t max_entries, double* out,
+                        int32_t* count);
+
+/* Last error message of this thread (never NULL). */
+const char* sbk_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SBK_H_ */

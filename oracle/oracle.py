@@ -49,7 +49,7 @@ def _declare(L):
     L.orc_return.argtypes = [_d, _d, _d, ctypes.c_int, _d, _d, _d, _d, _i]
     L.orc_log_strain.argtypes = [_d, _d, _d, _d, _d, _d]
     L.orc_elements.argtypes = ([_d] + [ctypes.c_int] * 4 + [_ll, _d, _d, _d, _d, ctypes.c_int, ctypes.c_int]
-                               + [_d, _d, _d, _d, _d, _i, _i, _i])
+                               + [_d, _d, _d, _d, _d, _i, _i, _i, ctypes.c_void_p])
     L.orc_count_flops.restype = _ll
     L.orc_count_flops.argtypes = [_d] + [ctypes.c_int] * 4 + [_ll, _d, _d, _d, _d, ctypes.c_int]
     L.orc_pattern_nnz.restype = _ll
@@ -111,6 +111,10 @@ def material_record(m: dict) -> np.ndarray:
 KIN = {"small": 0, "finite": 1, "logarithmic": 2}
 
 
+def rule_size(in_plane=2, thickness=0, axis=2) -> int:
+    return int(lib().orc_rule_size(in_plane, thickness, axis))
+
+
 def rule(in_plane=2, thickness=0, axis=2) -> np.ndarray:
     n = lib().orc_rule_size(in_plane, thickness, axis)
     out = np.zeros((n, 4))
@@ -167,10 +171,12 @@ def elements(m: dict, X, ue, committed=None, alpha_n=None, kinematics="logarithm
     y = np.zeros(ne, dtype=np.int32)
     it = np.zeros(ne, dtype=np.int32)
     st = np.zeros(ne, dtype=np.int32)
+    yf = np.zeros((ne, nq), dtype=np.int8)
     lib().orc_elements(_p(rec), in_plane, thickness, axis, KIN[kinematics], ne, _p(X), _p(ue), _p(committed),
                        _p(alpha_n), int(want_tangent), threads, _p(f), _p(K), _p(energy), _p(trial), _p(alpha),
-                       _p(y, _i), _p(it, _i), _p(st, _i))
-    return dict(force=f, tangent=K, energy=energy, states=trial, alpha=alpha, yielding=y, iterations=it, status=st)
+                       _p(y, _i), _p(it, _i), _p(st, _i), yf.ctypes.data_as(ctypes.c_void_p))
+    return dict(force=f, tangent=K, energy=energy, states=trial, alpha=alpha, yielding=y, iterations=it, status=st,
+                yield_flags=yf.astype(bool))
 
 
 def count_flops(m: dict, X, ue, committed=None, alpha_n=None, kinematics="logarithmic", in_plane=2, thickness=0,

@@ -187,6 +187,7 @@ struct ElementOut {
   int iterations = 0;
   int yielding = 0;
   std::vector<State<T>> states;
+  std::vector<char> point_yield;
   bool symmetric = true;
 };
 
@@ -208,6 +209,7 @@ class IMElement {
     out.states.reserve(points_.size());
     for (const PointWork<T>& p : points_) {
       out.states.push_back(p.state);
+      out.point_yield.push_back(p.yielding ? 1 : 0);
       if (p.yielding) ++out.yielding;
     }
     return out;

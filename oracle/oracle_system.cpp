@@ -101,6 +101,7 @@ struct ElementBatch {
   int* yielding;
   int* iterations;
   int* status;
+  signed char* yield_flags;  // nq per element, or null
 };
 
 template <class T>
@@ -123,6 +124,8 @@ void run_element(const ElementBatch& b, long long e) {
     if (b.alpha)
       for (int i = 0; i < 9; ++i) b.alpha[e * 9 + i] = val(out.alpha[i]);
     if (b.yielding) b.yielding[e] = out.yielding;
+    if (b.yield_flags)
+      for (int q = 0; q < nq; ++q) b.yield_flags[e * nq + q] = out.point_yield[q] ? 1 : 0;
     if (b.iterations) b.iterations[e] = out.iterations;
     b.status[e] = 0;
   } catch (const Failure& fail) {
@@ -280,12 +283,12 @@ int orc_elements(const double* material, int in_plane, int thickness, int axis, 
                  long long ne, const double* X, const double* ue, const double* committed,
                  const double* alpha_n, int want_tangent, int threads, double* f, double* K,
                  double* energy, double* trial, double* alpha, int* yielding, int* iterations,
-                 int* status) {
+                 int* status, signed char* yield_flags) {
   Material mat;
   if (!make_material(material, mat)) return -1;
   const std::vector<QPoint> rule = hex8_rule(in_plane, thickness, axis);
   ElementBatch b{&mat, &rule, kinematics, X, ue, committed, alpha_n, want_tangent, f, K, energy,
-                 trial, alpha, yielding, iterations, status};
+                 trial, alpha, yielding, iterations, status, yield_flags};
   const int nt = set_threads(threads);
   long long failed = 0;
 #pragma omp parallel for schedule(static) num_threads(nt) reduction(+ : failed)
@@ -312,7 +315,7 @@ long long orc_count_flops(const double* material, int in_plane, int thickness, i
     // Shift the inputs so that element e sits at index 0 of the batch.
     ElementBatch b{&mat, &rule, kinematics, X + e * 24, ue + e * 24, committed + e * nq * kNF,
                    alpha_n ? alpha_n + e * 9 : nullptr, want_tangent, f.data(), K.data(),
-                   energy.data(), trial.data(), alpha.data(), &y, &it, &st};
+                   energy.data(), trial.data(), alpha.data(), &y, &it, &st, nullptr};
     run_element<CD>(b, 0);
   }
   return g_flops;
@@ -384,7 +387,7 @@ int orc_system_evaluate(const double* material, int in_plane, int thickness, int
   (void)nq;
   orc_elements(material, in_plane, thickness, axis, kinematics, ne, X.data(), ue.data(), committed,
                alpha_n, want_tangent, threads, f.data(), want_tangent ? K.data() : nullptr, en.data(),
-               trial, alpha_out, y.data(), it.data(), st.data());
+               trial, alpha_out, y.data(), it.data(), st.data(), nullptr);
   for (int e = 0; e < ne; ++e)
     if (st[e] != 0) {
       *failed_element = e;

@@ -1,0 +1,178 @@
+// K2: assembly of the element forces and tangents into the node-block
+// pattern, by gather.
+//
+// The reference scatters every element's 24 x 24 tangent into the CSC value
+// array in element order (src/fem/Assembler.cpp:184-215) and gathers f_int,
+// the gross sums, the energy and the yield count serially
+// (src/fem/NonlinearSystem.hpp:240-266). Here every value entry (and every
+// DOF of f_int) is owned by one thread, which sums its contributions in
+// ascending element order from 0.0 - the reference's own order, so the
+// assembled values equal its bit for bit given the same element matrices,
+// with no atomics and the same result on every run. Scalar norms and sums
+// use a fixed two-stage tree.
+#include <cuda_runtime.h>
+
+#include "sbk_element.h"
+
+namespace sbk {
+namespace {
+
+constexpr int kReduceBlocks = 296;  // 2 x 148 SMs; fixed for a fixed tree
+constexpr int kReduceThreads = 256;
+
+// One thread per node block (A, B): 9 values from the element blocks that
+// couple A and B, in ascending element order.
+__global__ void __launch_bounds__(256) assemble_values_kernel(int64_t num_blocks, const int32_t* __restrict__ block_col,
+                                                              const int64_t* __restrict__ block_value,
+                                                              const int32_t* __restrict__ block_ptr,
+                                                              const int32_t* __restrict__ block_src,
+                                                              const int32_t* __restrict__ outer,
+                                                              const double* __restrict__ tangent,
+                                                              double* __restrict__ values) {
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < num_blocks;
+       b += (int64_t)gridDim.x * blockDim.x) {
+    double acc[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) acc[i] = 0.0;
+    const int32_t end = block_ptr[b + 1];
+    for (int32_t k = block_ptr[b]; k < end; ++k) {
+      const double* src = tangent + (int64_t)block_src[k] * 9;
+#pragma unroll
+      for (int i = 0; i < 9; ++i) acc[i] += src[i];
+    }
+    const int32_t B = block_col[b];
+    const int64_t stride = (int64_t)outer[3 * B + 1] - outer[3 * B];
+    const int64_t base = block_value[b];
+    // acc[3 ka + kb] is entry (3A + ka, 3B + kb): column 3B + kb, row offset ka.
+#pragma unroll
+    for (int kb = 0; kb < 3; ++kb)
+#pragma unroll
+      for (int ka = 0; ka < 3; ++ka) values[base + kb * stride + ka] = acc[3 * ka + kb];
+  }
+}
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  const double out = sh[0];
+  __syncthreads();
+  return out;
+}
+
+// f_int and |f| per DOF by node (ascending element order), and per-block
+// partials of gross^2, the energy and the yield count.
+__global__ void __launch_bounds__(kReduceThreads) assemble_forces_kernel(
+    int64_t nn, int64_t ne, int nq, const int32_t* __restrict__ node_ptr, const int32_t* __restrict__ node_src,
+    const double* __restrict__ force, const double* __restrict__ energy_e, const uint8_t* __restrict__ yield,
+    double* __restrict__ internal, double* __restrict__ partial) {
+  __shared__ double sh[kReduceThreads];
+  double g2 = 0.0, en = 0.0, yc = 0.0;
+  for (int64_t n = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
+    double f[3] = {0, 0, 0}, g[3] = {0, 0, 0};
+    const int32_t end = node_ptr[n + 1];
+    for (int32_t k = node_ptr[n]; k < end; ++k) {
+      const int32_t src = node_src[k];  // e * 8 + a
+      const double* fe = force + (int64_t)(src >> 3) * 24 + 3 * (src & 7);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        f[c] += fe[c];
+        g[c] += fabs(fe[c]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      internal[3 * n + c] = f[c];
+      g2 += g[c] * g[c];
+    }
+  }
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x) {
+    en += energy_e[e];
+    int y = 0;
+    for (int q = 0; q < nq; ++q) y += yield[e * nq + q];
+    yc += (double)y;
+  }
+  g2 = block_sum(g2, sh);
+  en = block_sum(en, sh);
+  yc = block_sum(yc, sh);
+  if (threadIdx.x == 0) {
+    partial[3 * blockIdx.x + 0] = en;
+    partial[3 * blockIdx.x + 1] = g2;
+    partial[3 * blockIdx.x + 2] = yc;
+  }
+}
+
+__global__ void __launch_bounds__(kReduceThreads) finish_kernel(int nblocks, const double* __restrict__ partial,
+                                                                double* __restrict__ scalars) {
+  __shared__ double sh[kReduceThreads];
+  double v[3] = {0, 0, 0};
+  for (int i = threadIdx.x; i < nblocks; i += blockDim.x)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) v[c] += partial[3 * i + c];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const double s = block_sum(v[c], sh);
+    if (threadIdx.x == 0) scalars[c] = s;
+  }
+}
+
+__global__ void add_node_blocks_kernel(const int32_t* __restrict__ outer, const int32_t* __restrict__ inner,
+                                       double* __restrict__ values, int32_t n, const int32_t* __restrict__ nodes,
+                                       const double* __restrict__ blocks, int32_t* missing) {
+  const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t node = nodes[i];
+  for (int b = 0; b < 3; ++b) {
+    const int32_t col = 3 * node + b;
+    int32_t lo = outer[col], hi = outer[col + 1];
+    for (int a = 0; a < 3; ++a) {
+      const int32_t row = 3 * node + a;
+      // lower_bound over the sorted rows of the column.
+      int32_t l = lo, h = hi;
+      while (l < h) {
+        const int32_t mid = l + (h - l) / 2;
+        if (inner[mid] < row) l = mid + 1; else h = mid;
+      }
+      if (l < hi && inner[l] == row) {
+        values[l] += blocks[9 * i + 3 * a + b];
+      } else {
+        atomicExch(missing, 1);
+      }
+    }
+  }
+}
+
+}  // namespace
+
+int launch_assemble_values(const GatherMaps& m, const double* tangent, double* values, cudaStream_t stream) {
+  if (m.num_blocks == 0) return 0;
+  const int threads = 256;
+  int64_t blocks = (m.num_blocks + threads - 1) / threads;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  assemble_values_kernel<<<(unsigned)blocks, threads, 0, stream>>>(m.num_blocks, m.block_col, m.block_value,
+                                                                     m.block_ptr, m.block_src, m.outer, tangent,
+                                                                     values);
+  return (int)cudaGetLastError();
+}
+
+int launch_assemble_forces(const GatherMaps& m, const double* force, const double* energy_e, const uint8_t* yield,
+                           int nq, double* internal, double* scratch, double* scalars, cudaStream_t stream) {
+  assemble_forces_kernel<<<kReduceBlocks, kReduceThreads, 0, stream>>>(
+      m.num_nodes, m.num_elements, nq, m.node_ptr, m.node_src, force, energy_e, yield, internal, scratch);
+  finish_kernel<<<1, kReduceThreads, 0, stream>>>(kReduceBlocks, scratch, scalars);
+  return (int)cudaGetLastError();
+}
+
+int launch_add_node_blocks(const int32_t* outer, const int32_t* inner, double* values, int32_t n,
+                           const int32_t* nodes, const double* blocks, int32_t* missing, cudaStream_t stream) {
+  if (n <= 0) return 0;
+  add_node_blocks_kernel<<<(n + 127) / 128, 128, 0, stream>>>(outer, inner, values, n, nodes, blocks, missing);
+  return (int)cudaGetLastError();
+}
+
+size_t assemble_scratch_doubles() { return 3 * kReduceBlocks; }
+
+}  // namespace sbk

@@ -1,0 +1,746 @@
+// The C ABI (include/sbk.h): materials and rules, the element batch, and the
+// system that stands in for detail::NonlinearSystem
+// (src/fem/NonlinearSystem.hpp:85-334) with its Assembler pattern
+// (src/fem/Assembler.cpp:86-173). Every device buffer belongs to a handle;
+// no exception crosses the ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "sbk.h"
+#include "sbk_element.h"
+#include "sbk_params.h"
+
+using sbk::Params;
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& what) {
+  g_error = what;
+  return code;
+}
+
+#define SBK_CUDA(call)                                                                     \
+  do {                                                                                     \
+    cudaError_t e_ = (call);                                                               \
+    if (e_ != cudaSuccess) return fail(SBK_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+int check_device() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(SBK_ERR_NO_EXTENSION, "no CUDA device: the element loop runs on the GPU only");
+  }
+  return SBK_OK;
+}
+
+bool finite_positive(double v) { return std::isfinite(v) && v > 0.0; }
+
+// Material::set_plasticity and derive_hill (src/material/Material.cpp:135-271).
+int yield_matrix(const sbk_material& m, double* P) {
+  std::memset(P, 0, 36 * sizeof(double));
+  if (m.criterion != SBK_HILL48) {
+    for (int i = 0; i < 3; ++i) {
+      for (int j = 0; j < 3; ++j) P[i * 6 + j] = -0.5;
+      P[i * 6 + i] = 1.0;
+      P[(3 + i) * 6 + 3 + i] = 3.0;
+    }
+    return SBK_OK;
+  }
+  if (!finite_positive(m.r0) || !finite_positive(m.r45) || !finite_positive(m.r90))
+    return fail(SBK_ERR_CONFIG, "the Hill48 r-values must be finite and positive");
+  const double G = 1.0 / (1.0 + m.r0);
+  const double H = m.r0 / (1.0 + m.r0);
+  const double F = m.r0 / (m.r90 * (1.0 + m.r0));
+  const double N = (m.r0 + m.r90) * (1.0 + 2.0 * m.r45) / (2.0 * m.r90 * (1.0 + m.r0));
+  const double L = m.shear_l, M = m.shear_m;
+  if (!(L > 0.0 && M > 0.0 && N > 0.0) || !(F + H > 0.0) || !(F * G + G * H + H * F > 0.0))
+    return fail(SBK_ERR_CONFIG, "the Hill48 coefficients do not make a convex yield surface");
+  double nd[3], rd[3];
+  const double nn = std::sqrt(m.sheet_normal[0] * m.sheet_normal[0] + m.sheet_normal[1] * m.sheet_normal[1] +
+                              m.sheet_normal[2] * m.sheet_normal[2]);
+  const double rn0 = std::sqrt(m.rolling_direction[0] * m.rolling_direction[0] +
+                               m.rolling_direction[1] * m.rolling_direction[1] +
+                               m.rolling_direction[2] * m.rolling_direction[2]);
+  if (!(nn > 0.0) || !(rn0 > 0.0) || !std::isfinite(nn) || !std::isfinite(rn0))
+    return fail(SBK_ERR_CONFIG, "the rolling direction and the sheet normal must be finite non-zero vectors");
+  for (int i = 0; i < 3; ++i) {
+    nd[i] = m.sheet_normal[i] / nn;
+    rd[i] = m.rolling_direction[i] / rn0;
+  }
+  const double d = rd[0] * nd[0] + rd[1] * nd[1] + rd[2] * nd[2];
+  for (int i = 0; i < 3; ++i) rd[i] -= d * nd[i];
+  const double rn = std::sqrt(rd[0] * rd[0] + rd[1] * rd[1] + rd[2] * rd[2]);
+  if (!(rn > 1.0e-6)) return fail(SBK_ERR_CONFIG, "the rolling direction is parallel to the sheet normal");
+  for (int i = 0; i < 3; ++i) rd[i] /= rn;
+  const double td[3] = {nd[1] * rd[2] - nd[2] * rd[1], nd[2] * rd[0] - nd[0] * rd[2], nd[0] * rd[1] - nd[1] * rd[0]};
+  const double* axes[3] = {rd, td, nd};
+  // Material-frame matrix, then P = T^T Pm T with T the Voigt stress
+  // rotation into the material axes (rows of `axes`).
+  double pm[6][6] = {};
+  pm[0][0] = G + H;
+  pm[1][1] = F + H;
+  pm[2][2] = F + G;
+  pm[0][1] = pm[1][0] = -H;
+  pm[1][2] = pm[2][1] = -F;
+  pm[0][2] = pm[2][0] = -G;
+  pm[3][3] = 2.0 * N;
+  pm[4][4] = 2.0 * L;
+  pm[5][5] = 2.0 * M;
+  static const int ii[6] = {0, 1, 2, 0, 1, 2};
+  static const int jj[6] = {0, 1, 2, 1, 2, 0};
+  double t[6][6];
+  for (int k = 0; k < 6; ++k) {
+    // Voigt image of q e q^T, e the symmetric unit tensor of component k.
+    for (int row = 0; row < 6; ++row) {
+      const int a = ii[row], b = jj[row];
+      const int c = ii[k], dd = jj[k];
+      double v = axes[a][c] * axes[b][dd];
+      if (c != dd) v += axes[a][dd] * axes[b][c];
+      t[row][k] = v;
+    }
+  }
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) {
+      double s = 0.0;
+      for (int a = 0; a < 6; ++a)
+        for (int b = 0; b < 6; ++b) s += t[a][i] * pm[a][b] * t[b][j];
+      P[i * 6 + j] = s;
+    }
+  return SBK_OK;
+}
+
+int validate_material(const sbk_material& m) {
+  if (!(m.youngs_modulus > 0.0) || !std::isfinite(m.youngs_modulus))
+    return fail(SBK_ERR_CONFIG, "the material needs a positive Young's modulus");
+  if (!(m.poisson_ratio > -1.0 && m.poisson_ratio < 0.5))
+    return fail(SBK_ERR_CONFIG, "the material needs a Poisson ratio in (-1, 0.5)");
+  const double vals[] = {m.yield_stress, m.hardening_modulus, m.kinematic_hardening_modulus, m.saturation_stress,
+                         m.saturation_rate};
+  for (double v : vals)
+    if (!std::isfinite(v) || v < 0.0) return fail(SBK_ERR_CONFIG, "plasticity parameters must be finite and >= 0");
+  if (m.saturation_stress > 0.0 && !(m.saturation_rate > 0.0))
+    return fail(SBK_ERR_CONFIG, "a Voce saturation stress needs a positive saturation rate");
+  if (m.num_backstresses < 0 || m.num_backstresses > SBK_MAX_BACKSTRESSES)
+    return fail(SBK_ERR_CONFIG, "at most 4 backstresses are supported");
+  for (int i = 0; i < m.num_backstresses; ++i)
+    if (!finite_positive(m.backstress_modulus[i]) || !std::isfinite(m.backstress_recovery[i]) ||
+        m.backstress_recovery[i] < 0.0)
+      return fail(SBK_ERR_CONFIG, "a backstress needs a finite positive modulus and a non-negative recovery");
+  const bool enabled = m.yield_stress > 0.0;
+  if (!enabled && (m.hardening_modulus > 0.0 || m.kinematic_hardening_modulus > 0.0 || m.saturation_stress > 0.0 ||
+                   m.num_backstresses > 0))
+    return fail(SBK_ERR_CONFIG, "hardening parameters need a yield stress");
+  if (!enabled && m.criterion != SBK_VON_MISES) return fail(SBK_ERR_CONFIG, "a yield criterion needs a yield stress");
+  const bool general = m.criterion == SBK_HILL48 || m.num_backstresses > 0;
+  const int terms = m.num_backstresses + (m.kinematic_hardening_modulus > 0.0 ? 1 : 0);
+  if (general && terms > SBK_MAX_BACKSTRESSES)
+    return fail(SBK_ERR_CONFIG, "backstresses plus Prager's modulus exceed 4 kinematic terms");
+  if (m.kinematic_integration != SBK_EXPONENTIAL && m.kinematic_integration != SBK_BACKWARD_EULER)
+    return fail(SBK_ERR_CONFIG, "unknown kinematic integration");
+  return SBK_OK;
+}
+
+// Gauss-Legendre rules (src/elements/Quadrature.cpp:16-219).
+std::vector<std::pair<double, double>> line_rule(int n) {
+  std::vector<std::pair<double, double>> r;
+  if (n == 1) return {{0.0, 2.0}};
+  if (n == 2) {
+    const double a = 1.0 / std::sqrt(3.0);
+    return {{-a, 1.0}, {a, 1.0}};
+  }
+  if (n == 3) {
+    const double a = std::sqrt(3.0 / 5.0);
+    return {{-a, 5.0 / 9.0}, {0.0, 8.0 / 9.0}, {a, 5.0 / 9.0}};
+  }
+  if (n == 4) {
+    const double s6 = std::sqrt(6.0 / 5.0);
+    const double x1 = std::sqrt((3.0 - 2.0 * s6) / 7.0), x2 = std::sqrt((3.0 + 2.0 * s6) / 7.0);
+    const double s = std::sqrt(30.0);
+    const double w1 = (18.0 + s) / 36.0, w2 = (18.0 - s) / 36.0;
+    return {{-x2, w2}, {-x1, w1}, {x1, w1}, {x2, w2}};
+  }
+  r.assign(static_cast<size_t>(n), {0.0, 0.0});
+  const double pi = std::acos(-1.0);
+  auto legendre = [n](double x, double& p0, double& p1) {
+    p0 = 1.0;
+    p1 = x;
+    for (int k = 2; k <= n; ++k) {
+      const double p2 = ((2.0 * k - 1.0) * x * p1 - (k - 1.0) * p0) / k;
+      p0 = p1;
+      p1 = p2;
+    }
+  };
+  for (int i = 0; i < (n + 1) / 2; ++i) {
+    double x = std::cos(pi * (i + 0.75) / (n + 0.5));
+    for (int it = 0; it < 100; ++it) {
+      double p0, p1;
+      legendre(x, p0, p1);
+      const double der = n * (x * p1 - p0) / (x * x - 1.0);
+      const double step = p1 / der;
+      x -= step;
+      if (std::fabs(step) <= 1.0e-16) break;
+    }
+    if (2 * i + 1 == n) x = 0.0;
+    double p0, p1;
+    legendre(x, p0, p1);
+    const double der = n * (x * p1 - p0) / (x * x - 1.0);
+    const double w = 2.0 / ((1.0 - x * x) * der * der);
+    r[static_cast<size_t>(i)] = {-x, w};
+    r[static_cast<size_t>(n - 1 - i)] = {x, w};
+  }
+  return r;
+}
+
+int make_rule(const sbk_rule& rule, std::vector<double>& pts) {
+  int np = rule.stiffness_points, nt = rule.thickness_points, axis = rule.thickness_axis;
+  if (np < 1 || np > 4) return fail(SBK_ERR_CONFIG, "stiffness points must be 1 to 4");
+  if (nt <= 0 || nt == np) {
+    nt = np;
+    axis = 2;
+  }
+  if (nt > 7) return fail(SBK_ERR_CONFIG, "thickness points must be 1 to 7");
+  if (axis < 0 || axis > 2) return fail(SBK_ERR_CONFIG, "the thickness axis must be 0, 1 or 2");
+  const auto plane = line_rule(np), through = line_rule(nt);
+  const auto& rx = axis == 0 ? through : plane;
+  const auto& ry = axis == 1 ? through : plane;
+  const auto& rz = axis == 2 ? through : plane;
+  pts.clear();
+  for (const auto& gk : rz)
+    for (const auto& gj : ry)
+      for (const auto& gi : rx) {
+        pts.push_back(gi.first);
+        pts.push_back(gj.first);
+        pts.push_back(gk.first);
+        pts.push_back(gi.second * gj.second * gk.second);
+      }
+  return SBK_OK;
+}
+
+int make_params(const sbk_material* mat, const sbk_rule* rule, int kinematics, Params& p) {
+  if (!mat || !rule) return fail(SBK_ERR_ARGUMENT, "null material or rule");
+  int rc = validate_material(*mat);
+  if (rc) return rc;
+  if (kinematics < SBK_SMALL_STRAIN || kinematics > SBK_FINITE_LOGARITHMIC)
+    return fail(SBK_ERR_ARGUMENT, "unknown kinematics");
+  std::vector<double> pts;
+  rc = make_rule(*rule, pts);
+  if (rc) return rc;
+  const int nq = static_cast<int>(pts.size() / 4);
+  if (nq > SBK_MAX_POINTS) return fail(SBK_ERR_UNSUPPORTED, "rules of more than 32 points are not supported");
+  std::memset(&p, 0, sizeof(Params));
+  const double E = mat->youngs_modulus, nu = mat->poisson_ratio;
+  p.G = E / (2.0 * (1.0 + nu));
+  const double lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+  p.K = lam + 2.0 * p.G / 3.0;
+  p.sy0 = mat->yield_stress;
+  p.H = mat->hardening_modulus;
+  p.Hkin = mat->kinematic_hardening_modulus;
+  p.Q = mat->saturation_stress;
+  p.delta = mat->saturation_rate;
+  rc = yield_matrix(*mat, p.P);
+  if (rc) return rc;
+  p.general = (mat->criterion == SBK_HILL48 || mat->num_backstresses > 0) ? 1 : 0;
+  p.enabled = p.sy0 > 0.0 ? 1 : 0;
+  p.integration = mat->kinematic_integration;
+  p.symmetric = 1;
+  for (int i = 0; i < mat->num_backstresses; ++i)
+    if (mat->backstress_recovery[i] > 0.0) p.symmetric = 0;
+  p.nterms = 0;
+  if (p.general) {
+    for (int i = 0; i < mat->num_backstresses; ++i) {
+      p.termC[p.nterms] = mat->backstress_modulus[i];
+      p.termG[p.nterms] = mat->backstress_recovery[i];
+      ++p.nterms;
+    }
+    if (p.Hkin > 0.0) {
+      p.termC[p.nterms] = p.Hkin;
+      p.termG[p.nterms] = 0.0;
+      ++p.nterms;
+    }
+  }
+  p.kinematics = kinematics;
+  p.nq = nq;
+  p.nfields = sbk::state_fields(p.nterms);
+  for (int q = 0; q < nq; ++q)
+    for (int k = 0; k < 4; ++k) p.qp[q][k] = pts[4 * q + k];
+  return SBK_OK;
+}
+
+template <class T>
+int dalloc(T** ptr, size_t count) {
+  *ptr = nullptr;
+  if (count == 0) return SBK_OK;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(ptr), count * sizeof(T));
+  if (e != cudaSuccess) return fail(SBK_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return SBK_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+struct sbk_system {
+  Params p;
+  int64_t nn = 0, ne = 0, nnz = 0, num_blocks = 0;
+  cudaStream_t stream = nullptr;
+  bool plastic = false;
+  // mesh
+  double* coords = nullptr;
+  int32_t* conn = nullptr;
+  // history and trial
+  double* committed = nullptr;
+  double* trial = nullptr;
+  double* alpha_c = nullptr;
+  double* alpha_t = nullptr;
+  // element outputs
+  double* force = nullptr;
+  double* tangent = nullptr;
+  double* energy_e = nullptr;
+  uint8_t* yield = nullptr;
+  int32_t* iters = nullptr;
+  int32_t* code = nullptr;
+  int32_t* first_fail = nullptr;
+  // assembly
+  int32_t* outer = nullptr;
+  int32_t* inner = nullptr;
+  double* values = nullptr;
+  double* internal = nullptr;
+  double* scratch = nullptr;
+  double* scalars = nullptr;
+  int32_t* missing = nullptr;
+  int32_t* block_col = nullptr;
+  int64_t* block_value = nullptr;
+  int32_t* block_ptr = nullptr;
+  int32_t* block_src = nullptr;
+  int32_t* node_ptr = nullptr;
+  int32_t* node_src = nullptr;
+  int elements_per_block = 0;
+  bool has_trial = false;
+
+  sbk::GatherMaps maps() const {
+    sbk::GatherMaps m;
+    m.num_nodes = nn;
+    m.num_elements = ne;
+    m.nnz = nnz;
+    m.num_blocks = num_blocks;
+    m.block_col = block_col;
+    m.block_value = block_value;
+    m.block_ptr = block_ptr;
+    m.block_src = block_src;
+    m.outer = outer;
+    m.node_ptr = node_ptr;
+    m.node_src = node_src;
+    return m;
+  }
+};
+
+namespace {
+
+void free_system(sbk_system* s) {
+  void* ptrs[] = {s->coords, s->conn, s->committed, s->trial, s->alpha_c, s->alpha_t, s->force,
+                  s->tangent, s->energy_e, s->yield, s->iters, s->code, s->first_fail, s->outer,
+                  s->inner, s->values, s->internal, s->scratch, s->scalars, s->missing, s->block_col,
+                  s->block_value, s->block_ptr, s->block_src, s->node_ptr, s->node_src};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete s;
+}
+
+// Assembler::build_pattern (src/fem/Assembler.cpp:86-173) and the gather
+// maps of the assembly kernels, on the host (once per mesh).
+struct HostPattern {
+  std::vector<int32_t> outer, inner;
+  std::vector<int32_t> block_col, block_ptr, block_src, node_ptr, node_src;
+  std::vector<int64_t> block_value;
+};
+
+int build_pattern(int64_t nn, int64_t ne, const int32_t* conn, HostPattern& hp) {
+  std::vector<int64_t> inc_ptr(static_cast<size_t>(nn) + 1, 0);
+  for (int64_t e = 0; e < ne; ++e)
+    for (int a = 0; a < 8; ++a) {
+      const int32_t n = conn[e * 8 + a];
+      if (n < 0 || n >= nn) return fail(SBK_ERR_MESH, "connectivity names a node out of range");
+      ++inc_ptr[static_cast<size_t>(n) + 1];
+    }
+  for (int64_t n = 0; n < nn; ++n) inc_ptr[n + 1] += inc_ptr[n];
+  // Incidences (node -> e * 8 + a), ascending element order.
+  hp.node_ptr.assign(inc_ptr.begin(), inc_ptr.end());
+  hp.node_src.assign(static_cast<size_t>(ne) * 8, 0);
+  {
+    std::vector<int64_t> fill(inc_ptr.begin(), inc_ptr.end() - 1);
+    for (int64_t e = 0; e < ne; ++e)
+      for (int a = 0; a < 8; ++a) hp.node_src[fill[conn[e * 8 + a]]++] = static_cast<int32_t>(e * 8 + a);
+  }
+  // Sorted neighbourhoods (the node itself included).
+  std::vector<int64_t> nbr_ptr(static_cast<size_t>(nn) + 1, 0);
+  std::vector<int32_t> nbr;
+  nbr.reserve(static_cast<size_t>(nn) * 27);
+  {
+    std::vector<int32_t> marker(static_cast<size_t>(nn), -1), list;
+    for (int64_t b = 0; b < nn; ++b) {
+      list.clear();
+      for (int64_t k = inc_ptr[b]; k < inc_ptr[b + 1]; ++k) {
+        const int32_t* nodes = conn + static_cast<int64_t>(hp.node_src[k] >> 3) * 8;
+        for (int a = 0; a < 8; ++a)
+          if (marker[nodes[a]] != b) {
+            marker[nodes[a]] = static_cast<int32_t>(b);
+            list.push_back(nodes[a]);
+          }
+      }
+      std::sort(list.begin(), list.end());
+      nbr.insert(nbr.end(), list.begin(), list.end());
+      nbr_ptr[b + 1] = static_cast<int64_t>(nbr.size());
+    }
+  }
+  const int64_t n = nn * 3;
+  hp.outer.assign(static_cast<size_t>(n) + 1, 0);
+  int64_t total = 0;
+  for (int64_t b = 0; b < nn; ++b) {
+    const int64_t deg = nbr_ptr[b + 1] - nbr_ptr[b];
+    for (int kb = 0; kb < 3; ++kb) {
+      total += deg * 3;
+      if (total > 0x7fffffffLL) return fail(SBK_ERR_UNSUPPORTED, "the pattern exceeds 2^31 entries (int32 indices)");
+      hp.outer[static_cast<size_t>(b * 3 + kb) + 1] = static_cast<int32_t>(total);
+    }
+  }
+  hp.inner.resize(static_cast<size_t>(total));
+  for (int64_t b = 0; b < nn; ++b)
+    for (int kb = 0; kb < 3; ++kb) {
+      int64_t q = hp.outer[static_cast<size_t>(b * 3 + kb)];
+      for (int64_t k = nbr_ptr[b]; k < nbr_ptr[b + 1]; ++k)
+        for (int ka = 0; ka < 3; ++ka) hp.inner[static_cast<size_t>(q++)] = nbr[k] * 3 + ka;
+    }
+  // Node blocks in CSC order and their element contributions.
+  const int64_t nb = static_cast<int64_t>(nbr.size());
+  hp.block_col.resize(static_cast<size_t>(nb));
+  hp.block_value.resize(static_cast<size_t>(nb));
+  for (int64_t b = 0; b < nn; ++b)
+    for (int64_t k = nbr_ptr[b]; k < nbr_ptr[b + 1]; ++k) {
+      hp.block_col[k] = static_cast<int32_t>(b);
+      hp.block_value[k] = hp.outer[static_cast<size_t>(b * 3)] + 3 * (k - nbr_ptr[b]);
+    }
+  std::vector<int64_t> bcount(static_cast<size_t>(nb) + 1, 0);
+  std::vector<int32_t> where(static_cast<size_t>(ne) * 64);
+  for (int64_t e = 0; e < ne; ++e) {
+    const int32_t* nodes = conn + e * 8;
+    for (int b = 0; b < 8; ++b) {
+      const int32_t* begin = nbr.data() + nbr_ptr[nodes[b]];
+      const int32_t* end = nbr.data() + nbr_ptr[nodes[b] + 1];
+      for (int a = 0; a < 8; ++a) {
+        const int32_t* hit = std::lower_bound(begin, end, nodes[a]);
+        const int64_t blk = (hit - nbr.data());
+        where[e * 64 + a * 8 + b] = static_cast<int32_t>(blk);
+        ++bcount[static_cast<size_t>(blk) + 1];
+      }
+    }
+  }
+  for (int64_t b = 0; b < nb; ++b) bcount[b + 1] += bcount[b];
+  if (bcount[nb] > 0x7fffffffLL) return fail(SBK_ERR_UNSUPPORTED, "too many element blocks for int32 maps");
+  hp.block_ptr.assign(bcount.begin(), bcount.end());
+  hp.block_src.resize(static_cast<size_t>(bcount[nb]));
+  {
+    std::vector<int64_t> fill(bcount.begin(), bcount.end() - 1);
+    for (int64_t e = 0; e < ne; ++e)
+      for (int ab = 0; ab < 64; ++ab) hp.block_src[fill[where[e * 64 + ab]]++] = static_cast<int32_t>(e * 64 + ab);
+  }
+  return SBK_OK;
+}
+
+template <class T>
+int upload(T** dst, const std::vector<T>& src, cudaStream_t s) {
+  int rc = dalloc(dst, src.size());
+  if (rc) return rc;
+  if (!src.empty()) SBK_CUDA(cudaMemcpyAsync(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  return SBK_OK;
+}
+
+}  // namespace
+
+namespace sbk {
+int set_error(int code, const std::string& what) { return fail(code, what); }
+}  // namespace sbk
+
+extern "C" {
+
+const char* sbk_last_error(void) { return g_error.c_str(); }
+
+int sbk_rule_size(const sbk_rule* rule) {
+  if (!rule) return 0;
+  std::vector<double> pts;
+  if (make_rule(*rule, pts) != SBK_OK) return 0;
+  return static_cast<int>(pts.size() / 4);
+}
+
+int sbk_state_fields(const sbk_material* material) {
+  if (!material) return 0;
+  const bool general = material->criterion == SBK_HILL48 || material->num_backstresses > 0;
+  int terms = 0;
+  if (general) terms = material->num_backstresses + (material->kinematic_hardening_modulus > 0.0 ? 1 : 0);
+  return sbk::state_fields(terms);
+}
+
+int sbk_yield_matrix(const sbk_material* material, double* p_out) {
+  if (!material || !p_out) return fail(SBK_ERR_ARGUMENT, "null argument");
+  int rc = validate_material(*material);
+  if (rc) return rc;
+  return yield_matrix(*material, p_out);
+}
+
+int sbk_element_batch(const sbk_material* material, const sbk_rule* rule, int kinematics, int64_t ne,
+                      const double* x_dev, const double* u_dev, const double* state_dev, const double* alpha_dev,
+                      double* force_dev, double* tangent_dev, double* energy_dev, double* trial_dev,
+                      double* alpha_out_dev, uint8_t* yield_dev, int32_t* iterations_dev, int32_t* code_dev,
+                      void* stream) {
+  int rc = check_device();
+  if (rc) return rc;
+  Params p;
+  rc = make_params(material, rule, kinematics, p);
+  if (rc) return rc;
+  if (ne < 0) return fail(SBK_ERR_ARGUMENT, "negative element count");
+  if (ne == 0) return SBK_OK;
+  if (!x_dev || !u_dev || !state_dev || !force_dev || !energy_dev || !trial_dev || !alpha_out_dev || !yield_dev ||
+      !iterations_dev || !code_dev)
+    return fail(SBK_ERR_ARGUMENT, "null device buffer");
+  if (ne * p.nq > 0x7fffffffLL) return fail(SBK_ERR_UNSUPPORTED, "too many points for one batch");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  rc = sbk::launch_elements(p, ne, x_dev, nullptr, u_dev, state_dev, alpha_dev, tangent_dev != nullptr, force_dev,
+                            tangent_dev, energy_dev, trial_dev, alpha_out_dev, yield_dev, iterations_dev, code_dev,
+                            nullptr, true, 0, s);
+  if (rc) return fail(SBK_ERR_CUDA, std::string("element kernel launch: ") + cudaGetErrorString((cudaError_t)rc));
+  return SBK_OK;
+}
+
+int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const sbk_rule* rule, int kinematics,
+                      sbk_system** out) {
+  if (!out) return fail(SBK_ERR_ARGUMENT, "null output handle");
+  *out = nullptr;
+  int rc = check_device();
+  if (rc) return rc;
+  if (!mesh || !mesh->coords || !mesh->connectivity || mesh->num_nodes <= 0 || mesh->num_elements <= 0)
+    return fail(SBK_ERR_ARGUMENT, "an empty or null mesh");
+  Params p;
+  rc = make_params(material, rule, kinematics, p);
+  if (rc) return rc;
+  sbk_system* s = new sbk_system();
+  s->p = p;
+  s->nn = mesh->num_nodes;
+  s->ne = mesh->num_elements;
+  s->plastic = p.enabled != 0;
+  if (s->ne * p.nq > 0x7fffffffLL) {
+    free_system(s);
+    return fail(SBK_ERR_UNSUPPORTED, "too many points");
+  }
+  HostPattern hp;
+  rc = build_pattern(s->nn, s->ne, mesh->connectivity, hp);
+  if (rc) {
+    free_system(s);
+    return rc;
+  }
+  s->nnz = static_cast<int64_t>(hp.inner.size());
+  s->num_blocks = static_cast<int64_t>(hp.block_col.size());
+  const int64_t npts = s->ne * p.nq;
+  const size_t state_size = static_cast<size_t>(npts) * p.nfields;
+  std::vector<double> coords(mesh->coords, mesh->coords + 3 * s->nn);
+  std::vector<int32_t> conn(mesh->connectivity, mesh->connectivity + 8 * s->ne);
+#define TRY(x)          \
+  do {                  \
+    rc = (x);           \
+    if (rc) {           \
+      free_system(s);   \
+      return rc;        \
+    }                   \
+  } while (0)
+  TRY(upload(&s->coords, coords, nullptr));
+  TRY(upload(&s->conn, conn, nullptr));
+  TRY(dalloc(&s->committed, state_size));
+  TRY(dalloc(&s->trial, state_size));
+  TRY(dalloc(&s->alpha_c, static_cast<size_t>(s->ne) * 9));
+  TRY(dalloc(&s->alpha_t, static_cast<size_t>(s->ne) * 9));
+  TRY(dalloc(&s->force, static_cast<size_t>(s->ne) * 24));
+  TRY(dalloc(&s->tangent, static_cast<size_t>(s->ne) * 576));
+  TRY(dalloc(&s->energy_e, static_cast<size_t>(s->ne)));
+  TRY(dalloc(&s->yield, static_cast<size_t>(npts)));
+  TRY(dalloc(&s->iters, static_cast<size_t>(s->ne)));
+  TRY(dalloc(&s->code, static_cast<size_t>(s->ne)));
+  TRY(dalloc(&s->first_fail, 1));
+  TRY(upload(&s->outer, hp.outer, nullptr));
+  TRY(upload(&s->inner, hp.inner, nullptr));
+  TRY(dalloc(&s->values, static_cast<size_t>(s->nnz)));
+  TRY(dalloc(&s->internal, static_cast<size_t>(s->nn) * 3));
+  TRY(dalloc(&s->scratch, sbk::assemble_scratch_doubles()));
+  TRY(dalloc(&s->scalars, 4));
+  TRY(dalloc(&s->missing, 1));
+  TRY(upload(&s->block_col, hp.block_col, nullptr));
+  TRY(upload(&s->block_value, hp.block_value, nullptr));
+  TRY(upload(&s->block_ptr, hp.block_ptr, nullptr));
+  TRY(upload(&s->block_src, hp.block_src, nullptr));
+  TRY(upload(&s->node_ptr, hp.node_ptr, nullptr));
+  TRY(upload(&s->node_src, hp.node_src, nullptr));
+#undef TRY
+  // Virgin points and zero modes (initialise_history).
+  cudaMemset(s->committed, 0, state_size * sizeof(double));
+  cudaMemset(s->alpha_c, 0, static_cast<size_t>(s->ne) * 9 * sizeof(double));
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    free_system(s);
+    return fail(SBK_ERR_CUDA, std::string("system upload: ") + cudaGetErrorString(e));
+  }
+  *out = s;
+  return SBK_OK;
+}
+
+int sbk_system_destroy(sbk_system* sys) {
+  if (!sys) return SBK_OK;
+  cudaStreamSynchronize(sys->stream);
+  free_system(sys);
+  return SBK_OK;
+}
+
+int sbk_system_set_stream(sbk_system* sys, void* stream) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  sys->stream = static_cast<cudaStream_t>(stream);
+  return SBK_OK;
+}
+
+int sbk_system_set_elements_per_block(sbk_system* sys, int epb) {
+  if (!sys || epb < 0 || epb > 16) return fail(SBK_ERR_ARGUMENT, "bad elements per block");
+  sys->elements_per_block = epb;
+  return SBK_OK;
+}
+
+int sbk_system_pattern(const sbk_system* sys, sbk_pattern* out) {
+  if (!sys || !out) return fail(SBK_ERR_ARGUMENT, "null argument");
+  out->num_dofs = sys->nn * 3;
+  out->nnz = sys->nnz;
+  out->outer_dev = sys->outer;
+  out->inner_dev = sys->inner;
+  return SBK_OK;
+}
+
+int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int want_tangent,
+                        sbk_evaluation* out) {
+  (void)lambda;  // the forming system carries no dead load: f_ext = 0 (NonlinearSystem.hpp:87-92)
+  if (!sys || !u_dev || !out) return fail(SBK_ERR_ARGUMENT, "null argument");
+  cudaStream_t st = sys->stream;
+  std::memset(out, 0, sizeof(*out));
+  out->failed_element = -1;
+  SBK_CUDA(cudaMemsetAsync(sys->first_fail, 0x7f, sizeof(int32_t), st));
+  int rc = sbk::launch_elements(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c,
+                                want_tangent, sys->force, sys->tangent, sys->energy_e, sys->trial, sys->alpha_t,
+                                sys->yield, sys->iters, sys->code, sys->first_fail, false,
+                                sys->elements_per_block, st);
+  if (rc) return fail(SBK_ERR_CUDA, std::string("element kernel: ") + cudaGetErrorString((cudaError_t)rc));
+  int32_t first = 0;
+  SBK_CUDA(cudaMemcpyAsync(&first, sys->first_fail, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  SBK_CUDA(cudaStreamSynchronize(st));
+  if (first != 0x7f7f7f7f) {
+    int32_t code = 0;
+    SBK_CUDA(cudaMemcpy(&code, sys->code + first, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    out->failed_element = first;
+    out->failure_code = code;
+    sys->has_trial = false;
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "Hex8 element %d: SolverError (code %d)", first, code);
+    return fail(SBK_ERR_SOLVER, buf);
+  }
+  rc = sbk::launch_assemble_forces(sys->maps(), sys->force, sys->energy_e, sys->yield, sys->p.nq, sys->internal,
+                                   sys->scratch, sys->scalars, st);
+  if (rc) return fail(SBK_ERR_CUDA, std::string("assembly: ") + cudaGetErrorString((cudaError_t)rc));
+  if (want_tangent) {
+    rc = sbk::launch_assemble_values(sys->maps(), sys->tangent, sys->values, st);
+    if (rc) return fail(SBK_ERR_CUDA, std::string("assembly: ") + cudaGetErrorString((cudaError_t)rc));
+  }
+  double sc[3];
+  SBK_CUDA(cudaMemcpyAsync(sc, sys->scalars, sizeof(sc), cudaMemcpyDeviceToHost, st));
+  SBK_CUDA(cudaStreamSynchronize(st));
+  out->internal_dev = sys->internal;
+  out->residual_dev = sys->internal;
+  out->values_dev = want_tangent ? sys->values : nullptr;
+  out->energy = sc[0];
+  out->gross = std::sqrt(sc[1]);
+  out->yielding_points = static_cast<int32_t>(sc[2]);
+  sys->has_trial = true;
+  return SBK_OK;
+}
+
+int sbk_system_commit(sbk_system* sys) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  if (!sys->has_trial) return fail(SBK_ERR_ARGUMENT, "no successful evaluation to commit");
+  std::swap(sys->committed, sys->trial);
+  std::swap(sys->alpha_c, sys->alpha_t);
+  sys->has_trial = false;
+  return SBK_OK;
+}
+
+int sbk_system_get_committed(const sbk_system* sys, double* state, double* alpha) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  const size_t ns = static_cast<size_t>(sys->ne) * sys->p.nq * sys->p.nfields;
+  if (state) SBK_CUDA(cudaMemcpy(state, sys->committed, ns * sizeof(double), cudaMemcpyDeviceToHost));
+  if (alpha) SBK_CUDA(cudaMemcpy(alpha, sys->alpha_c, static_cast<size_t>(sys->ne) * 9 * sizeof(double),
+                                 cudaMemcpyDeviceToHost));
+  return SBK_OK;
+}
+
+int sbk_system_set_committed(sbk_system* sys, const double* state, const double* alpha) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  const size_t ns = static_cast<size_t>(sys->ne) * sys->p.nq * sys->p.nfields;
+  if (state) {
+    for (size_t i = 0; i < ns; ++i)
+      if (!std::isfinite(state[i])) return fail(SBK_ERR_CONFIG, "the saved plastic history is not finite");
+    SBK_CUDA(cudaMemcpy(sys->committed, state, ns * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  if (alpha) {
+    for (size_t i = 0; i < static_cast<size_t>(sys->ne) * 9; ++i)
+      if (!std::isfinite(alpha[i])) return fail(SBK_ERR_CONFIG, "the saved internal-mode parameters are not finite");
+    SBK_CUDA(cudaMemcpy(sys->alpha_c, alpha, static_cast<size_t>(sys->ne) * 9 * sizeof(double),
+                        cudaMemcpyHostToDevice));
+  }
+  return SBK_OK;
+}
+
+int sbk_system_get_trial(const sbk_system* sys, double* state, double* alpha, uint8_t* yield) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  const size_t npts = static_cast<size_t>(sys->ne) * sys->p.nq;
+  if (state) SBK_CUDA(cudaMemcpy(state, sys->trial, npts * sys->p.nfields * sizeof(double), cudaMemcpyDeviceToHost));
+  if (alpha) SBK_CUDA(cudaMemcpy(alpha, sys->alpha_t, static_cast<size_t>(sys->ne) * 9 * sizeof(double),
+                                 cudaMemcpyDeviceToHost));
+  if (yield) SBK_CUDA(cudaMemcpy(yield, sys->yield, npts, cudaMemcpyDeviceToHost));
+  return SBK_OK;
+}
+
+int sbk_system_buffers(const sbk_system* sys, const double** committed_state_dev, const double** committed_alpha_dev,
+                       const double** trial_state_dev, const double** trial_alpha_dev) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  if (committed_state_dev) *committed_state_dev = sys->committed;
+  if (committed_alpha_dev) *committed_alpha_dev = sys->alpha_c;
+  if (trial_state_dev) *trial_state_dev = sys->trial;
+  if (trial_alpha_dev) *trial_alpha_dev = sys->alpha_t;
+  return SBK_OK;
+}
+
+int sbk_system_symmetric(const sbk_system* sys) { return sys && sys->p.symmetric ? 1 : 0; }
+int sbk_system_plastic(const sbk_system* sys) { return sys && sys->plastic ? 1 : 0; }
+
+int sbk_system_add_node_blocks(sbk_system* sys, int32_t n, const int32_t* nodes_dev, const double* blocks_dev) {
+  if (!sys || (n > 0 && (!nodes_dev || !blocks_dev))) return fail(SBK_ERR_ARGUMENT, "null argument");
+  if (n <= 0) return SBK_OK;
+  cudaStream_t st = sys->stream;
+  SBK_CUDA(cudaMemsetAsync(sys->missing, 0, sizeof(int32_t), st));
+  int rc = sbk::launch_add_node_blocks(sys->outer, sys->inner, sys->values, n, nodes_dev, blocks_dev, sys->missing, st);
+  if (rc) return fail(SBK_ERR_CUDA, "add_node_blocks launch");
+  int32_t missing = 0;
+  SBK_CUDA(cudaMemcpyAsync(&missing, sys->missing, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  SBK_CUDA(cudaStreamSynchronize(st));
+  if (missing) return fail(SBK_ERR_ARGUMENT, "a node block lies outside the pattern");
+  return SBK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,1205 @@
+// K1: the incompatible-mode Hex8 element on the GPU.
+//
+// One group of G lanes (G = 8 for rules of up to 8 points, 16 or 32 for
+// larger ones) evaluates one element; a 32-lane warp holds 32 / G elements.
+// Lane q owns integration point q: its kinematics, its return map and its
+// share of K_aa, which a shuffle reduce-scatter sums over the group into
+// shared memory. The element-level work of the local Newton iteration - the
+// 9x9 factorisations, the line searches and their fallbacks - runs on lane 0
+// over shared memory, every decision being read back by the whole group, so
+// the group's control flow stays uniform. After convergence the lanes split
+// the condensation by element node: lane a forms the rows of node a of K_ua,
+// K_uu and K* = K_uu - K_ua K_aa^-1 K_au.
+//
+// Algorithm: incompatible_elastoplastic_element and solve_and_condense
+// (src/fem/IncompatibleModes.cpp:134-600, constants
+// src/fem/IncompatibleModes.hpp:98-127). The local iteration, the line
+// search on the directional residual, the shifted direction, the
+// Levenberg-Marquardt fallback and the condensation follow it step for
+// step; the arithmetic is reorganised for the GPU (the strain operator is
+// never stored: B^T D B products are formed from F, D and the gradients).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "sbk_element.h"
+#include "sbk_material.cuh"
+
+namespace sbk {
+namespace {
+
+constexpr int kMaxLocal = 25;
+constexpr double kFullStepReduction = 1.0 - 1.0e-4;
+constexpr int kMaxLineSearch = 8;
+constexpr double kLineSearchRatio = 0.5;
+constexpr double kLocalShift = 1.0e-3;
+constexpr double kLocalMarquardt = 1.0e-6;
+constexpr double kLocalTolerance = 1.0e-8;
+constexpr double kLocalRoundOff = 1.0e-13;
+
+constexpr int kSlot = 56;  // per point: D 36 | S 6 | F 9 | w | energy | floor factor | pad
+constexpr int kSlotS = 36, kSlotF = 42, kSlotW = 51, kSlotE = 52, kSlotFl = 53;
+
+__constant__ double kCorner[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
+                                     {-1, -1, 1},  {1, -1, 1},  {1, 1, 1},  {-1, 1, 1}};
+
+template <int G>
+struct __align__(16) ElemShared {
+  double X[24];
+  double U[24];
+  double jinv0[9];
+  double geo[G][12];  // J^-1 (9), w det J, det0 / det
+  double hu[G][9];
+  double slot[G][kSlot];
+  double kaa[((81 + G - 1) / G) * G];
+  double r[33];
+  double scale[9];
+  double flo[9];
+  double energy;
+  double alpha[9];
+  double dir[9];
+  double dir2[9];
+  double r0[9];
+  double lu[81];
+  double maxpivot;
+  double work[243];  // k0 | sym | scratch; the coupling C (9 x 24) at the end
+  double dval[4];
+  int rowp[9], colp[9], perm[9];
+  int ival[4];
+};
+
+__device__ __forceinline__ void shape_grad(int a, double xi, double eta, double zeta, double dn[3]) {
+  const double fx = 1.0 + xi * kCorner[a][0];
+  const double fy = 1.0 + eta * kCorner[a][1];
+  const double fz = 1.0 + zeta * kCorner[a][2];
+  dn[0] = 0.125 * kCorner[a][0] * fy * fz;
+  dn[1] = 0.125 * kCorner[a][1] * fx * fz;
+  dn[2] = 0.125 * kCorner[a][2] * fx * fy;
+}
+
+__device__ __forceinline__ double det3(const double m[9]) {
+  return m[0] * (m[4] * m[8] - m[7] * m[5]) - m[3] * (m[1] * m[8] - m[7] * m[2]) +
+         m[6] * (m[1] * m[5] - m[4] * m[2]);
+}
+__device__ __forceinline__ void inv3(const double m[9], double out[9]) {
+  out[0] = m[4] * m[8] - m[5] * m[7];
+  out[3] = m[5] * m[6] - m[3] * m[8];
+  out[6] = m[3] * m[7] - m[4] * m[6];
+  const double det = m[0] * out[0] + m[1] * out[3] + m[2] * out[6];
+  const double inv = 1.0 / det;
+  out[1] = m[2] * m[7] - m[1] * m[8];
+  out[4] = m[0] * m[8] - m[2] * m[6];
+  out[7] = m[1] * m[6] - m[0] * m[7];
+  out[2] = m[1] * m[5] - m[2] * m[4];
+  out[5] = m[2] * m[3] - m[0] * m[5];
+  out[8] = m[0] * m[4] - m[1] * m[3];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) out[i] *= inv;
+}
+
+// Reduce-scatter of G values over the G lanes of a group: lane l returns the
+// group sum of v[l]. Fixed pairing, so the result is deterministic.
+template <int G>
+__device__ __forceinline__ double reduce_scatter(double (&v)[G], int lane, unsigned mask) {
+  double cur[G];
+#pragma unroll
+  for (int i = 0; i < G; ++i) cur[i] = v[i];
+#pragma unroll
+  for (int half = G / 2; half >= 1; half >>= 1) {
+    const bool upper = (lane & half) != 0;
+#pragma unroll
+    for (int j = 0; j < half; ++j) {
+      const double send = upper ? cur[j] : cur[half + j];
+      const double keep = upper ? cur[half + j] : cur[j];
+      cur[j] = keep + __shfl_xor_sync(mask, send, half, G);
+    }
+  }
+  return cur[0];
+}
+
+// Voigt index of the tensor pair (i, j).
+__device__ __forceinline__ int voigt(int i, int j) {
+  if (i == j) return i;
+  const int s = i + j;  // (0,1) -> 3, (1,2) -> 4, (0,2) -> 5
+  return s == 1 ? 3 : (s == 3 ? 4 : 5);
+}
+
+// Column (3 m + k) of the Green-Lagrange strain variation for an
+// augmented node with gradient g (3): b[c] for Voigt c = (i, j).
+__device__ __forceinline__ void bcol(const double F[9], const double g[3], int k, double b[6]) {
+  b[0] = F[k * 3 + 0] * g[0];
+  b[1] = F[k * 3 + 1] * g[1];
+  b[2] = F[k * 3 + 2] * g[2];
+  b[3] = F[k * 3 + 0] * g[1] + F[k * 3 + 1] * g[0];
+  b[4] = F[k * 3 + 1] * g[2] + F[k * 3 + 2] * g[1];
+  b[5] = F[k * 3 + 2] * g[0] + F[k * 3 + 0] * g[2];
+}
+
+// V(k, l, n) = sum_{j,i,m} g(j) F(k,i) F(l,m) D[v(i,j)][v(m,n)] (D, or D^T
+// with `transpose`), times w, plus the geometric w S(j,n) g(j) delta_kl:
+// K_ab(k, l) = sum_n V(k, l, n) g_b(n) is the block of B_a^T D B_b + G_a^T S G_b.
+__device__ __forceinline__ void vtensor(const double* slot, const double g[3], bool transpose, bool geometric,
+                                        double V[27]) {
+  const double w = slot[kSlotW];
+  const double* D = slot;
+  const double* F = slot + kSlotF;
+  double W[3][6];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) {
+      double s = 0.0;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const int r = voigt(i, j);
+        s += g[j] * (transpose ? D[c * 6 + r] : D[r * 6 + c]);
+      }
+      W[i][c] = w * s;
+    }
+  double Uk[3][6];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int c = 0; c < 6; ++c) Uk[k][c] = F[k * 3 + 0] * W[0][c] + F[k * 3 + 1] * W[1][c] + F[k * 3 + 2] * W[2][c];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int l = 0; l < 3; ++l)
+#pragma unroll
+      for (int n = 0; n < 3; ++n) {
+        double s = 0.0;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) s += F[l * 3 + m] * Uk[k][voigt(m, n)];
+        V[(k * 3 + l) * 3 + n] = s;
+      }
+  if (geometric) {
+    const double* S = slot + kSlotS;
+    double sg[3];
+#pragma unroll
+    for (int n = 0; n < 3; ++n)
+      sg[n] = w * (g[0] * S[voigt(0, n)] + g[1] * S[voigt(1, n)] + g[2] * S[voigt(2, n)]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int n = 0; n < 3; ++n) V[(k * 3 + k) * 3 + n] += sg[n];
+  }
+}
+
+template <int G>
+struct Ctx {
+  const Params* p;
+  ElemShared<G>* s;
+  int lane;
+  unsigned mask;
+  int64_t e;
+  int64_t npts;  // ne * nq: the state stride
+  const double* state;
+  double* trial;
+  uint8_t* yield;
+  __device__ __forceinline__ void sync() const { __syncwarp(mask); }
+};
+
+// Mode gradients of point q: g~(i, m) = (det0 / det)(-2 xi_m) J0^-1(m, i).
+template <int G>
+__device__ __forceinline__ void mode_grads(const Ctx<G>& c, int q, double gt[9]) {
+  const double ratio = c.s->geo[q][10];
+  const double nat[3] = {c.p->qp[q][0], c.p->qp[q][1], c.p->qp[q][2]};
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const double f = ratio * (-2.0 * nat[m]);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) gt[i * 3 + m] = f * c.s->jinv0[m * 3 + i];
+  }
+}
+// Gradient of node a at point q: g(i) = sum_c dN_a/dxi_c J^-1(c, i).
+template <int G>
+__device__ __forceinline__ void node_grad(const Ctx<G>& c, int q, int a, double g[3]) {
+  double dn[3];
+  shape_grad(a, c.p->qp[q][0], c.p->qp[q][1], c.p->qp[q][2], dn);
+  const double* ji = c.s->geo[q];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) g[i] = dn[0] * ji[i] + dn[1] * ji[3 + i] + dn[2] * ji[6 + i];
+}
+
+// Reference geometry (set_up, IncompatibleModes.cpp:134-192). Returns 0 or
+// SBK_EL_MESH_INVERTED (group-uniform).
+template <int G>
+__device__ int set_up(const Ctx<G>& c) {
+  ElemShared<G>& s = *c.s;
+  const Params& p = *c.p;
+  // Centre Jacobian, every lane alike.
+  double j0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    double dn[3];
+    shape_grad(a, 0.0, 0.0, 0.0, dn);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int k = 0; k < 3; ++k) j0[i * 3 + k] += s.X[3 * a + i] * dn[k];
+  }
+  const double det0 = det3(j0);
+  int bad = !(det0 > 0.0);
+  if (c.lane == 0 && !bad) inv3(j0, s.jinv0);
+  const int q = c.lane;
+  if (q < p.nq && !bad) {
+    double jq[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double dnq[8][3];
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      shape_grad(a, p.qp[q][0], p.qp[q][1], p.qp[q][2], dnq[a]);
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int k = 0; k < 3; ++k) jq[i * 3 + k] += s.X[3 * a + i] * dnq[a][k];
+    }
+    const double det = det3(jq);
+    if (!(det > 0.0)) {
+      bad = 1;
+    } else {
+      double ji[9];
+      inv3(jq, ji);
+#pragma unroll
+      for (int i = 0; i < 9; ++i) s.geo[q][i] = ji[i];
+      s.geo[q][9] = p.qp[q][3] * det;
+      s.geo[q][10] = det0 / det;
+      // hu = U G^T with G(i, a) = sum_c dN_a/dxi_c J^-1(c, i).
+      double hu[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+      for (int a = 0; a < 8; ++a) {
+        double g[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) g[i] = dnq[a][0] * ji[i] + dnq[a][1] * ji[3 + i] + dnq[a][2] * ji[6 + i];
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) hu[i * 3 + j] += s.U[3 * a + i] * g[j];
+      }
+#pragma unroll
+      for (int i = 0; i < 9; ++i) s.hu[q][i] = hu[i];
+    }
+  }
+  bad = __any_sync(c.mask, bad);
+  c.sync();
+  return bad ? SBK_EL_MESH_INVERTED : 0;
+}
+
+// One pass (IncompatibleModes.cpp:337-342): the kinematics, the returns and
+// the sums at `at` (9 values, identical in every lane). Returns 0 or the
+// failure code of the first failing point in the reference's order.
+template <int G>
+__device__ __noinline__ int pass(const Ctx<G>& c, const double at[9]) {
+  ElemShared<G>& s = *c.s;
+  const Params& p = *c.p;
+  const int q = c.lane;
+  const bool active = q < p.nq;
+  const bool geometric = p.kinematics != SBK_SMALL_STRAIN;
+  int fail = 0;  // (stage << 8) | q, stage 1 kinematics, 2 return
+  int code = 0;
+  double gt[9], F[9], hmax = 0.0;
+  double kbuf[G];
+  double M[36], S[6];
+  double w = 0.0;
+  if (active) {
+    w = s.geo[q][9];
+    mode_grads(c, q, gt);
+    double h[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        double v = s.hu[q][i * 3 + j];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) v += at[3 * m + i] * gt[j * 3 + m];
+        h[i * 3 + j] = v;
+      }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      hmax = fmax(hmax, fabs(h[i]));
+      F[i] = h[i] + ((i % 4) == 0 ? 1.0 : 0.0);
+    }
+    double strain[6];
+    LogKin L;
+    if (p.kinematics == SBK_SMALL_STRAIN) {
+      strain[0] = h[0];
+      strain[1] = h[4];
+      strain[2] = h[8];
+      strain[3] = h[1] + h[3];
+      strain[4] = h[5] + h[7];
+      strain[5] = h[6] + h[2];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) F[i] = (i % 4) == 0 ? 1.0 : 0.0;
+    } else {
+      double E[9];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          E[i * 3 + j] = 0.5 * (h[i * 3 + j] + h[j * 3 + i] + h[0 * 3 + i] * h[0 * 3 + j] +
+                                h[1 * 3 + i] * h[1 * 3 + j] + h[2 * 3 + i] * h[2 * 3 + j]);
+      double green[6] = {E[0], E[4], E[8], 2.0 * E[1], 2.0 * E[5], 2.0 * E[6]};
+      if (p.kinematics == SBK_FINITE) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) strain[i] = green[i];
+      } else {
+        if (!(det3(F) > 0.0)) {
+          code = SBK_EL_INVERTED_POINT;
+        } else {
+          code = log_strain(green, L, strain);
+        }
+        if (code) fail = (1 << 8) | q;
+      }
+    }
+    if (!fail) {
+      PointState st{c.state + c.e * p.nq + q, c.trial + c.e * p.nq + q, c.npts};
+      Response r;
+      code = p.general ? general_return(p, strain, st, r) : radial_return(p, strain, st, r);
+      if (code) {
+        fail = (2 << 8) | q;
+      } else {
+        c.yield[c.e * p.nq + q] = r.yielding ? 1 : 0;
+#pragma unroll
+        for (int i = 0; i < 36; ++i) M[i] = r.C[i];
+        if (p.kinematics == SBK_FINITE_LOGARITHMIC) {
+          log_transform(L, r.stress, S, M);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 6; ++i) S[i] = r.stress[i];
+        }
+        double mmax = 0.0;
+#pragma unroll
+        for (int i = 0; i < 36; ++i) {
+          s.slot[q][i] = M[i];
+          mmax = fmax(mmax, fabs(M[i]));
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) s.slot[q][kSlotS + i] = S[i];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) s.slot[q][kSlotF + i] = F[i];
+        s.slot[q][kSlotW] = w;
+        s.slot[q][kSlotE] = r.energy;
+        s.slot[q][kSlotFl] = w * mmax * hmax * (1.0 + hmax);
+      }
+    }
+  }
+  // The failure of the group: the first point of the earliest stage.
+  int key = fail ? fail : 0x7fffffff;
+#pragma unroll
+  for (int o = G / 2; o >= 1; o >>= 1) key = min(key, __shfl_xor_sync(c.mask, key, o, G));
+  if (key != 0x7fffffff) {
+    const int owner = key & 0xff;
+    const int out = __shfl_sync(c.mask, code, owner, G);
+    c.sync();
+    return out;
+  }
+  // K_aa: w ba^T (D ba) + geometric, streamed through the reduce-scatter in
+  // chunks of G (row-major 9 x 9).
+  const bool live = active;
+  double Mba[6][9];
+  if (live) {
+#pragma unroll
+    for (int col = 0; col < 9; ++col) {
+      const int m = col / 3, k = col % 3;
+      const double g[3] = {gt[0 * 3 + m], gt[1 * 3 + m], gt[2 * 3 + m]};
+      double b[6];
+      bcol(F, g, k, b);
+#pragma unroll
+      for (int r = 0; r < 6; ++r) {
+        double v = 0.0;
+#pragma unroll
+        for (int d = 0; d < 6; ++d) v += M[r * 6 + d] * b[d];
+        Mba[r][col] = v;
+      }
+    }
+  }
+  double geo[9];
+  if (live && geometric) {
+#pragma unroll
+    for (int m = 0; m < 3; ++m)
+#pragma unroll
+      for (int n = 0; n < 3; ++n) {
+        double v = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) v += gt[i * 3 + m] * S[voigt(i, j)] * gt[j * 3 + n];
+        geo[m * 3 + n] = w * v;
+      }
+  }
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    double bi[6];
+    if (live) {
+      const int m = i / 3, k = i % 3;
+      const double g[3] = {gt[0 * 3 + m], gt[1 * 3 + m], gt[2 * 3 + m]};
+      bcol(F, g, k, bi);
+    }
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      const int idx = i * 9 + j;
+      double v = 0.0;
+      if (live) {
+#pragma unroll
+        for (int r = 0; r < 6; ++r) v += bi[r] * Mba[r][j];
+        v *= w;
+        if (geometric && (i % 3) == (j % 3)) v += geo[(i / 3) * 3 + (j / 3)];
+      }
+      kbuf[idx % G] = v;
+      if (idx % G == G - 1) {
+        const double y = reduce_scatter<G>(kbuf, c.lane, c.mask);
+        s.kaa[(idx / G) * G + c.lane] = y;
+      }
+    }
+  }
+  if (81 % G != 0) {
+#pragma unroll
+    for (int i = 81 % G; i < G; ++i) kbuf[i] = 0.0;
+    const double y = reduce_scatter<G>(kbuf, c.lane, c.mask);
+    s.kaa[(81 / G) * G + c.lane] = y;
+  }
+  c.sync();
+  // The force and the scale sums over the points, in point order: lane a
+  // (a < 8) node a, lanes 0-2 also mode a with its scale and floor sums,
+  // lane 7 the energy.
+  if (c.lane < 8) {
+    const int a = c.lane;
+    double ra[3] = {0, 0, 0}, rm[3] = {0, 0, 0}, sc[3] = {0, 0, 0}, fl[3] = {0, 0, 0}, en = 0.0;
+    for (int qq = 0; qq < p.nq; ++qq) {
+      const double* sl = s.slot[qq];
+      const double* Fq = sl + kSlotF;
+      const double* Sq = sl + kSlotS;
+      const double wq = sl[kSlotW];
+      double FS[9];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          FS[k * 3 + j] = Fq[k * 3 + 0] * Sq[voigt(0, j)] + Fq[k * 3 + 1] * Sq[voigt(1, j)] + Fq[k * 3 + 2] * Sq[voigt(2, j)];
+      double g[3];
+      node_grad(c, qq, a, g);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) ra[k] += wq * (FS[k * 3 + 0] * g[0] + FS[k * 3 + 1] * g[1] + FS[k * 3 + 2] * g[2]);
+      if (a < 3) {
+        double gtq[9];
+        mode_grads(c, qq, gtq);
+        const double gm[3] = {gtq[0 * 3 + a], gtq[1 * 3 + a], gtq[2 * 3 + a]};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          rm[k] += wq * (FS[k * 3 + 0] * gm[0] + FS[k * 3 + 1] * gm[1] + FS[k * 3 + 2] * gm[2]);
+          double b[6];
+          bcol(Fq, gm, k, b);
+          double s1 = 0.0, s2 = 0.0;
+#pragma unroll
+          for (int r = 0; r < 6; ++r) {
+            s1 += fabs(b[r]) * fabs(Sq[r]);
+            s2 += fabs(b[r]);
+          }
+          sc[k] += wq * s1;
+          fl[k] += sl[kSlotFl] * s2;
+        }
+      }
+      if (a == 7) en += wq * sl[kSlotE];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s.r[3 * a + k] = ra[k];
+    if (a < 3) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        s.r[24 + 3 * a + k] = rm[k];
+        s.scale[3 * a + k] = sc[k];
+        s.flo[3 * a + k] = fl[k];
+      }
+    }
+    if (a == 7) s.energy = en;
+  }
+  c.sync();
+  return 0;
+}
+
+// ---- element-level helpers (lane 0, shared memory) ---------------------------
+
+// FullPivLU of a (9x9 row-major) into lu; true if invertible (Eigen's rank test).
+__device__ bool fullpiv_lu9(const double* a, double* lu, int* rowp, int* colp, double* maxpivot_out) {
+  for (int i = 0; i < 81; ++i) lu[i] = a[i];
+  double maxpivot = 0.0;
+  int nonzero = 9;
+  for (int k = 0; k < 9; ++k) {
+    int pr = k, pc = k;
+    double big = -1.0;
+    for (int j = k; j < 9; ++j)
+      for (int i = k; i < 9; ++i) {
+        const double v = fabs(lu[i * 9 + j]);
+        if (v > big) {
+          big = v;
+          pr = i;
+          pc = j;
+        }
+      }
+    if (big == 0.0) {
+      nonzero = k;
+      for (int i = k; i < 9; ++i) rowp[i] = colp[i] = i;
+      break;
+    }
+    if (big > maxpivot) maxpivot = big;
+    rowp[k] = pr;
+    colp[k] = pc;
+    if (pr != k)
+      for (int j = 0; j < 9; ++j) {
+        const double t = lu[k * 9 + j];
+        lu[k * 9 + j] = lu[pr * 9 + j];
+        lu[pr * 9 + j] = t;
+      }
+    if (pc != k)
+      for (int i = 0; i < 9; ++i) {
+        const double t = lu[i * 9 + k];
+        lu[i * 9 + k] = lu[i * 9 + pc];
+        lu[i * 9 + pc] = t;
+      }
+    const double inv = 1.0 / lu[k * 9 + k];
+    for (int i = k + 1; i < 9; ++i) lu[i * 9 + k] *= inv;
+    for (int i = k + 1; i < 9; ++i) {
+      const double l = lu[i * 9 + k];
+      for (int j = k + 1; j < 9; ++j) lu[i * 9 + j] -= l * lu[k * 9 + j];
+    }
+  }
+  *maxpivot_out = maxpivot;
+  if (nonzero < 9) return false;
+  const double threshold = kEps * 9.0 * maxpivot;
+  for (int i = 0; i < 9; ++i)
+    if (!(fabs(lu[i * 9 + i]) > threshold)) return false;
+  return true;
+}
+
+// x = A^-1 b with the FullPivLU factors (any lane; b and x may alias).
+__device__ __forceinline__ void fullpiv_solve9(const double* lu, const int* rowp, const int* colp, const double* b,
+                                               double* x) {
+  double y[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) y[i] = b[i];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const int pk = rowp[k];
+#pragma unroll
+    for (int i = k + 1; i < 9; ++i) {
+      if (i == pk) {
+        const double t = y[k];
+        y[k] = y[i];
+        y[i] = t;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 1; i < 9; ++i)
+#pragma unroll
+    for (int j = 0; j < i; ++j) y[i] -= lu[i * 9 + j] * y[j];
+#pragma unroll
+  for (int i = 8; i >= 0; --i) {
+#pragma unroll
+    for (int j = i + 1; j < 9; ++j) y[i] -= lu[i * 9 + j] * y[j];
+    y[i] /= lu[i * 9 + i];
+  }
+#pragma unroll
+  for (int k = 8; k >= 0; --k) {
+    const int pk = colp[k];
+#pragma unroll
+    for (int i = k + 1; i < 9; ++i) {
+      if (i == pk) {
+        const double t = y[k];
+        y[k] = y[i];
+        y[i] = t;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 9; ++i) x[i] = y[i];
+}
+
+// Cholesky (lower, in place); false at the first non-positive pivot.
+__device__ bool llt9(double* a) {
+  for (int k = 0; k < 9; ++k) {
+    double x = a[k * 9 + k];
+    for (int j = 0; j < k; ++j) x -= a[k * 9 + j] * a[k * 9 + j];
+    if (x <= 0.0) return false;
+    a[k * 9 + k] = sqrt(x);
+    for (int i = k + 1; i < 9; ++i) {
+      double v = a[i * 9 + k];
+      for (int j = 0; j < k; ++j) v -= a[i * 9 + j] * a[k * 9 + j];
+      a[i * 9 + k] = v / a[k * 9 + k];
+    }
+  }
+  return true;
+}
+__device__ void llt9_solve(const double* l, const double* b, double* x) {
+  double y[9];
+  for (int i = 0; i < 9; ++i) {
+    double v = b[i];
+    for (int j = 0; j < i; ++j) v -= l[i * 9 + j] * y[j];
+    y[i] = v / l[i * 9 + i];
+  }
+  for (int i = 8; i >= 0; --i) {
+    double v = y[i];
+    for (int j = i + 1; j < 9; ++j) v -= l[j * 9 + i] * y[j];
+    y[i] = v / l[i * 9 + i];
+  }
+  for (int i = 0; i < 9; ++i) x[i] = y[i];
+}
+
+// Smallest eigenvalue and largest |eigenvalue| of a symmetric 9x9 (cyclic
+// Jacobi on a copy in `a`, destroyed).
+__device__ void sym_eig9(double* a, double* lo, double* top) {
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0.0, diag = 0.0;
+    for (int p = 0; p < 9; ++p) {
+      diag += a[p * 9 + p] * a[p * 9 + p];
+      for (int q = p + 1; q < 9; ++q) off += a[p * 9 + q] * a[p * 9 + q];
+    }
+    if (off == 0.0 || off <= 1.0e-36 * diag) break;
+    for (int p = 0; p < 8; ++p)
+      for (int q = p + 1; q < 9; ++q) {
+        const double apq = a[p * 9 + q];
+        if (apq == 0.0) continue;
+        const double theta = (a[q * 9 + q] - a[p * 9 + p]) / (2.0 * apq);
+        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+        const double cs = 1.0 / sqrt(t * t + 1.0);
+        const double sn = t * cs;
+        for (int k = 0; k < 9; ++k) {
+          const double akp = a[k * 9 + p], akq = a[k * 9 + q];
+          a[k * 9 + p] = cs * akp - sn * akq;
+          a[k * 9 + q] = sn * akp + cs * akq;
+        }
+        for (int k = 0; k < 9; ++k) {
+          const double apk = a[p * 9 + k], aqk = a[q * 9 + k];
+          a[p * 9 + k] = cs * apk - sn * aqk;
+          a[q * 9 + k] = sn * apk + cs * aqk;
+        }
+      }
+  }
+  double mn = a[0], mx = fabs(a[0]);
+  for (int i = 1; i < 9; ++i) {
+    mn = fmin(mn, a[i * 9 + i]);
+    mx = fmax(mx, fabs(a[i * 9 + i]));
+  }
+  *lo = mn;
+  *top = mx;
+}
+
+// Partial-pivoting LU solve of a 9x9 (in place), x = A^-1 b.
+__device__ void plu9_solve(double* a, int* perm, const double* b, double* x) {
+  for (int k = 0; k < 9; ++k) {
+    int p = k;
+    double big = fabs(a[k * 9 + k]);
+    for (int i = k + 1; i < 9; ++i)
+      if (fabs(a[i * 9 + k]) > big) {
+        big = fabs(a[i * 9 + k]);
+        p = i;
+      }
+    perm[k] = p;
+    if (big != 0.0) {
+      if (p != k)
+        for (int j = 0; j < 9; ++j) {
+          const double t = a[k * 9 + j];
+          a[k * 9 + j] = a[p * 9 + j];
+          a[p * 9 + j] = t;
+        }
+      const double inv = 1.0 / a[k * 9 + k];
+      for (int i = k + 1; i < 9; ++i) a[i * 9 + k] *= inv;
+    }
+    for (int i = k + 1; i < 9; ++i)
+      for (int j = k + 1; j < 9; ++j) a[i * 9 + j] -= a[i * 9 + k] * a[k * 9 + j];
+  }
+  double y[9];
+  for (int i = 0; i < 9; ++i) y[i] = b[i];
+  for (int k = 0; k < 9; ++k)
+    if (perm[k] != k) {
+      const double t = y[k];
+      y[k] = y[perm[k]];
+      y[perm[k]] = t;
+    }
+  for (int i = 1; i < 9; ++i)
+    for (int j = 0; j < i; ++j) y[i] -= a[i * 9 + j] * y[j];
+  for (int i = 8; i >= 0; --i) {
+    for (int j = i + 1; j < 9; ++j) y[i] -= a[i * 9 + j] * y[j];
+    y[i] /= a[i * 9 + i];
+  }
+  for (int i = 0; i < 9; ++i) x[i] = y[i];
+}
+
+// ---- the local iteration -------------------------------------------------------
+
+template <int G>
+struct Local {
+  const Ctx<G>& c;
+  ElemShared<G>& s;
+  double residual;
+  int iterations;
+  __device__ Local(const Ctx<G>& cc) : c(cc), s(*cc.s), residual(0.0), iterations(0) {}
+
+  __device__ double rnorm() const {
+    double v = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) v += s.r[24 + i] * s.r[24 + i];
+    return sqrt(v);
+  }
+  __device__ double rinf() const {
+    double v = fabs(s.r[24]);
+#pragma unroll
+    for (int i = 1; i < 9; ++i) v = fmax(v, fabs(s.r[24 + i]));
+    return v;
+  }
+  __device__ double vmax(const double* v) const {
+    double m = fabs(v[0]);
+#pragma unroll
+    for (int i = 1; i < 9; ++i) m = fmax(m, fabs(v[i]));
+    return m;
+  }
+  __device__ double ddot(const double* a, const double* b) const {
+    double v = 0.0;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) v += a[i] * b[i];
+    return v;
+  }
+  // A pass at alpha + t d; true if every point evaluated.
+  __device__ bool try_at(const double* d, double t) {
+    double at[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) at[i] = s.alpha[i] + t * d[i];
+    return pass<G>(c, at) == 0;
+  }
+  __device__ void advance(const double* d, double t) {
+    c.sync();
+    if (c.lane == 0)
+#pragma unroll
+      for (int i = 0; i < 9; ++i) s.alpha[i] += t * d[i];
+    c.sync();
+  }
+
+  // search_norm (IncompatibleModes.cpp:359-383).
+  __device__ __noinline__ bool search_norm(const double* d, double reach) {
+    double best_step = 0.0, best = residual;
+    bool last_is_best = false;
+    double trial_step = reach;
+    for (int search = 0; search < kMaxLineSearch; ++search, trial_step *= 0.5) {
+      if (!try_at(d, trial_step)) {
+        last_is_best = false;
+        continue;
+      }
+      const double n = rnorm();
+      last_is_best = n < best;
+      if (last_is_best) {
+        best = n;
+        best_step = trial_step;
+      }
+      if (n <= kFullStepReduction * residual) break;
+    }
+    if (best_step == 0.0) return false;
+    if (!last_is_best) try_at(d, best_step);
+    advance(d, best_step);
+    residual = best;
+    return true;
+  }
+
+  // line_search (IncompatibleModes.cpp:398-456).
+  __device__ __noinline__ bool line_search(const double* d) {
+    const double phi0 = ddot(d, s.r0);
+    double reach = 1.0;
+    bool evaluated = try_at(d, 1.0);
+    for (int halving = 0; !evaluated && halving < kMaxLineSearch; ++halving) {
+      reach *= 0.5;
+      evaluated = try_at(d, reach);
+    }
+    if (!evaluated) return false;
+    const double full = rnorm();
+    if (full <= kFullStepReduction * residual ||
+        rinf() <= kLocalTolerance * vmax(s.scale) + kLocalRoundOff * vmax(s.flo)) {
+      advance(d, reach);
+      residual = full;
+      return true;
+    }
+    const double phi1 = ddot(d, s.r + 24);
+    if (!(phi0 < 0.0) || !(phi1 > 0.0) || !isfinite(phi1)) return search_norm(d, 0.5 * reach);
+    double s0 = 0.0, f0 = phi0, s1 = reach, f1 = phi1, step = reach;
+    int side = 0;
+    for (int search = 0; search < kMaxLineSearch; ++search) {
+      const double width = s1 - s0;
+      step = fmin(fmax((s0 * f1 - s1 * f0) / (f1 - f0), s0 + 0.1 * width), s1 - 0.1 * width);
+      evaluated = try_at(d, step);
+      const double f = evaluated ? ddot(d, s.r + 24) : __longlong_as_double(0x7ff0000000000000LL);
+      if (evaluated && fabs(f) <= kLineSearchRatio * fabs(phi0)) break;
+      if (!evaluated || f > 0.0) {
+        s1 = step;
+        f1 = evaluated ? f : 0.5 * f1;
+        if (side == 1) f0 *= 0.5;
+        side = 1;
+      } else {
+        s0 = step;
+        f0 = f;
+        if (side == -1) f1 *= 0.5;
+        side = -1;
+      }
+    }
+    if (!evaluated) {
+      if (s0 == 0.0) return false;
+      step = s0;
+      try_at(d, step);
+    }
+    advance(d, step);
+    residual = rnorm();
+    return true;
+  }
+
+  // solve_and_condense's loop (IncompatibleModes.cpp:353-546). Returns 0 or
+  // a failure code; on success the last pass is at s.alpha and s.lu holds
+  // the factors of its K_aa.
+  __device__ __noinline__ int run() {
+    {
+      double at[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) at[i] = s.alpha[i];
+      const int code = pass<G>(c, at);
+      if (code) return code;
+    }
+    residual = rnorm();
+    for (;;) {
+      const double largest = rinf();
+      const double scale = vmax(s.scale);
+      const double floor_ = kLocalRoundOff * vmax(s.flo);
+      if (c.lane == 0) {
+        s.ival[0] = fullpiv_lu9(s.kaa, s.lu, s.rowp, s.colp, &s.maxpivot) ? 1 : 0;
+        // k0 and r0 copies (the trial passes overwrite the sums).
+        for (int i = 0; i < 81; ++i) s.work[i] = s.kaa[i];
+        for (int i = 0; i < 9; ++i) s.r0[i] = s.r[24 + i];
+      }
+      c.sync();
+      if (!s.ival[0]) return SBK_EL_LOCAL_SINGULAR;
+      if (largest <= kLocalTolerance * scale + floor_ || largest == 0.0) return 0;
+      if (iterations == kMaxLocal || !isfinite(largest)) return SBK_EL_LOCAL_NO_CONVERGE;
+      ++iterations;
+      // Newton's direction and the Cholesky test of the symmetric part.
+      if (c.lane == 0) {
+        double nw[9];
+        fullpiv_solve9(s.lu, s.rowp, s.colp, s.r0, nw);
+        for (int i = 0; i < 9; ++i) s.dir[i] = -nw[i];
+        double* sym = s.work + 81;
+        for (int i = 0; i < 9; ++i)
+          for (int j = 0; j < 9; ++j) sym[i * 9 + j] = 0.5 * (s.work[i * 9 + j] + s.work[j * 9 + i]);
+        double* chol = s.work + 162;
+        for (int i = 0; i < 81; ++i) chol[i] = sym[i];
+        s.ival[1] = llt9(chol) ? 1 : 0;
+      }
+      c.sync();
+      if (s.ival[1]) {
+        if (line_search(s.dir)) continue;
+      } else {
+        if (try_at(s.dir, 1.0)) {
+          const double full = rnorm();
+          if (full <= kFullStepReduction * residual) {
+            advance(s.dir, 1.0);
+            residual = full;
+            continue;
+          }
+        }
+        if (c.lane == 0) {
+          // The shifted direction (K_aa + mu I) d = -r_alpha.
+          double* sym = s.work + 81;
+          double* tmp = s.work + 162;
+          for (int i = 0; i < 81; ++i) tmp[i] = sym[i];
+          double lo, top;
+          sym_eig9(tmp, &lo, &top);
+          const double mu = kLocalShift * top - lo;
+          for (int i = 0; i < 81; ++i) tmp[i] = s.work[i];
+          for (int i = 0; i < 9; ++i) tmp[i * 9 + i] += mu;
+          double x[9];
+          plu9_solve(tmp, s.perm, s.r0, x);
+          for (int i = 0; i < 9; ++i) s.dir2[i] = -x[i];
+        }
+        c.sync();
+        if (line_search(s.dir2)) continue;
+        if (search_norm(s.dir, 0.5)) continue;
+      }
+      // Levenberg-Marquardt (IncompatibleModes.cpp:522-545).
+      double mu = 0.0;
+      if (c.lane == 0) {
+        double* normal = s.work + 81;
+        for (int i = 0; i < 9; ++i)
+          for (int j = 0; j < 9; ++j) {
+            double v = 0.0;
+            for (int k = 0; k < 9; ++k) v += s.work[k * 9 + i] * s.work[k * 9 + j];
+            normal[i * 9 + j] = v;
+          }
+        double dmax = normal[0];
+        for (int i = 1; i < 9; ++i) dmax = fmax(dmax, normal[i * 9 + i]);
+        s.dval[0] = kLocalMarquardt * dmax;
+      }
+      c.sync();
+      mu = s.dval[0];
+      bool moved = false;
+      for (int search = 0; search < kMaxLineSearch && !moved; ++search, mu *= 10.0) {
+        c.sync();
+        if (c.lane == 0) {
+          double* normal = s.work + 81;
+          double* a = s.work + 162;
+          for (int i = 0; i < 81; ++i) a[i] = normal[i];
+          for (int i = 0; i < 9; ++i) a[i * 9 + i] += mu;
+          double grad[9];
+          for (int i = 0; i < 9; ++i) {
+            double v = 0.0;
+            for (int j = 0; j < 9; ++j) v += s.work[j * 9 + i] * s.r0[j];
+            grad[i] = v;
+          }
+          const bool ok = llt9(a);
+          s.ival[2] = ok ? 1 : 0;
+          if (ok) {
+            double x[9];
+            llt9_solve(a, grad, x);
+            for (int i = 0; i < 9; ++i) s.dir2[i] = -x[i];
+          }
+        }
+        c.sync();
+        if (!s.ival[2]) continue;
+        if (!try_at(s.dir2, 1.0)) continue;
+        const double n = rnorm();
+        if (n < residual) {
+          advance(s.dir2, 1.0);
+          residual = n;
+          moved = true;
+        }
+      }
+      if (!moved) return SBK_EL_LOCAL_NO_DESCENT;
+    }
+  }
+};
+
+// ---- the condensation ---------------------------------------------------------
+
+template <int G>
+__global__ void __launch_bounds__(128) element_kernel(const Params p, int64_t ne, bool batch,
+                                                      const double* __restrict__ coords,
+                                                      const int32_t* __restrict__ conn, const double* __restrict__ u,
+                                                      const double* __restrict__ state,
+                                                      const double* __restrict__ alpha_n, int want_tangent,
+                                                      double* __restrict__ force, double* __restrict__ tangent,
+                                                      double* __restrict__ energy, double* __restrict__ trial,
+                                                      double* __restrict__ alpha_out, uint8_t* __restrict__ yield,
+                                                      int32_t* __restrict__ iterations, int32_t* __restrict__ code,
+                                                      int32_t* __restrict__ first_failure) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int epb = blockDim.x / G;
+  const int slot_in_block = threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  const int64_t e = (int64_t)blockIdx.x * epb + slot_in_block;
+  ElemShared<G>* sh = reinterpret_cast<ElemShared<G>*>(smem_raw) + slot_in_block;
+  const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+  const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
+  if (e >= ne) return;  // whole groups leave together
+  Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, trial, yield};
+  ElemShared<G>& s = *sh;
+  // Stage the element's coordinates and displacements (lane a: node a).
+  if (lane < 8) {
+    if (batch) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        s.X[3 * lane + k] = coords[e * 24 + 3 * lane + k];
+        s.U[3 * lane + k] = u[e * 24 + 3 * lane + k];
+      }
+    } else {
+      const int64_t node = conn[e * 8 + lane];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        s.X[3 * lane + k] = coords[node * 3 + k];
+        s.U[3 * lane + k] = u[node * 3 + k];
+      }
+    }
+  }
+  for (int i = lane; i < 9; i += G) s.alpha[i] = alpha_n ? alpha_n[e * 9 + i] : 0.0;
+  c.sync();
+  int status = set_up<G>(c);
+  Local<G> loc(c);
+  if (!status) status = loc.run();
+  if (status) {
+    if (lane == 0) {
+      code[e] = status;
+      if (first_failure) atomicMin(first_failure, (int32_t)e);
+    }
+    return;
+  }
+  const bool sym = p.symmetric != 0;
+  const bool geometric = p.kinematics != SBK_SMALL_STRAIN;
+  const int nq = p.nq;
+  // K_ua rows of node a (and K_au columns for a non-symmetric tangent).
+  double kua[3][9], kau[3][9];
+  if (lane < 8) {
+    const int a = lane;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int j = 0; j < 9; ++j) kua[k][j] = kau[k][j] = 0.0;
+    for (int q = 0; q < nq; ++q) {
+      double g[3], gt[9], V[27];
+      node_grad(c, q, a, g);
+      mode_grads(c, q, gt);
+      vtensor(s.slot[q], g, false, geometric, V);
+#pragma unroll
+      for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int l = 0; l < 3; ++l)
+            kua[k][3 * m + l] += V[(k * 3 + l) * 3 + 0] * gt[0 * 3 + m] + V[(k * 3 + l) * 3 + 1] * gt[1 * 3 + m] +
+                                 V[(k * 3 + l) * 3 + 2] * gt[2 * 3 + m];
+      if (!sym) {
+        vtensor(s.slot[q], g, true, geometric, V);
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+          for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int l = 0; l < 3; ++l)
+              kau[k][3 * m + l] += V[(k * 3 + l) * 3 + 0] * gt[0 * 3 + m] + V[(k * 3 + l) * 3 + 1] * gt[1 * 3 + m] +
+                                   V[(k * 3 + l) * 3 + 2] * gt[2 * 3 + m];
+      }
+    }
+    // The coupling C = K_aa^-1 K_au, columns of node a, into shared memory
+    // (K_au(3m+l, 3a+k) = kau[k][3m+l], or kua[k][3m+l] when symmetric).
+    double* C = s.work;  // 9 x 24, column-major by DOF: C[col * 9 + i]
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double b[9];
+#pragma unroll
+      for (int j = 0; j < 9; ++j) b[j] = sym ? kua[k][j] : kau[k][j];
+      double x[9];
+      fullpiv_solve9(s.lu, s.rowp, s.colp, b, x);
+#pragma unroll
+      for (int j = 0; j < 9; ++j) C[(3 * a + k) * 9 + j] = x[j];
+    }
+  }
+  c.sync();
+  if (lane < 8) {
+    const int a = lane;
+    // f* = f_u - K_ua K_aa^-1 r_alpha.
+    double corr[9];
+    fullpiv_solve9(s.lu, s.rowp, s.colp, s.r + 24, corr);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double v = 0.0;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) v += kua[k][j] * corr[j];
+      force[e * 24 + 3 * a + k] = s.r[3 * a + k] - v;
+    }
+    if (want_tangent) {
+      const double* C = s.work;
+#pragma unroll
+      for (int chunk = 0; chunk < 2; ++chunk) {
+        double acc[4][9];
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+          for (int i = 0; i < 9; ++i) acc[b][i] = 0.0;
+        for (int q = 0; q < nq; ++q) {
+          double g[3], V[27];
+          node_grad(c, q, a, g);
+          vtensor(s.slot[q], g, false, geometric, V);
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            double gb[3];
+            node_grad(c, q, chunk * 4 + b, gb);
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+#pragma unroll
+              for (int l = 0; l < 3; ++l)
+                acc[b][k * 3 + l] += V[(k * 3 + l) * 3 + 0] * gb[0] + V[(k * 3 + l) * 3 + 1] * gb[1] +
+                                     V[(k * 3 + l) * 3 + 2] * gb[2];
+          }
+        }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int bb = chunk * 4 + b;
+          double* out = tangent + e * 576 + (8 * a + bb) * 9;
+#pragma unroll
+          for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+              double v = acc[b][k * 3 + l];
+#pragma unroll
+              for (int m = 0; m < 9; ++m) v -= kua[k][m] * C[(3 * bb + l) * 9 + m];
+              out[k * 3 + l] = v;
+            }
+        }
+      }
+    }
+  }
+  if (want_tangent && sym) {
+    // K* = (K* + K*^T) / 2: the unordered pair {(i, j), (j, i)} by the lane
+    // that owns row min(i, j).
+    __threadfence_block();
+    c.sync();
+    if (lane < 8) {
+      double* Ke = tangent + e * 576;
+      auto at = [&](int i, int j) -> double* { return Ke + (8 * (i / 3) + j / 3) * 9 + 3 * (i % 3) + (j % 3); };
+      for (int k = 0; k < 3; ++k) {
+        const int i = 3 * lane + k;
+        for (int j = i + 1; j < 24; ++j) {
+          double* x = at(i, j);
+          double* y = at(j, i);
+          const double v = 0.5 * (*x + *y);
+          *x = v;
+          *y = v;
+        }
+      }
+    }
+  }
+  if (lane == 0) {
+    energy[e] = s.energy;
+    iterations[e] = loc.iterations;
+    code[e] = 0;
+  }
+  for (int i = lane; i < 9; i += G) alpha_out[e * 9 + i] = s.alpha[i];
+}
+
+template <int G>
+int launch_g(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
+             const double* state, const double* alpha_n, int want_tangent, double* force, double* tangent,
+             double* energy, double* trial, double* alpha_out, uint8_t* yield, int32_t* iterations, int32_t* code,
+             int32_t* first_failure, bool batch, int epb, cudaStream_t stream) {
+  const int threads = epb * G;
+  const size_t smem = sizeof(ElemShared<G>) * epb;
+  const int64_t blocks = (ne + epb - 1) / epb;
+  if (blocks == 0) return 0;
+  auto kern = element_kernel<G>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return (int)err;
+  kern<<<(unsigned)blocks, threads, smem, stream>>>(p, ne, batch, coords, conn, u, state, alpha_n, want_tangent,
+                                                     force, tangent, energy, trial, alpha_out, yield, iterations,
+                                                     code, first_failure);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace
+
+size_t element_smem_bytes(int group) {
+  if (group == 8) return sizeof(ElemShared<8>);
+#ifdef SBK_WIDE_RULES
+  return sizeof(ElemShared<32>);
+#else
+  return 0;
+#endif
+}
+
+int launch_elements(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
+                    const double* state, const double* alpha_n, int want_tangent, double* force, double* tangent,
+                    double* energy, double* trial, double* alpha_out, uint8_t* yield, int32_t* iterations,
+                    int32_t* code, int32_t* first_failure, bool batch, int elements_per_block,
+                    cudaStream_t stream) {
+  if (p.nq <= 8) {
+    const int epb = elements_per_block > 0 ? elements_per_block : 4;
+    return launch_g<8>(p, ne, coords, conn, u, state, alpha_n, want_tangent, force, tangent, energy, trial,
+                       alpha_out, yield, iterations, code, first_failure, batch, epb, stream);
+  }
+#ifdef SBK_WIDE_RULES
+  const int epb = elements_per_block > 0 ? elements_per_block : 1;
+  return launch_g<32>(p, ne, coords, conn, u, state, alpha_n, want_tangent, force, tangent, energy, trial,
+                      alpha_out, yield, iterations, code, first_failure, batch, epb, stream);
+#else
+  return -1;  // rules of more than 8 points: not in this build
+#endif
+}
+
+}  // namespace sbk

@@ -1,0 +1,56 @@
+// Kernel launchers of the element loop (K1), the assembly (K2) and the
+// contact (K3), called by the C ABI in sbk_capi.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "sbk_params.h"
+
+namespace sbk {
+
+// Records the message sbk_last_error returns; returns `code`.
+int set_error(int code, const std::string& what);
+
+// K1: ne elements. Mesh mode (batch = false): coords 3 per node, conn 8 per
+// element, u 3 per node. Batch mode: coords and u hold 24 per element.
+int launch_elements(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
+                    const double* state, const double* alpha_n, int want_tangent, double* force, double* tangent,
+                    double* energy, double* trial, double* alpha_out, uint8_t* yield, int32_t* iterations,
+                    int32_t* code, int32_t* first_failure, bool batch, int elements_per_block,
+                    cudaStream_t stream);
+size_t element_smem_bytes(int group);
+
+// The gather maps of the assembly (built once on the host).
+struct GatherMaps {
+  int64_t num_nodes, num_elements, nnz, num_blocks;
+  // Node blocks of the pattern in CSC order (column node B, its sorted
+  // neighbours A): the block's first value index in column 3B (the rows of
+  // the same block in columns 3B+1, 3B+2 follow at +col_stride[B]).
+  const int32_t* block_col;     // num_blocks: column node B
+  const int64_t* block_value;   // num_blocks: index of value (3A, 3B)
+  const int32_t* block_ptr;     // num_blocks + 1: contributions of each block
+  const int32_t* block_src;     // e * 64 + a * 8 + b, ascending e per block
+  const int32_t* outer;         // CSC column pointers (3 nn + 1)
+  // Node incidences (node -> e * 8 + a, ascending e) for f_int and gross.
+  const int32_t* node_ptr;      // nn + 1
+  const int32_t* node_src;      // 8 ne
+};
+
+// K2: values (nnz) from the element tangents, in element order per entry.
+int launch_assemble_values(const GatherMaps& m, const double* tangent, double* values, cudaStream_t stream);
+// K2: f_int and the per-DOF gross sums from the element forces; the partial
+// sums of energy, gross^2 and the yield count into `scalars`
+// (double[3]: energy, gross^2, yielding).
+int launch_assemble_forces(const GatherMaps& m, const double* force, const double* energy_e,
+                           const uint8_t* yield, int nq, double* internal, double* scratch, double* scalars,
+                           cudaStream_t stream);
+size_t assemble_scratch_doubles();
+// add_node_block for n blocks, in list order.
+int launch_add_node_blocks(const int32_t* outer, const int32_t* inner, double* values, int32_t n,
+                           const int32_t* nodes, const double* blocks, int32_t* missing, cudaStream_t stream);
+
+}  // namespace sbk

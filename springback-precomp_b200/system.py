@@ -1,0 +1,256 @@
+"""The element loop behind the reference's own interfaces.
+
+`NonlinearSystem` mirrors detail::NonlinearSystem
+(src/fem/NonlinearSystem.hpp:85-334): evaluate(u, lambda, want_tangent)
+returns an `Evaluation` (f_int, residual, the tangent in the Assembler's CSC
+pattern, energy, gross, yield count, trial states and modes), commit() makes
+the trial history the committed one, committed_all / set_committed and
+internal_all / set_internal carry a restart. A failing element raises
+`SolverError`, as the reference's SolverError does.
+
+`element_batch` is incompatible_elastoplastic_element
+(src/fem/IncompatibleModes.cpp:577-600) over a batch of independent
+elements.
+
+Everything runs in libsbk.so on the GPU; device buffers are torch tensors.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _capi
+from .material import Material, rule_c, rule_size
+from .mesh import HexMesh
+
+
+class _DeviceView:
+    """A zero-copy torch view of library-owned device memory."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr, "data": (int(ptr), False),
+                                         "version": 2, "strides": None, "stream": None}
+
+
+def device_view(ptr: int, shape, dtype=torch.float64) -> torch.Tensor:
+    typestr = {torch.float64: "<f8", torch.int32: "<i4", torch.uint8: "|u1"}[dtype]
+    if int(np.prod(shape)) == 0 or not ptr:
+        return torch.empty(shape, dtype=dtype, device="cuda")
+    return torch.as_tensor(_DeviceView(ptr, shape, typestr), device="cuda")
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    if t is None:
+        return None
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("device buffers must be contiguous CUDA tensors")
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _stream_ptr(stream) -> ctypes.c_void_p:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+@dataclasses.dataclass
+class ElementBatchResult:
+    force: torch.Tensor       # (ne, 24)
+    tangent: Optional[torch.Tensor]  # (ne, 64, 3, 3) node blocks (a, b)
+    energy: torch.Tensor      # (ne,)
+    states: torch.Tensor      # (nfields, ne, nq)
+    alpha: torch.Tensor       # (ne, 9)
+    yielding: torch.Tensor    # (ne, nq) uint8
+    iterations: torch.Tensor  # (ne,) int32
+    code: torch.Tensor        # (ne,) int32
+
+    def dense_tangent(self) -> torch.Tensor:
+        """(ne, 24, 24) from the node-block layout."""
+        t = self.tangent.view(-1, 8, 8, 3, 3).permute(0, 1, 3, 2, 4)
+        return t.reshape(-1, 24, 24)
+
+
+def element_batch(material: Material, x: torch.Tensor, u: torch.Tensor, state: Optional[torch.Tensor] = None,
+                  alpha: Optional[torch.Tensor] = None, kinematics: str = "logarithmic", stiffness_points: int = 2,
+                  thickness_points: int = 0, thickness_axis: int = 2, want_tangent: bool = True,
+                  stream=None) -> ElementBatchResult:
+    """Evaluate independent IM Hex8 elements on the GPU. x, u: (ne, 24)
+    float64 CUDA tensors; state: (nfields, ne, nq) committed points (None:
+    virgin); alpha: (ne, 9) committed modes (None: zero)."""
+    ne = int(x.shape[0])
+    nq = rule_size(stiffness_points, thickness_points, thickness_axis)
+    if nq == 0:
+        raise _capi.SbkError(2, "invalid integration rule")
+    nf = material.state_fields
+    dev = x.device
+    f64 = dict(dtype=torch.float64, device=dev)
+    if state is None:
+        state = torch.zeros((nf, ne, nq), **f64)
+    out = ElementBatchResult(
+        force=torch.empty((ne, 24), **f64),
+        tangent=torch.empty((ne, 64, 3, 3), **f64) if want_tangent else None,
+        energy=torch.empty((ne,), **f64),
+        states=torch.empty((nf, ne, nq), **f64),
+        alpha=torch.empty((ne, 9), **f64),
+        yielding=torch.zeros((ne, nq), dtype=torch.uint8, device=dev),
+        iterations=torch.zeros((ne,), dtype=torch.int32, device=dev),
+        code=torch.zeros((ne,), dtype=torch.int32, device=dev),
+    )
+    mat = material.to_c()
+    rule = rule_c(stiffness_points, thickness_points, thickness_axis)
+    st = _capi.lib().sbk_element_batch(ctypes.byref(mat), ctypes.byref(rule), _capi.KINEMATICS[kinematics], ne,
+                                       _ptr(x.contiguous()), _ptr(u.contiguous()), _ptr(state.contiguous()),
+                                       _ptr(alpha.contiguous()) if alpha is not None else None, _ptr(out.force),
+                                       _ptr(out.tangent) if want_tangent else None, _ptr(out.energy),
+                                       _ptr(out.states), _ptr(out.alpha), _ptr(out.yielding), _ptr(out.iterations),
+                                       _ptr(out.code), _stream_ptr(stream))
+    _capi.check(st)
+    return out
+
+
+@dataclasses.dataclass
+class Evaluation:
+    """NonlinearSystem.hpp:27-47. Tensors are views of the system's buffers,
+    valid until its next evaluate (clone to keep them)."""
+
+    internal: torch.Tensor
+    residual: torch.Tensor
+    tangent: Optional[torch.Tensor]  # CSC values in the pattern
+    energy: float
+    gross: float
+    yielding_points: int
+    system: "NonlinearSystem"
+
+    @property
+    def states(self) -> np.ndarray:
+        return self.system.trial_states()
+
+    @property
+    def modes(self) -> np.ndarray:
+        return self.system.trial_modes()
+
+
+class NonlinearSystem:
+    def __init__(self, mesh: HexMesh, material: Material, kinematics: str = "logarithmic", stiffness_points: int = 2,
+                 thickness_points: int = 0, thickness_axis: int = 2, stream=None):
+        self.mesh = mesh
+        self.material = material
+        self.kinematics = kinematics
+        self.nq = rule_size(stiffness_points, thickness_points, thickness_axis)
+        self.nfields = material.state_fields
+        self._coords = np.ascontiguousarray(mesh.coords, dtype=np.float64)
+        self._conn = np.ascontiguousarray(mesh.connectivity, dtype=np.int32)
+        m = _capi.sbk_mesh()
+        m.num_nodes = mesh.num_nodes
+        m.num_elements = mesh.num_elements
+        m.coords = self._coords.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        m.connectivity = self._conn.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        self._mat = material.to_c()
+        self._rule = rule_c(stiffness_points, thickness_points, thickness_axis)
+        h = ctypes.c_void_p()
+        _capi.check(_capi.lib().sbk_system_create(ctypes.byref(m), ctypes.byref(self._mat), ctypes.byref(self._rule),
+                                                  _capi.KINEMATICS[kinematics], ctypes.byref(h)))
+        self._h = h
+        self.set_stream(stream)
+        pat = _capi.sbk_pattern()
+        _capi.check(_capi.lib().sbk_system_pattern(self._h, ctypes.byref(pat)))
+        self.num_dofs = int(pat.num_dofs)
+        self.nnz = int(pat.nnz)
+        self.outer = device_view(pat.outer_dev, (self.num_dofs + 1,), torch.int32)
+        self.inner = device_view(pat.inner_dev, (self.nnz,), torch.int32)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _capi.lib().sbk_system_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream=None):
+        _capi.check(_capi.lib().sbk_system_set_stream(self._h, _stream_ptr(stream)))
+
+    def set_elements_per_block(self, epb: int):
+        _capi.check(_capi.lib().sbk_system_set_elements_per_block(self._h, int(epb)))
+
+    def symmetric(self) -> bool:
+        return bool(_capi.lib().sbk_system_symmetric(self._h))
+
+    def plastic(self) -> bool:
+        return bool(_capi.lib().sbk_system_plastic(self._h))
+
+    def evaluate(self, u: torch.Tensor, lam: float = 0.0, want_tangent: bool = True) -> Evaluation:
+        if u.dtype != torch.float64 or u.numel() != self.num_dofs:
+            raise ValueError("u must hold num_dofs float64 values")
+        ev = _capi.sbk_evaluation()
+        st = _capi.lib().sbk_system_evaluate(self._h, _ptr(u.contiguous()), float(lam), int(want_tangent),
+                                             ctypes.byref(ev))
+        if st == 4:
+            raise _capi.SolverError(st, _capi.last_error(), ev.failed_element, ev.failure_code)
+        _capi.check(st)
+        internal = device_view(ev.internal_dev, (self.num_dofs,))
+        values = device_view(ev.values_dev, (self.nnz,)) if want_tangent else None
+        return Evaluation(internal=internal, residual=internal, tangent=values, energy=float(ev.energy),
+                          gross=float(ev.gross), yielding_points=int(ev.yielding_points), system=self)
+
+    def commit(self, ev: Optional[Evaluation] = None):
+        _capi.check(_capi.lib().sbk_system_commit(self._h))
+
+    def _state_shape(self):
+        return (self.nfields, self.mesh.num_elements, self.nq)
+
+    def committed_all(self) -> np.ndarray:
+        out = np.empty(self._state_shape())
+        _capi.check(_capi.lib().sbk_system_get_committed(self._h, out.ctypes.data_as(ctypes.c_void_p), None))
+        return out
+
+    def internal_all(self) -> np.ndarray:
+        out = np.empty((self.mesh.num_elements, 9))
+        _capi.check(_capi.lib().sbk_system_get_committed(self._h, None, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+    def set_committed(self, states: np.ndarray):
+        states = np.ascontiguousarray(states, dtype=np.float64)
+        if states.shape != self._state_shape():
+            raise _capi.SbkError(2, f"the saved plastic history has shape {states.shape}; the system keeps "
+                                    f"{self._state_shape()}")
+        _capi.check(_capi.lib().sbk_system_set_committed(self._h, states.ctypes.data_as(ctypes.c_void_p), None))
+
+    def set_internal(self, alpha: np.ndarray):
+        alpha = np.ascontiguousarray(alpha, dtype=np.float64)
+        if alpha.shape != (self.mesh.num_elements, 9):
+            raise _capi.SbkError(2, "the saved internal-mode history does not match the mesh")
+        _capi.check(_capi.lib().sbk_system_set_committed(self._h, None, alpha.ctypes.data_as(ctypes.c_void_p)))
+
+    def trial_states(self) -> np.ndarray:
+        out = np.empty(self._state_shape())
+        _capi.check(_capi.lib().sbk_system_get_trial(self._h, out.ctypes.data_as(ctypes.c_void_p), None, None))
+        return out
+
+    def trial_modes(self) -> np.ndarray:
+        out = np.empty((self.mesh.num_elements, 9))
+        _capi.check(_capi.lib().sbk_system_get_trial(self._h, None, out.ctypes.data_as(ctypes.c_void_p), None))
+        return out
+
+    def trial_yield(self) -> np.ndarray:
+        out = np.empty((self.mesh.num_elements, self.nq), dtype=np.uint8)
+        _capi.check(_capi.lib().sbk_system_get_trial(self._h, None, None, out.ctypes.data_as(ctypes.c_void_p)))
+        return out
+
+    def max_plastic_strain(self) -> float:
+        st = self.committed_all()
+        return float(st[12 + 6 * self.material.kinematic_terms].max()) if st.size else 0.0
+
+    def add_node_blocks(self, nodes: torch.Tensor, blocks: torch.Tensor):
+        """add_node_block (src/fem/Forming.cpp:280-297) into the tangent of
+        the last evaluate; nodes distinct within one call."""
+        n = int(nodes.numel())
+        _capi.check(_capi.lib().sbk_system_add_node_blocks(self._h, n, _ptr(nodes.to(torch.int32).contiguous()),
+                                                           _ptr(blocks.to(torch.float64).contiguous())))

@@ -1,0 +1,169 @@
+"""Parity of the CUDA element kernel (through the C ABI's sbk_element_batch)
+with the oracle: per-element K_T and R within 1e-11 relative Frobenius,
+per-point yield flags bit-exact, the modes, states, energies and local
+iteration counts alike, on the reference's own test elements
+(tests/test_incompatible_modes.cpp:433-595) and on seeded microbenchmark
+elements."""
+from __future__ import annotations
+
+import importlib
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import X_DISTORTED, deformation, dense_from_blocks, device_to_oracle, oracle_to_device, rel_frobenius
+
+pytestmark = pytest.mark.gpu
+
+TOL_K = 1.0e-11  # relative Frobenius, per element
+TOL_F = 1.0e-11
+
+LAWS = ["elastic", "j2", "hill", "chaboche"]
+KINEMATICS = ["small", "finite", "logarithmic"]
+SCALES = {("small", False): 1e-3, ("small", True): 4e-3, ("finite", False): 0.05, ("finite", True): 0.02,
+          ("logarithmic", False): 0.05, ("logarithmic", True): 0.1}
+
+
+def material(pkg, law):
+    m = pkg.material
+    return {"elastic": m.elastic_steel, "j2": m.j2_steel, "hill": m.hill_sheet, "chaboche": m.chaboche_steel,
+            "hill_chaboche": m.hill_chaboche_sheet, "perfect": m.perfectly_plastic}[law]()
+
+
+def run_gpu(pkg, mat, X, ue, state_dev, alpha, kin, cuda, want_tangent=True):
+    x = torch.tensor(np.asarray(X).reshape(-1, 24), device=cuda)
+    u = torch.tensor(np.asarray(ue).reshape(-1, 24), device=cuda)
+    st = torch.tensor(np.ascontiguousarray(state_dev), device=cuda) if state_dev is not None else None
+    al = torch.tensor(np.asarray(alpha).reshape(-1, 9), device=cuda) if alpha is not None else None
+    r = pkg.element_batch(mat, x, u, st, al, kinematics=kin, want_tangent=want_tangent)
+    torch.cuda.synchronize()
+    return r
+
+
+def compare(ref, r, nterms, want_tangent=True, tol_k=TOL_K, tol_f=TOL_F):
+    np.testing.assert_array_equal(r.code.cpu().numpy(), ref["status"])
+    ok = ref["status"] == 0
+    if not ok.any():
+        return
+    f = r.force.cpu().numpy()[ok]
+    ef = rel_frobenius(f, ref["force"][ok])
+    assert ef.max() <= tol_f, f"force error {ef.max():.3e}"
+    if want_tangent:
+        K = dense_from_blocks(r.tangent.cpu().numpy())[ok]
+        ek = rel_frobenius(K, ref["tangent"][ok])
+        assert ek.max() <= tol_k, f"tangent error {ek.max():.3e}"
+    np.testing.assert_array_equal(r.yielding.cpu().numpy()[ok].astype(bool), ref["yield_flags"][ok])
+    np.testing.assert_array_equal(r.iterations.cpu().numpy()[ok], ref["iterations"][ok])
+    a, ra = r.alpha.cpu().numpy()[ok], ref["alpha"][ok]
+    assert np.abs(a - ra).max() <= 1e-10 * (np.abs(ra).max() + 1e-300)
+    st = device_to_oracle(r.states.cpu().numpy(), nterms)[ok]
+    rs = ref["states"][ok]
+    for lo, hi in [(0, 6), (6, 12), (12, 12 + 6 * nterms), (36, 37)]:
+        if hi > lo:
+            d = np.abs(st[..., lo:hi] - rs[..., lo:hi]).max()
+            assert d <= 1e-10 * (np.abs(rs[..., lo:hi]).max() + 1e-30), (lo, hi, d)
+    np.testing.assert_array_equal(st[..., 38], rs[..., 38])
+    e, re_ = r.energy.cpu().numpy()[ok], ref["energy"][ok]
+    assert np.abs(e - re_).max() <= 1e-11 * (np.abs(re_).max() + 1e-300)
+
+
+@pytest.mark.parametrize("kin", KINEMATICS)
+@pytest.mark.parametrize("law", LAWS)
+def test_two_step_cases(pkg, orc, cuda, law, kin):
+    """The reference's condensed-tangent cases: a committed first step, then
+    the check at a second one (test_incompatible_modes.cpp:433-508, with the
+    2 x 2 x 2 rule)."""
+    mat = material(pkg, law)
+    plastic = mat.yield_stress > 0
+    s = SCALES[(kin, plastic)]
+    X = X_DISTORTED.reshape(1, 24)
+    first = orc.elements(mat.as_dict(), X, deformation(X_DISTORTED, s).reshape(1, 24), kinematics=kin,
+                         want_tangent=False)
+    committed = first["states"] if plastic else np.zeros_like(first["states"])
+    ue = deformation(X_DISTORTED, 1.3 * s)
+    for a in range(8):
+        ue[3 * a + 2] += 0.2 * s * X_DISTORTED[a, 0] * X_DISTORTED[a, 1]
+    ref = orc.elements(mat.as_dict(), X, ue.reshape(1, 24), committed, first["alpha"], kinematics=kin)
+    nt = mat.kinematic_terms
+    r = run_gpu(pkg, mat, X, ue, oracle_to_device(committed, nt), first["alpha"], kin, cuda)
+    compare(ref, r, nt)
+    if plastic:
+        assert int(r.yielding.sum()) == 8
+
+
+@pytest.mark.parametrize("law", ["j2", "chaboche", "hill", "perfect"])
+@pytest.mark.parametrize("factor", [-6.0, -10.0, -15.0])
+def test_reversal(pkg, orc, cuda, law, factor):
+    """A committed plastic step, then a reversal of several times the strain
+    in one increment under logarithmic kinematics
+    (test_incompatible_modes.cpp:510-595): the line searches, the shifted
+    direction and the Levenberg-Marquardt fallback of the local iteration."""
+    mat = material(pkg, law)
+    X = X_DISTORTED.reshape(1, 24)
+    first = orc.elements(mat.as_dict(), X, deformation(X_DISTORTED, 0.02).reshape(1, 24), kinematics="logarithmic",
+                         want_tangent=False)
+    ue = deformation(X_DISTORTED, factor * 0.02)
+    ref = orc.elements(mat.as_dict(), X, ue.reshape(1, 24), first["states"], first["alpha"],
+                       kinematics="logarithmic")
+    nt = mat.kinematic_terms
+    r = run_gpu(pkg, mat, X, ue, oracle_to_device(first["states"], nt), first["alpha"], "logarithmic", cuda)
+    # Long local iterations amplify round-off: the tangent within 1e-9 here.
+    compare(ref, r, nt, tol_k=1e-9, tol_f=1e-9)
+
+
+def test_random_batch(pkg, orc, cuda):
+    """Seeded microbenchmark elements (Hill48 + two-term Chaboche,
+    logarithmic strain, about 40 % of the points yielding)."""
+    wl = importlib.import_module("springback-precomp_b200.workload")
+    prob = wl.make_problem(40, 20, 2, seed=3, sample=512)
+    mesh, mat = prob.mesh, prob.material
+    X = mesh.element_coordinates()
+    ue = mesh.gather(prob.u)
+    nt = mat.kinematic_terms
+    committed = device_to_oracle(prob.state, nt)
+    ref = orc.elements(mat.as_dict(), X, ue, committed, prob.alpha, kinematics="logarithmic")
+    r = run_gpu(pkg, mat, X, ue, prob.state, prob.alpha, "logarithmic", cuda)
+    frac = ref["yield_flags"].mean()
+    assert 0.2 < frac < 0.6, frac
+    compare(ref, r, nt)
+
+
+def test_residual_only_matches(pkg, cuda):
+    """want_tangent = false gives the same force, modes and states."""
+    mat = pkg.material.hill_chaboche_sheet()
+    X = np.tile(X_DISTORTED.reshape(1, 24) * 1e-3, (4, 1))
+    ue = np.stack([deformation(X_DISTORTED * 1e-3, s) for s in (0.01, 0.02, -0.015, 0.03)])
+    a = run_gpu(pkg, mat, X, ue, None, None, "logarithmic", cuda, want_tangent=True)
+    b = run_gpu(pkg, mat, X, ue, None, None, "logarithmic", cuda, want_tangent=False)
+    assert torch.equal(a.force, b.force)
+    assert torch.equal(a.alpha, b.alpha)
+    assert torch.equal(a.states, b.states)
+
+
+def test_failure_codes(pkg, orc, cuda):
+    """An element inverted at rest (MeshError) and one whose deformation
+    inverts a point under logarithmic kinematics (SolverError) report the
+    oracle's codes; the good element beside them is unaffected."""
+    mat = pkg.material.j2_steel()
+    good = X_DISTORTED.reshape(24)
+    bad = X_DISTORTED[[4, 5, 6, 7, 0, 1, 2, 3]].reshape(24)  # top and bottom swapped: det J < 0
+    X = np.stack([good, bad, good])
+    ue = np.stack([deformation(X_DISTORTED, 0.01), np.zeros(24), np.zeros(24)])
+    for a in range(4, 8):
+        ue[2, 3 * a + 2] = -2.5 * X_DISTORTED[a, 2]  # crush the third through itself
+    ref = orc.elements(mat.as_dict(), X, ue, kinematics="logarithmic")
+    r = run_gpu(pkg, mat, X, ue, None, None, "logarithmic", cuda)
+    assert ref["status"][1] == 6 and ref["status"][2] != 0 and ref["status"][0] == 0
+    compare(ref, r, mat.kinematic_terms)
+
+
+def test_deterministic(pkg, cuda):
+    """Two launches give bit-identical results."""
+    mat = pkg.material.hill_chaboche_sheet()
+    rng = np.random.default_rng(0)
+    X = np.tile(X_DISTORTED.reshape(1, 24) * 1e-3, (64, 1))
+    ue = np.stack([deformation(X_DISTORTED * 1e-3, s) for s in rng.uniform(-0.03, 0.03, 64)])
+    a = run_gpu(pkg, mat, X, ue, None, None, "logarithmic", cuda)
+    b = run_gpu(pkg, mat, X, ue, None, None, "logarithmic", cuda)
+    assert torch.equal(a.force, b.force) and torch.equal(a.tangent, b.tangent)

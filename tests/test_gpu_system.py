@@ -1,0 +1,114 @@
+"""The system (NonlinearSystem::evaluate / commit through the C ABI) against
+the oracle's restatement of the reference's element loop, gather and
+element-order scatter (src/fem/NonlinearSystem.hpp:192-268,
+src/fem/Assembler.cpp:86-215)."""
+from __future__ import annotations
+
+import importlib
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import dense_from_blocks, device_to_oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def problem(pkg, cuda):
+    wl = importlib.import_module("springback-precomp_b200.workload")
+    return wl.make_problem(24, 12, 2, seed=11, sample=576)
+
+
+def make_system(pkg, prob):
+    sys_ = pkg.NonlinearSystem(prob.mesh, prob.material, kinematics="logarithmic")
+    sys_.set_committed(prob.state)
+    sys_.set_internal(prob.alpha)
+    return sys_
+
+
+def test_pattern_is_the_reference_pattern(pkg, orc, problem):
+    sys_ = make_system(pkg, problem)
+    pat = orc.pattern(problem.mesh.num_nodes, problem.mesh.connectivity)
+    np.testing.assert_array_equal(sys_.outer.cpu().numpy(), pat["outer"])
+    np.testing.assert_array_equal(sys_.inner.cpu().numpy(), pat["inner"])
+
+
+def test_evaluate_matches_oracle(pkg, orc, problem, cuda):
+    mesh, mat = problem.mesh, problem.material
+    sys_ = make_system(pkg, problem)
+    u = torch.tensor(problem.u, device=cuda)
+    ev = sys_.evaluate(u, 0.0, True)
+    nt = mat.kinematic_terms
+    ref = orc.system_evaluate(mat.as_dict(), mesh.coords, mesh.connectivity, problem.u,
+                              device_to_oracle(problem.state, nt), problem.alpha, kinematics="logarithmic")
+    assert ref["code"] == 0
+    f = ev.internal.cpu().numpy()
+    scale = np.abs(ref["internal"]).max()
+    assert np.abs(f - ref["internal"]).max() <= 1e-11 * ref["gross"]
+    v = ev.tangent.cpu().numpy()
+    assert np.linalg.norm(v - ref["values"]) <= 1e-11 * np.linalg.norm(ref["values"])
+    assert ev.yielding_points == ref["yielding_points"]
+    assert abs(ev.gross - ref["gross"]) <= 1e-12 * ref["gross"]
+    assert abs(ev.energy - ref["energy"]) <= 1e-11 * abs(ref["energy"])
+    st = device_to_oracle(sys_.trial_states(), nt)
+    assert np.abs(st[..., 36] - ref["states"][..., 36]).max() <= 1e-10 * scale + 1e-12
+    assert (sys_.trial_yield().sum() == ref["yielding_points"])
+
+
+def test_assembly_is_the_element_order_sum(pkg, orc, problem, cuda):
+    """Given the same element matrices, the gathered values equal the
+    reference's element-by-element scatter bit for bit."""
+    mesh, mat = problem.mesh, problem.material
+    sys_ = make_system(pkg, problem)
+    u = torch.tensor(problem.u, device=cuda)
+    ev = sys_.evaluate(u, 0.0, True)
+    values = ev.tangent.cpu().numpy().copy()
+    x = torch.tensor(mesh.element_coordinates(), device=cuda)
+    ue = torch.tensor(mesh.gather(problem.u), device=cuda)
+    r = pkg.element_batch(mat, x, ue, torch.tensor(problem.state, device=cuda), torch.tensor(problem.alpha,
+                                                                                                device=cuda))
+    K = dense_from_blocks(r.tangent.cpu().numpy())
+    pat = orc.pattern(mesh.num_nodes, mesh.connectivity)
+    ref = orc.scatter(mesh.num_nodes, mesh.connectivity, pat, K)
+    assert np.array_equal(values, ref)
+    # f_int likewise, in element order per DOF.
+    f = r.force.cpu().numpy()
+    fi = np.zeros(mesh.num_dofs)
+    for e in range(mesh.num_elements):
+        for a in range(8):
+            n = mesh.connectivity[e, a]
+            fi[3 * n:3 * n + 3] += f[e, 3 * a:3 * a + 3]
+    assert np.array_equal(ev.internal.cpu().numpy(), fi)
+
+
+def test_commit_and_restart(pkg, problem, cuda):
+    sys_ = make_system(pkg, problem)
+    u = torch.tensor(problem.u, device=cuda)
+    sys_.evaluate(u, 0.0, False)
+    trial = sys_.trial_states()
+    modes = sys_.trial_modes()
+    sys_.commit()
+    np.testing.assert_array_equal(sys_.committed_all(), trial)
+    np.testing.assert_array_equal(sys_.internal_all(), modes)
+    # A restart from the saved history evaluates alike.
+    other = make_system(pkg, problem)
+    other.set_committed(trial)
+    other.set_internal(modes)
+    a = sys_.evaluate(u, 0.0, True)
+    fa, va = a.internal.clone(), a.tangent.clone()
+    b = other.evaluate(u, 0.0, True)
+    assert torch.equal(fa, b.internal) and torch.equal(va, b.tangent)
+
+
+def test_solver_error_names_the_element(pkg, problem, cuda):
+    sys_ = make_system(pkg, problem)
+    u = torch.tensor(problem.u, device=cuda).clone()
+    mesh = problem.mesh
+    # Fold element 5 through itself: its top nodes below its bottom ones.
+    top = mesh.connectivity[5, 4:]
+    u.view(-1, 3)[torch.tensor(top, device=cuda), 2] -= 3.0 * 5e-4
+    with pytest.raises(pkg.SolverError) as err:
+        sys_.evaluate(u, 0.0, True)
+    assert err.value.element >= 0
