@@ -1,0 +1,381 @@
+"""Throughput of the element loop: incompatible-mode Hex8 tangent + residual +
+assembly, element updates per second, FP64.
+
+Workload (one step): NonlinearSystem.evaluate(u, 0, want_tangent=True) on
+the element-kernel microbenchmark - a 1000 x 500 x 2 sheet of 0.04 x 0.04 x
+0.5 mm cells (1,000,000 incompatible-mode Hex8, 8 points each), Hill48 +
+two-term Chaboche with Voce hardening, logarithmic strain, a committed
+plastic history and an increment that makes about 40 % of the points yield
+(springback-precomp_b200/workload.py). One step is the element kernel
+(local Newton, condensation), the gather of f_int / gross / energy / yield
+count and the gather of the tangent into the 283.8M-entry CSC pattern.
+
+`value` is elements / s with the inputs resident on the device; `e2e` the
+same through the C ABI with host buffers: u copied in from pinned memory
+and f_int plus the tangent values copied back, every step. Under torchrun
+every rank evaluates its own part (independent meshes, no collective on the
+data path; weak scaling); the time is the max over ranks.
+
+--impl reference times the reference's CPU algorithm - the oracle's
+restatement of it (the reference needs Eigen, which this image lacks) - on
+all host cores, on a bounded sample of the same workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+PKG = "springback-precomp_b200"
+METRIC = "Hex8 tangent+residual+assembly elem/s (FP64)"
+UNIT = "elem/s"
+
+
+def env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def oracle_module():
+    """The checker (test infrastructure), for the CPU-baseline legs only."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    oracle.build()
+    return oracle
+
+
+def oracle_problem(orc, nx, ny, nz, seed):
+    """A sample problem of the same construction, built with the oracle on
+    the CPU (no GPU on the reference arm's path)."""
+    wl = importlib.import_module(PKG + ".workload")
+    device_to_oracle, oracle_to_device = orc.device_to_oracle, orc.oracle_to_device
+
+    def evaluate(mesh, mat, u, state, alpha, want_yield=False):
+        nt = mat.kinematic_terms
+        r = orc.elements(mat.as_dict(), mesh.element_coordinates(), mesh.gather(u), device_to_oracle(state, nt),
+                         alpha, want_tangent=False)
+        out = (oracle_to_device(r["states"], nt), r["alpha"], r["status"])
+        return out + ((r["yield_flags"],) if want_yield else ())
+
+    prob = wl.make_problem(nx, ny, nz, seed=seed, evaluate=evaluate, sample=min(1024, nx * ny * nz))
+    return prob, device_to_oracle(prob.state, prob.material.kinematic_terms)
+
+
+def time_oracle(orc, prob, committed, threads, min_seconds):
+    """elements/s of the oracle's NonlinearSystem::evaluate (element loop on
+    `threads` OpenMP threads, serial gather and scatter) on the sample."""
+    mesh, mat = prob.mesh, prob.material
+    pat = orc.pattern(mesh.num_nodes, mesh.connectivity)
+    orc.system_evaluate(mat.as_dict(), mesh.coords, mesh.connectivity, prob.u, committed, prob.alpha,
+                        threads=threads, pat=pat)
+    times = []
+    t_end = time.perf_counter() + min_seconds
+    while time.perf_counter() < t_end or len(times) < 3:
+        t0 = time.perf_counter()
+        r = orc.system_evaluate(mat.as_dict(), mesh.coords, mesh.connectivity, prob.u, committed, prob.alpha,
+                                threads=threads, pat=pat)
+        times.append(time.perf_counter() - t0)
+        assert r["code"] == 0
+    return mesh.num_elements / statistics.median(times), len(times)
+
+
+def cpu_count():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "100", "-i", str(self.gpu)], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.file.flush()
+
+    def summary(self):
+        self.file.seek(0)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.file.read().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.file.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp64_peak_tflops(torch, dev):
+    """Measured FP64 peak of this GPU: a cuBLAS DGEMM (8192^3, best of 5)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the oracle port on all host cores."""
+    if rank != 0:
+        return 0
+    orc = oracle_module()
+    nx, ny, nz = args.sample_nx, args.sample_ny, args.nz
+    prob, committed = oracle_problem(orc, nx, ny, nz, seed=7)
+    cores = cpu_count()
+    mesh, mat = prob.mesh, prob.material
+    pat = orc.pattern(mesh.num_nodes, mesh.connectivity)
+    for _ in range(args.warmup):
+        orc.system_evaluate(mat.as_dict(), mesh.coords, mesh.connectivity, prob.u, committed, prob.alpha,
+                            threads=cores, pat=pat)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        r = orc.system_evaluate(mat.as_dict(), mesh.coords, mesh.connectivity, prob.u, committed, prob.alpha,
+                                threads=cores, pat=pat)
+        assert r["code"] == 0
+    dt = (time.perf_counter() - t0) / args.steps
+    value = mesh.num_elements / dt
+    sample = (f"{mesh.num_elements} elements ({nx}x{ny}x{nz} of the same sheet, law and history construction) "
+              f"per step")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config(args, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config(args, world):
+    return {"workload": f"element-kernel microbenchmark: {args.nx}x{args.ny}x{args.nz} IM Hex8 sheet "
+                        f"(0.04x0.04x0.5 mm cells), 2x2x2 points, Hill48 r=(0.73,0.80,0.70) + Chaboche "
+                        f"(8000 MPa/200, 1200 MPa/20) + Voce, logarithmic strain, ~40% of points yielding; "
+                        f"one step = NonlinearSystem.evaluate with tangent",
+            "elements_per_rank": args.nx * args.ny * args.nz, "parallelism": f"replicas x{world}",
+            "l2": "inputs larger than L2 (1.7 GB committed state, 4.6 GB element tangents, 2.3 GB CSC values "
+                  "per rank)"}
+
+
+def main():
+    p = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--nx", type=int, default=1000)
+    p.add_argument("--ny", type=int, default=500)
+    p.add_argument("--nz", type=int, default=2)
+    p.add_argument("--sample-nx", type=int, default=50)
+    p.add_argument("--sample-ny", type=int, default=40)
+    p.add_argument("--epb", type=int, default=0, help="elements per block of the element kernel (0: default)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    args = p.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local = env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+
+    pkg = importlib.import_module(PKG)
+    wl = importlib.import_module(PKG + ".workload")
+    peaks = measured_peaks()
+    fp64_peak = fp64_peak_tflops(torch, dev)
+
+    t_setup = time.perf_counter()
+    sysm, u, s, mesh = wl.make_system_problem(args.nx, args.ny, args.nz, seed=7 + rank, device=dev)
+    ne = mesh.num_elements
+    if args.epb:
+        sysm.set_elements_per_block(args.epb)
+    sysm.set_timing(True)
+    setup_s = time.perf_counter() - t_setup
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        ev = sysm.evaluate(u, 0.0, True)
+    yielding = ev.yielding_points
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    elem_ms, force_ms, value_ms = [], [], []
+    with ClockSampler(local) as clocks:
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(args.steps):
+            ev = sysm.evaluate(u, 0.0, True)
+            t = sysm.last_timings()
+            elem_ms.append(t["element"])
+            force_ms.append(t["forces"])
+            value_ms.append(t["values"])
+        end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / args.steps
+    if world > 1:
+        m = torch.tensor([ms], device=dev)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        ms = float(m.item())
+    value = world * ne / (ms / 1e3)
+
+    # End to end through the C ABI with host buffers.
+    e2e = None
+    if not args.no_e2e:
+        u_host = u.cpu().pin_memory()
+        f_host = torch.empty(sysm.num_dofs, dtype=torch.float64).pin_memory()
+        v_host = torch.empty(sysm.nnz, dtype=torch.float64).pin_memory()
+        u_dev = torch.empty_like(u)
+        barrier()
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(args.steps):
+            u_dev.copy_(u_host, non_blocking=True)
+            ev = sysm.evaluate(u_dev, 0.0, True)
+            f_host.copy_(ev.internal, non_blocking=True)
+            v_host.copy_(ev.tangent, non_blocking=True)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e_ms = s0.elapsed_time(s1) / args.steps
+        if world > 1:
+            m = torch.tensor([e_ms], device=dev)
+            dist.all_reduce(m, op=dist.ReduceOp.MAX)
+            e_ms = float(m.item())
+        e2e = {"value": world * ne / (e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 8 * sysm.num_dofs,
+               "d2h_bytes_per_step": 8 * (sysm.num_dofs + sysm.nnz), "ms_per_step": e_ms}
+
+    line = None
+    if rank == 0:
+        cpu = None
+        flops_per_element = None
+        if world == 1 and not args.no_cpu_baseline:
+            orc = oracle_module()
+            prob, committed = oracle_problem(orc, args.sample_nx, args.sample_ny, args.nz, seed=7)
+            cores = cpu_count()
+            all_rate, n_all = time_oracle(orc, prob, committed, cores, 10.0)
+            one_rate, n_one = time_oracle(orc, prob, committed, 1, 5.0)
+            cpu = {"value": all_rate, "unit": UNIT, "cores": cores, "kind": "port",
+                   "sample": f"{prob.mesh.num_elements} elements ({args.sample_nx}x{args.sample_ny}x{args.nz} of the "
+                             f"same sheet, law and history construction), median of {n_all} runs on {cores} "
+                             f"threads", "single_thread": one_rate}
+            # Algorithmic flops per element (counting scalar) on the same sample.
+            cnt = orc.count_flops(prob.material.as_dict(), prob.mesh.element_coordinates(),
+                                  prob.mesh.gather(prob.u), committed, prob.alpha)
+            flops_per_element = cnt / prob.mesh.num_elements
+        el_ms = statistics.mean(elem_ms)
+        roofline = None
+        if flops_per_element:
+            achieved = flops_per_element * ne / (el_ms / 1e3) / 1e12
+            roofline = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                        "frac": achieved / fp64_peak, "traffic": None,
+                        "kernel": "element_kernel (K1)", "kernel_ms": el_ms,
+                        "flops_per_element": flops_per_element,
+                        "peak_source": "measured in this run: cuBLAS FP64 GEMM 8192^3 burst (FP64 has no entry in "
+                                       "MEASURED_PEAKS.json)"}
+        # Assembly (K2) is bandwidth bound: its algorithmic bytes per step.
+        nnz = sysm.nnz
+        asm_bytes = ne * 576 * 8 + nnz * 8 + ne * 64 * 4 + (nnz // 9) * (4 + 8 + 4 + 4)
+        asm_ms = statistics.mean(value_ms)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config(args, world),
+                "roofline": roofline,
+                "roofline_assembly": {"bound": "hbm", "achieved": asm_bytes / (asm_ms / 1e3) / 1e9,
+                                      "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                                      "frac": asm_bytes / (asm_ms / 1e3) / 1e9 / peaks.get("hbm_gbs", 6650.0),
+                                      "kernel": "assemble_values (K2)", "kernel_ms": asm_ms,
+                                      "traffic": None},
+                "phases_ms": {"element": el_ms, "forces": statistics.mean(force_ms), "values": asm_ms},
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 4 * args.steps,
+                "clocks": clocks.summary(), "yielding_fraction": yielding / (8.0 * ne), "increment_s": s,
+                "setup_s": setup_s}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

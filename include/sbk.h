@@ -176,6 +176,14 @@ typedef struct sbk_evaluation {
 int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int want_tangent,
                         sbk_evaluation* out);
 
+/* Device time of each phase of the last evaluate, in ms, recorded with CUDA
+ * events on the system's stream when timing is on: [0] the element kernel,
+ * [1] the force gather and reductions, [2] the tangent value gather (the
+ * element_tangent / element_residual phases of the reference's TimingLedger,
+ * src/fem/Forming.cpp:766-783, split by kernel). */
+int sbk_system_set_timing(sbk_system* sys, int enable);
+int sbk_system_last_timings(const sbk_system* sys, double* ms3);
+
 /* NonlinearSystem::commit (NonlinearSystem.hpp:119-129): the trial points
  * and modes of the last successful evaluate become the committed ones. */
 int sbk_system_commit(sbk_system* sys);

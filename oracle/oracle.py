@@ -326,3 +326,28 @@ class Contact:
         out = np.zeros((cap, 7))
         n = lib().orc_contact_history(self.h, k, cap, _p(out))
         return out[:n].copy()
+
+
+def oracle_to_device(st: np.ndarray, nterms: int) -> np.ndarray:
+    """(ne, nq, 39) oracle states -> (nfields, ne, nq), the product's device
+    layout (plastic strain, back stress, kinematic terms, eqps, loading)."""
+    ne, nq, _ = st.shape
+    out = np.zeros((14 + 6 * nterms, ne, nq))
+    out[0:12] = np.moveaxis(st[..., 0:12], -1, 0)
+    for t in range(nterms):
+        out[12 + 6 * t:18 + 6 * t] = np.moveaxis(st[..., 12 + 6 * t:18 + 6 * t], -1, 0)
+    out[12 + 6 * nterms] = st[..., 36]
+    out[13 + 6 * nterms] = st[..., 38]
+    return out
+
+
+def device_to_oracle(st: np.ndarray, nterms: int) -> np.ndarray:
+    """The inverse of oracle_to_device."""
+    _, ne, nq = st.shape
+    out = np.zeros((ne, nq, NF))
+    out[..., 0:12] = np.moveaxis(st[0:12], 0, -1)
+    for t in range(nterms):
+        out[..., 12 + 6 * t:18 + 6 * t] = np.moveaxis(st[12 + 6 * t:18 + 6 * t], 0, -1)
+    out[..., 36] = st[12 + 6 * nterms]
+    out[..., 38] = st[13 + 6 * nterms]
+    return out

@@ -324,6 +324,9 @@ struct sbk_system {
   int32_t* node_src = nullptr;
   int elements_per_block = 0;
   bool has_trial = false;
+  bool timing = false;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  double last_ms[3] = {0.0, 0.0, 0.0};
 
   sbk::GatherMaps maps() const {
     sbk::GatherMaps m;
@@ -351,6 +354,8 @@ void free_system(sbk_system* s) {
                   s->block_value, s->block_ptr, s->block_src, s->node_ptr, s->node_src};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  for (cudaEvent_t e : s->ev)
+    if (e) cudaEventDestroy(e);
   delete s;
 }
 
@@ -633,14 +638,37 @@ int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int
   std::memset(out, 0, sizeof(*out));
   out->failed_element = -1;
   SBK_CUDA(cudaMemsetAsync(sys->first_fail, 0x7f, sizeof(int32_t), st));
+  if (sys->timing) SBK_CUDA(cudaEventRecord(sys->ev[0], st));
   int rc = sbk::launch_elements(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c,
                                 want_tangent, sys->force, sys->tangent, sys->energy_e, sys->trial, sys->alpha_t,
                                 sys->yield, sys->iters, sys->code, sys->first_fail, false,
                                 sys->elements_per_block, st);
   if (rc) return fail(SBK_ERR_CUDA, std::string("element kernel: ") + cudaGetErrorString((cudaError_t)rc));
+  if (sys->timing) SBK_CUDA(cudaEventRecord(sys->ev[1], st));
+  // The assembly runs unconditionally; a failed element is reported after
+  // it, with the scalars, in a single synchronisation (its sums are then
+  // discarded, as the reference discards them when it throws).
+  rc = sbk::launch_assemble_forces(sys->maps(), sys->force, sys->energy_e, sys->yield, sys->p.nq, sys->internal,
+                                   sys->scratch, sys->scalars, st);
+  if (rc) return fail(SBK_ERR_CUDA, std::string("assembly: ") + cudaGetErrorString((cudaError_t)rc));
+  if (sys->timing) SBK_CUDA(cudaEventRecord(sys->ev[2], st));
+  if (want_tangent) {
+    rc = sbk::launch_assemble_values(sys->maps(), sys->tangent, sys->values, st);
+    if (rc) return fail(SBK_ERR_CUDA, std::string("assembly: ") + cudaGetErrorString((cudaError_t)rc));
+  }
+  if (sys->timing) SBK_CUDA(cudaEventRecord(sys->ev[3], st));
+  double sc[3];
   int32_t first = 0;
+  SBK_CUDA(cudaMemcpyAsync(sc, sys->scalars, sizeof(sc), cudaMemcpyDeviceToHost, st));
   SBK_CUDA(cudaMemcpyAsync(&first, sys->first_fail, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   SBK_CUDA(cudaStreamSynchronize(st));
+  if (sys->timing) {
+    float ms = 0.0f;
+    for (int i = 0; i < 3; ++i) {
+      SBK_CUDA(cudaEventElapsedTime(&ms, sys->ev[i], sys->ev[i + 1]));
+      sys->last_ms[i] = ms;
+    }
+  }
   if (first != 0x7f7f7f7f) {
     int32_t code = 0;
     SBK_CUDA(cudaMemcpy(&code, sys->code + first, sizeof(int32_t), cudaMemcpyDeviceToHost));
@@ -651,16 +679,6 @@ int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int
     std::snprintf(buf, sizeof(buf), "Hex8 element %d: SolverError (code %d)", first, code);
     return fail(SBK_ERR_SOLVER, buf);
   }
-  rc = sbk::launch_assemble_forces(sys->maps(), sys->force, sys->energy_e, sys->yield, sys->p.nq, sys->internal,
-                                   sys->scratch, sys->scalars, st);
-  if (rc) return fail(SBK_ERR_CUDA, std::string("assembly: ") + cudaGetErrorString((cudaError_t)rc));
-  if (want_tangent) {
-    rc = sbk::launch_assemble_values(sys->maps(), sys->tangent, sys->values, st);
-    if (rc) return fail(SBK_ERR_CUDA, std::string("assembly: ") + cudaGetErrorString((cudaError_t)rc));
-  }
-  double sc[3];
-  SBK_CUDA(cudaMemcpyAsync(sc, sys->scalars, sizeof(sc), cudaMemcpyDeviceToHost, st));
-  SBK_CUDA(cudaStreamSynchronize(st));
   out->internal_dev = sys->internal;
   out->residual_dev = sys->internal;
   out->values_dev = want_tangent ? sys->values : nullptr;
@@ -668,6 +686,20 @@ int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int
   out->gross = std::sqrt(sc[1]);
   out->yielding_points = static_cast<int32_t>(sc[2]);
   sys->has_trial = true;
+  return SBK_OK;
+}
+
+int sbk_system_set_timing(sbk_system* sys, int enable) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  if (enable && !sys->ev[0])
+    for (cudaEvent_t& e : sys->ev) SBK_CUDA(cudaEventCreate(&e));
+  sys->timing = enable != 0;
+  return SBK_OK;
+}
+
+int sbk_system_last_timings(const sbk_system* sys, double* ms3) {
+  if (!sys || !ms3) return fail(SBK_ERR_ARGUMENT, "null argument");
+  for (int i = 0; i < 3; ++i) ms3[i] = sys->last_ms[i];
   return SBK_OK;
 }
 

@@ -245,7 +245,7 @@ struct Terms {
   double a[SBK_MAX_BACKSTRESSES][6];
 };
 
-__device__ __forceinline__ bool gr_evaluate(const Params& p, const double s_trial[6], const Terms& tn,
+__device__ __noinline__ bool gr_evaluate(const Params& p, const double s_trial[6], const Terms& tn,
                                             double a_n, const double xi[6], double dl, GPoint& e) {
   double pxi[6];
 #pragma unroll
@@ -271,9 +271,9 @@ __device__ __forceinline__ bool gr_evaluate(const Params& p, const double s_tria
   }
   e.b = 2.0 * p.G * dl;
   e.db = 2.0 * p.G;
-#pragma unroll
-  for (int t = 0; t < SBK_MAX_BACKSTRESSES; ++t) {
-    if (t < p.nterms) {
+#pragma unroll 1
+  for (int t = 0; t < p.nterms; ++t) {
+    {
       const Decay d = decay_of(p.termG[t], dl, p.integration);
 #pragma unroll
       for (int i = 0; i < 6; ++i) {
@@ -373,7 +373,7 @@ __device__ __forceinline__ void lu7_solve(const double A[49], const int piv[7], 
 
 // C_alg = C^e - 2G [m_t a^T + (dl / sigma_bar) S^-1 (P - m m^T) A] with
 // [A; a^T] = J^-1 [D_dev; 0] (Plasticity.cpp:299-311).
-__device__ __forceinline__ void gr_tangent(const Params& p, const GPoint& e, double a_n, double dl, double C[36]) {
+__device__ __noinline__ void gr_tangent(const Params& p, const GPoint& e, double a_n, double dl, double C[36]) {
   double J[49];
   int piv[7];
   gr_jacobian(p, e, a_n, dl, J);
@@ -381,7 +381,7 @@ __device__ __forceinline__ void gr_tangent(const Params& p, const GPoint& e, dou
   const double g = p.G;
   elastic_C(p, C);
   const double f = (dl > 0.0) ? 2.0 * g * dl / e.eq : 0.0;
-#pragma unroll
+#pragma unroll 1
   for (int col = 0; col < 6; ++col) {
     double x[7];
 #pragma unroll
@@ -404,6 +404,17 @@ __device__ __forceinline__ void gr_tangent(const Params& p, const GPoint& e, dou
       C[i * 6 + col] -= v;
     }
   }
+}
+
+// The Newton step of the closest-point equations: J step = -R.
+__device__ __noinline__ void gr_newton_step(const Params& p, const GPoint& e, double a_n, double dl, double step[7]) {
+  double J[49];
+  int piv[7];
+  gr_jacobian(p, e, a_n, dl, J);
+  lu7(J, piv);
+#pragma unroll
+  for (int i = 0; i < 7; ++i) step[i] = -e.res[i];
+  lu7_solve(J, piv, step);
 }
 
 __device__ __noinline__ int general_return(const Params& p, const double strain[6], const PointState& st,
@@ -510,15 +521,7 @@ __device__ __noinline__ int general_return(const Params& p, const double strain[
       break;
     }
     double step[7];
-    {
-      double J[49];
-      int piv[7];
-      gr_jacobian(p, e, a_n, dl, J);
-      lu7(J, piv);
-#pragma unroll
-      for (int i = 0; i < 7; ++i) step[i] = -e.res[i];
-      lu7_solve(J, piv, step);
-    }
+    gr_newton_step(p, e, a_n, dl, step);
     const double r0 = rnorm(e);
     double t = 1.0;
     bool accepted = false;
@@ -547,15 +550,7 @@ __device__ __noinline__ int general_return(const Params& p, const double strain[
   if (rinf(e) > 4.0 * eps_scale) {
     // One more full Newton step (Plasticity.cpp:431-448).
     double step[7];
-    {
-      double J[49];
-      int piv[7];
-      gr_jacobian(p, e, a_n, dl, J);
-      lu7(J, piv);
-#pragma unroll
-      for (int i = 0; i < 7; ++i) step[i] = -e.res[i];
-      lu7_solve(J, piv, step);
-    }
+    gr_newton_step(p, e, a_n, dl, step);
     double xp[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) xp[i] = xi[i] + step[i];
@@ -775,7 +770,7 @@ __device__ __forceinline__ double rot_m(const double q[9], int r, int c) {
 
 // S = P^T T, and material = P^T C P + T : L in global axes (engineering
 // strain columns, tensorial stress rows). C is overwritten by the material.
-__device__ __forceinline__ void log_transform(const LogKin& L, const double t[6], double s_out[6], double C[36]) {
+__device__ __noinline__ void log_transform(const LogKin& L, const double t[6], double s_out[6], double C[36]) {
   const int kr[6] = {0, 1, 2, 0, 1, 2};
   const int kc[6] = {0, 1, 2, 1, 2, 0};
   double M[36];

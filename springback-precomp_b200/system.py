@@ -180,6 +180,15 @@ class NonlinearSystem:
     def set_elements_per_block(self, epb: int):
         _capi.check(_capi.lib().sbk_system_set_elements_per_block(self._h, int(epb)))
 
+    def set_timing(self, enable: bool = True):
+        _capi.check(_capi.lib().sbk_system_set_timing(self._h, int(enable)))
+
+    def last_timings(self) -> dict:
+        """Device ms of the last evaluate: element kernel, force gather, value gather."""
+        out = (ctypes.c_double * 3)()
+        _capi.check(_capi.lib().sbk_system_last_timings(self._h, out))
+        return {"element": out[0], "forces": out[1], "values": out[2]}
+
     def symmetric(self) -> bool:
         return bool(_capi.lib().sbk_system_symmetric(self._h))
 
@@ -228,6 +237,14 @@ class NonlinearSystem:
         if alpha.shape != (self.mesh.num_elements, 9):
             raise _capi.SbkError(2, "the saved internal-mode history does not match the mesh")
         _capi.check(_capi.lib().sbk_system_set_committed(self._h, None, alpha.ctypes.data_as(ctypes.c_void_p)))
+
+    def committed_views(self):
+        """Zero-copy device views of the committed points (nfields, ne, nq)
+        and modes (ne, 9); valid until the next commit."""
+        c_st, c_al, t_st, t_al = (ctypes.c_void_p() for _ in range(4))
+        _capi.check(_capi.lib().sbk_system_buffers(self._h, ctypes.byref(c_st), ctypes.byref(c_al),
+                                                   ctypes.byref(t_st), ctypes.byref(t_al)))
+        return (device_view(c_st.value, self._state_shape()), device_view(c_al.value, (self.mesh.num_elements, 9)))
 
     def trial_states(self) -> np.ndarray:
         out = np.empty(self._state_shape())

@@ -1,8 +1,8 @@
 """Synthetic inputs of the element-kernel microbenchmark: a regular
 nx x ny x nz Hex8 sheet of 0.04 x 0.04 x 0.5 mm cells (1000 x 500 x 2 =
 1,000,000 elements at full size), the Hill48 + two-term Chaboche law, and
-nodal displacements u_ref of uniform noise (+-2 % of the cell size per axis)
-plus a smooth bending field. Every point starts from a seeded history
+nodal displacements u_ref of uniform noise (+-2 % of the mesh size h = 0.04 mm
+on every component) plus a smooth bending field. Every point starts from a seeded history
 (accumulated plastic strain U[0, 0.15], deviatoric backstresses of tensor
 norm <= 20 MPa); loading to u_ref in four committed increments gives a
 converged plastic history; the evaluated state is then u_ref + s du, du
@@ -23,6 +23,10 @@ from .material import Material, hill_chaboche_sheet
 from .mesh import HexMesh, structured_hex_mesh
 
 CELL = (4.0e-5, 4.0e-5, 5.0e-4)  # m
+# The noise of every displacement component: 2 % of the mesh size h of the
+# sheet (its in-plane cell edge); 2 % of the 0.5 mm thickness cell would shear
+# the 0.04 mm wide columns by about 25 %.
+NOISE = 0.02 * CELL[0]
 
 
 @dataclasses.dataclass
@@ -36,44 +40,6 @@ class Problem:
     kinematics: str = "logarithmic"
 
 
-def _point_gradients(x8: np.ndarray, nq_rule: np.ndarray) -> np.ndarray:
-    """G (nq, 3, 8): reference gradients of one element's nodes at the rule's
-    points (every cell of the regular grid has the same)."""
-    corners = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1], [-1, -1, 1], [1, -1, 1], [1, 1, 1],
-                        [-1, 1, 1]], dtype=np.float64)
-    out = []
-    for xi, eta, zeta, _ in nq_rule:
-        f = np.stack([1 + xi * corners[:, 0], 1 + eta * corners[:, 1], 1 + zeta * corners[:, 2]], axis=1)
-        dn = np.stack([0.125 * corners[:, 0] * f[:, 1] * f[:, 2], 0.125 * corners[:, 1] * f[:, 0] * f[:, 2],
-                       0.125 * corners[:, 2] * f[:, 0] * f[:, 1]], axis=1)  # (8, 3)
-        jac = x8.T @ dn  # (3, 3)
-        out.append((dn @ np.linalg.inv(jac)).T)
-    return np.array(out)
-
-
-def gauss2_rule() -> np.ndarray:
-    a = 1.0 / np.sqrt(3.0)
-    pts = []
-    for z in (-a, a):
-        for y in (-a, a):
-            for x in (-a, a):
-                pts.append((x, y, z, 1.0))
-    return np.array(pts)
-
-
-def _log_strain(ue: np.ndarray, G: np.ndarray) -> np.ndarray:
-    """E_log (n, nq, 6) engineering Voigt of displacements ue (n, 24) with
-    the modes at zero."""
-    U = ue.reshape(-1, 8, 3)  # (n, a, i)
-    H = np.einsum("nai,qja->nqij", U, G)
-    E = 0.5 * (H + np.swapaxes(H, -1, -2) + np.einsum("nqki,nqkj->nqij", H, H))
-    w, v = np.linalg.eigh(E)
-    lw = 0.5 * np.log1p(2.0 * w)
-    L = np.einsum("nqia,nqa,nqja->nqij", v, lw, v)
-    return np.stack([L[..., 0, 0], L[..., 1, 1], L[..., 2, 2], 2 * L[..., 0, 1], 2 * L[..., 1, 2],
-                     2 * L[..., 2, 0]], axis=-1)
-
-
 def displacement(mesh: HexMesh, seed: int) -> np.ndarray:
     rng = np.random.default_rng(seed)
     x, y, z = mesh.coords[:, 0], mesh.coords[:, 1], mesh.coords[:, 2]
@@ -83,7 +49,7 @@ def displacement(mesh: HexMesh, seed: int) -> np.ndarray:
     u[:, 0] = -kx * (x - xc) * (z - zc)
     u[:, 1] = -ky * (y - yc) * (z - zc)
     u[:, 2] = 0.5 * kx * (x - xc) ** 2 + 0.5 * ky * (y - yc) ** 2
-    u += rng.uniform(-0.02, 0.02, size=u.shape) * np.array(CELL)
+    u += rng.uniform(-NOISE, NOISE, size=u.shape)
     return u.reshape(-1)
 
 
@@ -136,9 +102,7 @@ def make_problem(nx: int = 1000, ny: int = 500, nz: int = 2, seed: int = 7, s: O
     mesh = structured_hex_mesh(nx, ny, nz, nx * CELL[0], ny * CELL[1], nz * CELL[2])
     material = material or hill_chaboche_sheet()
     evaluate = evaluate or gpu_evaluate
-    u_ref = displacement(mesh, seed)
-    rng = np.random.default_rng(seed + 3)
-    du = -u_ref + 0.25 * (rng.uniform(-0.02, 0.02, size=(mesh.num_nodes, 3)) * np.array(CELL)).reshape(-1)
+    u_ref, du = increment(mesh, seed)
     state, alpha = load_history(mesh, material, u_ref, seeded_state(mesh, material, seed), evaluate, steps)
     if s is None:
         els = np.sort(np.random.default_rng(seed + 2).choice(mesh.num_elements,
@@ -156,6 +120,83 @@ def make_problem(nx: int = 1000, ny: int = 500, nz: int = 2, seed: int = 7, s: O
                 hi = mid
         s = 0.5 * (lo + hi)
     return Problem(mesh=mesh, material=material, u=u_ref + s * du, state=state, alpha=alpha, s=s)
+
+
+def increment(mesh: HexMesh, seed: int):
+    """u_ref and the mostly reversing direction du of the increment."""
+    u_ref = displacement(mesh, seed)
+    rng = np.random.default_rng(seed + 3)
+    du = -u_ref + 0.25 * rng.uniform(-NOISE, NOISE, size=3 * mesh.num_nodes)
+    return u_ref, du
+
+
+def make_system_problem(nx: int = 1000, ny: int = 500, nz: int = 2, seed: int = 7, target: float = 0.4,
+                        sample: int = 4096, steps: int = 4, material: Optional[Material] = None, device=None):
+    """The same problem, built on the GPU without host round trips: the
+    history is loaded by the element kernel straight into the committed
+    buffers of a NonlinearSystem; the bisection runs the kernel on a sample.
+    Returns (system, u on the device, s, mesh)."""
+    import torch
+
+    from .system import NonlinearSystem, element_batch
+
+    dev = torch.device(device or "cuda")
+    mesh = structured_hex_mesh(nx, ny, nz, nx * CELL[0], ny * CELL[1], nz * CELL[2])
+    material = material or hill_chaboche_sheet()
+    u_ref, du = increment(mesh, seed)
+    sysm = NonlinearSystem(mesh, material, kinematics="logarithmic")
+    u_ref_d = torch.tensor(u_ref, device=dev)
+    du_d = torch.tensor(du, device=dev)
+    cs, ca = sysm.committed_views()
+    cs.copy_(torch.tensor(seeded_state(mesh, material, seed), device=dev))
+    ca.zero_()
+    conn_all = torch.tensor(mesh.connectivity, device=dev).long()
+    coords = torch.tensor(mesh.coords, device=dev)
+    # The history: `steps` committed increments to u_ref, element by element
+    # (an element whose local iteration fails keeps its last history).
+    chunk = 262144
+    for k in range(1, steps + 1):
+        uk = ((k / steps) * u_ref_d).view(-1, 3)
+        for lo in range(0, mesh.num_elements, chunk):
+            hi = min(mesh.num_elements, lo + chunk)
+            cc = conn_all[lo:hi]
+            r = element_batch(material, coords[cc].reshape(-1, 24).contiguous(), uk[cc].reshape(-1, 24).contiguous(),
+                              cs[:, lo:hi].contiguous(), ca[lo:hi].contiguous(), want_tangent=False)
+            ok = r.code == 0
+            cs[:, lo:hi] = torch.where(ok[None, :, None], r.states, cs[:, lo:hi])
+            ca[lo:hi] = torch.where(ok[:, None], r.alpha, ca[lo:hi])
+    cs, ca = sysm.committed_views()
+    els = torch.tensor(np.sort(np.random.default_rng(seed + 2).choice(mesh.num_elements,
+                                                                      size=min(sample, mesh.num_elements),
+                                                                      replace=False)), device=dev)
+    conn = conn_all.index_select(0, els)
+    x_s = coords[conn].reshape(-1, 24).contiguous()
+    st_s = cs.index_select(1, els).contiguous()
+    al_s = ca.index_select(0, els).contiguous()
+    lo, hi = 0.0, 1.0
+    for _ in range(16):
+        mid = 0.5 * (lo + hi)
+        u = (u_ref_d + mid * du_d).view(-1, 3)
+        r = element_batch(material, x_s, u[conn].reshape(-1, 24).contiguous(), st_s, al_s, want_tangent=False)
+        ok = r.code == 0
+        f = float(r.yielding[ok].float().mean().item()) if bool(ok.any()) else 1.0
+        if f < target:
+            lo = mid
+        else:
+            hi = mid
+    s = 0.5 * (lo + hi)
+    # Every element must converge at the evaluated state (the reference would
+    # cut the increment): shorten it until they do.
+    for _ in range(20):
+        u = (u_ref_d + s * du_d).contiguous()
+        try:
+            sysm.evaluate(u, 0.0, False)
+            break
+        except Exception as err:
+            if not hasattr(err, "element"):
+                raise
+            s *= 0.9
+    return sysm, u, s, mesh
 
 
 def gpu_evaluate(mesh, material, u, state, alpha, want_yield=False):
