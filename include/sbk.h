@@ -271,6 +271,38 @@ int sbk_contact_commit(sbk_contact* c);
 int sbk_contact_history(const sbk_contact* c, int32_t k, int32_t max_entries, double* out,
                         int32_t* count);
 
+/* ---- the element loop of a small mesh, allocating nothing ---------------
+ * No counterpart in the reference. For callers that cannot allocate device
+ * memory - a solver working in a fixed device arena its host application
+ * hands it, or code that must not call cudaMalloc while it runs - this
+ * evaluates one mesh of at most SBK_NOALLOC_MAX_ELEMENTS elements and
+ * SBK_NOALLOC_MAX_NODES nodes like sbk_system_evaluate, with every input and
+ * output in the caller's device memory. The element tangents and forces
+ * between the element kernel and the assembly live in one fixed file-scope
+ * device array (about 10 MB), which every GPU that loads the library holds
+ * until the process exits; larger meshes are refused (SBK_ERR_UNSUPPORTED).
+ *   coords_dev 3 per node, connectivity_dev 8 per element, u_dev 3 per node,
+ *   state_dev / alpha_dev the committed points and modes (sbk_element_batch
+ *   layout; alpha NULL: zero), outer_dev / inner_dev / nnz the node-block
+ *   CSC pattern of the mesh (as sbk_system_pattern gives it).
+ * outputs: internal_dev (f_int, 3 per node), values_dev (nnz CSC values,
+ *   summed element by element in element order; NULL: no tangent),
+ *   trial_dev / alpha_out_dev / yield_dev (as sbk_element_batch), and
+ *   summary_dev: 5 doubles - energy, gross, yielding points, the lowest
+ *   failing element (-1 if none) and its sbk_element_code.
+ * The call only enqueues work on `stream`; read summary_dev after it. The
+ * first call on a device looks up the array's device address (with that
+ * device current), so make it before any stream capture. All calls share
+ * the array: calls that overlap on the GPU race. */
+#define SBK_NOALLOC_MAX_ELEMENTS 2048
+#define SBK_NOALLOC_MAX_NODES 16384
+int sbk_evaluate_noalloc(const sbk_material* material, const sbk_rule* rule, int kinematics,
+                         int32_t num_nodes, int32_t num_elements, const double* coords_dev,
+                         const int32_t* connectivity_dev, const double* u_dev, const double* state_dev,
+                         const double* alpha_dev, const int32_t* outer_dev, const int32_t* inner_dev,
+                         int64_t nnz, double* internal_dev, double* values_dev, double* trial_dev,
+                         double* alpha_out_dev, uint8_t* yield_dev, double* summary_dev, void* stream);
+
 /* Last error message of this thread (never NULL). */
 const char* sbk_last_error(void);
 

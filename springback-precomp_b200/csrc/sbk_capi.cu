@@ -149,26 +149,34 @@ int validate_material(const sbk_material& m) {
   return SBK_OK;
 }
 
-// Gauss-Legendre rules (src/elements/Quadrature.cpp:16-219).
-std::vector<std::pair<double, double>> line_rule(int n) {
-  std::vector<std::pair<double, double>> r;
-  if (n == 1) return {{0.0, 2.0}};
+// Gauss-Legendre rules (src/elements/Quadrature.cpp:16-219), into fixed
+// arrays (no heap): n points (x, w) of the line rule.
+void line_rule(int n, double x_out[7], double w_out[7]) {
+  if (n == 1) {
+    x_out[0] = 0.0;
+    w_out[0] = 2.0;
+    return;
+  }
   if (n == 2) {
     const double a = 1.0 / std::sqrt(3.0);
-    return {{-a, 1.0}, {a, 1.0}};
+    x_out[0] = -a, x_out[1] = a, w_out[0] = w_out[1] = 1.0;
+    return;
   }
   if (n == 3) {
     const double a = std::sqrt(3.0 / 5.0);
-    return {{-a, 5.0 / 9.0}, {0.0, 8.0 / 9.0}, {a, 5.0 / 9.0}};
+    x_out[0] = -a, x_out[1] = 0.0, x_out[2] = a;
+    w_out[0] = w_out[2] = 5.0 / 9.0, w_out[1] = 8.0 / 9.0;
+    return;
   }
   if (n == 4) {
     const double s6 = std::sqrt(6.0 / 5.0);
     const double x1 = std::sqrt((3.0 - 2.0 * s6) / 7.0), x2 = std::sqrt((3.0 + 2.0 * s6) / 7.0);
     const double s = std::sqrt(30.0);
     const double w1 = (18.0 + s) / 36.0, w2 = (18.0 - s) / 36.0;
-    return {{-x2, w2}, {-x1, w1}, {x1, w1}, {x2, w2}};
+    x_out[0] = -x2, x_out[1] = -x1, x_out[2] = x1, x_out[3] = x2;
+    w_out[0] = w2, w_out[1] = w1, w_out[2] = w1, w_out[3] = w2;
+    return;
   }
-  r.assign(static_cast<size_t>(n), {0.0, 0.0});
   const double pi = std::acos(-1.0);
   auto legendre = [n](double x, double& p0, double& p1) {
     p0 = 1.0;
@@ -194,35 +202,45 @@ std::vector<std::pair<double, double>> line_rule(int n) {
     legendre(x, p0, p1);
     const double der = n * (x * p1 - p0) / (x * x - 1.0);
     const double w = 2.0 / ((1.0 - x * x) * der * der);
-    r[static_cast<size_t>(i)] = {-x, w};
-    r[static_cast<size_t>(n - 1 - i)] = {x, w};
+    x_out[i] = -x, w_out[i] = w;
+    x_out[n - 1 - i] = x, w_out[n - 1 - i] = w;
   }
-  return r;
 }
 
-int make_rule(const sbk_rule& rule, std::vector<double>& pts) {
+// The Hex8 stiffness rule: xi fastest, weights multiplied x * y * z
+// (Hex8Kernels.hpp:125-130, Quadrature.cpp:165-219). Returns the point count
+// (points with more than SBK_MAX_POINTS are counted but not stored), or a
+// negative status.
+int make_rule(const sbk_rule& rule, double pts[SBK_MAX_POINTS][4]) {
   int np = rule.stiffness_points, nt = rule.thickness_points, axis = rule.thickness_axis;
-  if (np < 1 || np > 4) return fail(SBK_ERR_CONFIG, "stiffness points must be 1 to 4");
+  if (np < 1 || np > 4) return -fail(SBK_ERR_CONFIG, "stiffness points must be 1 to 4");
   if (nt <= 0 || nt == np) {
     nt = np;
     axis = 2;
   }
-  if (nt > 7) return fail(SBK_ERR_CONFIG, "thickness points must be 1 to 7");
-  if (axis < 0 || axis > 2) return fail(SBK_ERR_CONFIG, "the thickness axis must be 0, 1 or 2");
-  const auto plane = line_rule(np), through = line_rule(nt);
-  const auto& rx = axis == 0 ? through : plane;
-  const auto& ry = axis == 1 ? through : plane;
-  const auto& rz = axis == 2 ? through : plane;
-  pts.clear();
-  for (const auto& gk : rz)
-    for (const auto& gj : ry)
-      for (const auto& gi : rx) {
-        pts.push_back(gi.first);
-        pts.push_back(gj.first);
-        pts.push_back(gk.first);
-        pts.push_back(gi.second * gj.second * gk.second);
+  if (nt > 7) return -fail(SBK_ERR_CONFIG, "thickness points must be 1 to 7");
+  if (axis < 0 || axis > 2) return -fail(SBK_ERR_CONFIG, "the thickness axis must be 0, 1 or 2");
+  double px[7], pw[7], tx[7], tw[7];
+  line_rule(np, px, pw);
+  line_rule(nt, tx, tw);
+  const int nx = axis == 0 ? nt : np, ny = axis == 1 ? nt : np, nz = axis == 2 ? nt : np;
+  const double* rxx = axis == 0 ? tx : px;
+  const double* rxw = axis == 0 ? tw : pw;
+  const double* ryx = axis == 1 ? tx : px;
+  const double* ryw = axis == 1 ? tw : pw;
+  const double* rzx = axis == 2 ? tx : px;
+  const double* rzw = axis == 2 ? tw : pw;
+  int q = 0;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i, ++q) {
+        if (q >= SBK_MAX_POINTS) continue;
+        pts[q][0] = rxx[i];
+        pts[q][1] = ryx[j];
+        pts[q][2] = rzx[k];
+        pts[q][3] = rxw[i] * ryw[j] * rzw[k];
       }
-  return SBK_OK;
+  return q;
 }
 
 int make_params(const sbk_material* mat, const sbk_rule* rule, int kinematics, Params& p) {
@@ -231,10 +249,9 @@ int make_params(const sbk_material* mat, const sbk_rule* rule, int kinematics, P
   if (rc) return rc;
   if (kinematics < SBK_SMALL_STRAIN || kinematics > SBK_FINITE_LOGARITHMIC)
     return fail(SBK_ERR_ARGUMENT, "unknown kinematics");
-  std::vector<double> pts;
-  rc = make_rule(*rule, pts);
-  if (rc) return rc;
-  const int nq = static_cast<int>(pts.size() / 4);
+  double pts[SBK_MAX_POINTS][4];
+  const int nq = make_rule(*rule, pts);
+  if (nq < 0) return -nq;
   if (nq > SBK_MAX_POINTS) return fail(SBK_ERR_UNSUPPORTED, "rules of more than 32 points are not supported");
   std::memset(&p, 0, sizeof(Params));
   const double E = mat->youngs_modulus, nu = mat->poisson_ratio;
@@ -271,7 +288,7 @@ int make_params(const sbk_material* mat, const sbk_rule* rule, int kinematics, P
   p.nq = nq;
   p.nfields = sbk::state_fields(p.nterms);
   for (int q = 0; q < nq; ++q)
-    for (int k = 0; k < 4; ++k) p.qp[q][k] = pts[4 * q + k];
+    for (int k = 0; k < 4; ++k) p.qp[q][k] = pts[q][k];
   return SBK_OK;
 }
 
@@ -471,6 +488,9 @@ int upload(T** dst, const std::vector<T>& src, cudaStream_t s) {
 
 namespace sbk {
 int set_error(int code, const std::string& what) { return fail(code, what); }
+int make_launch_params(const sbk_material* material, const sbk_rule* rule, int kinematics, Params& p) {
+  return make_params(material, rule, kinematics, p);
+}
 }  // namespace sbk
 
 extern "C" {
@@ -479,9 +499,9 @@ const char* sbk_last_error(void) { return g_error.c_str(); }
 
 int sbk_rule_size(const sbk_rule* rule) {
   if (!rule) return 0;
-  std::vector<double> pts;
-  if (make_rule(*rule, pts) != SBK_OK) return 0;
-  return static_cast<int>(pts.size() / 4);
+  double pts[SBK_MAX_POINTS][4];
+  const int n = make_rule(*rule, pts);
+  return n < 0 ? 0 : n;
 }
 
 int sbk_state_fields(const sbk_material* material) {

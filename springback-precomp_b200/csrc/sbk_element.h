@@ -14,6 +14,9 @@ namespace sbk {
 
 // Records the message sbk_last_error returns; returns `code`.
 int set_error(int code, const std::string& what);
+// The launch parameters of a material, rule and kinematics (validated; no
+// allocation).
+int make_launch_params(const sbk_material* material, const sbk_rule* rule, int kinematics, Params& p);
 
 // K1: ne elements. Mesh mode (batch = false): coords 3 per node, conn 8 per
 // element, u 3 per node. Batch mode: coords and u hold 24 per element.

@@ -112,6 +112,33 @@ def element_batch(material: Material, x: torch.Tensor, u: torch.Tensor, state: O
     return out
 
 
+NOALLOC_MAX_ELEMENTS = 2048
+NOALLOC_MAX_NODES = 16384
+
+
+def evaluate_noalloc(material: Material, coords: torch.Tensor, connectivity: torch.Tensor, u: torch.Tensor,
+                     state: torch.Tensor, alpha: Optional[torch.Tensor], outer: torch.Tensor, inner: torch.Tensor,
+                     internal: torch.Tensor, values: Optional[torch.Tensor], trial: torch.Tensor,
+                     alpha_out: torch.Tensor, yielding: torch.Tensor, summary: torch.Tensor,
+                     kinematics: str = "logarithmic", stiffness_points: int = 2, thickness_points: int = 0,
+                     thickness_axis: int = 2, stream=None):
+    """sbk_evaluate_noalloc: the element loop of a small mesh (at most
+    2048 elements, 16384 nodes) for callers that cannot allocate device
+    memory; every buffer is the caller's (device tensors), the library
+    allocates nothing. Results land in the given tensors on `stream`;
+    summary (5 doubles): energy, gross, yielding points, lowest failing
+    element (-1: none), its code."""
+    mat = material.to_c()
+    rule = rule_c(stiffness_points, thickness_points, thickness_axis)
+    st = _capi.lib().sbk_evaluate_noalloc(
+        ctypes.byref(mat), ctypes.byref(rule), _capi.KINEMATICS[kinematics], int(coords.numel() // 3),
+        int(connectivity.numel() // 8), _ptr(coords), _ptr(connectivity), _ptr(u), _ptr(state),
+        _ptr(alpha) if alpha is not None else None, _ptr(outer), _ptr(inner), int(inner.numel()), _ptr(internal),
+        _ptr(values) if values is not None else None, _ptr(trial), _ptr(alpha_out), _ptr(yielding), _ptr(summary),
+        _stream_ptr(stream))
+    _capi.check(st)
+
+
 @dataclasses.dataclass
 class Evaluation:
     """NonlinearSystem.hpp:27-47. Tensors are views of the system's buffers,
