@@ -36,7 +36,7 @@ constexpr double kLocalMarquardt = 1.0e-6;
 constexpr double kLocalTolerance = 1.0e-8;
 constexpr double kLocalRoundOff = 1.0e-13;
 
-constexpr int kSlot = 56;  // per point: D 36 | S 6 | F 9 | w | energy | floor factor | pad
+constexpr int kSlot = 54;  // per point: D 36 | S 6 | F 9 | w | energy | floor factor
 constexpr int kSlotS = 36, kSlotF = 42, kSlotW = 51, kSlotE = 52, kSlotFl = 53;
 
 __constant__ double kCorner[8][3] = {{-1, -1, -1}, {1, -1, -1}, {1, 1, -1}, {-1, 1, -1},
@@ -48,9 +48,10 @@ struct __align__(16) ElemShared {
   double U[24];
   double jinv0[9];
   double geo[G][12];  // J^-1 (9), w det J, det0 / det
-  double hu[G][9];
   double slot[G][kSlot];
-  double kaa[((81 + G - 1) / G) * G];
+  // K_aa (the reduced sums) during the local iteration; the coupling
+  // C = K_aa^-1 K_au (9 x 24) in the condensation.
+  double kc[216];
   double r[33];
   double scale[9];
   double flo[9];
@@ -61,7 +62,6 @@ struct __align__(16) ElemShared {
   double r0[9];
   double lu[81];
   double maxpivot;
-  double work[243];  // k0 | sym | scratch; the coupling C (9 x 24) at the end
   double dval[4];
   int rowp[9], colp[9], perm[9];
   int ival[4];
@@ -195,6 +195,7 @@ struct Ctx {
   const double* state;
   double* trial;
   uint8_t* yield;
+  double* hu;  // this lane's U G^T (per-lane memory)
   __device__ __forceinline__ void sync() const { __syncwarp(mask); }
 };
 
@@ -275,7 +276,7 @@ __device__ int set_up(const Ctx<G>& c) {
           for (int j = 0; j < 3; ++j) hu[i * 3 + j] += s.U[3 * a + i] * g[j];
       }
 #pragma unroll
-      for (int i = 0; i < 9; ++i) s.hu[q][i] = hu[i];
+      for (int i = 0; i < 9; ++i) c.hu[i] = hu[i];
     }
   }
   bad = __any_sync(c.mask, bad);
@@ -307,7 +308,7 @@ __device__ __noinline__ int pass(const Ctx<G>& c, const double at[9]) {
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int j = 0; j < 3; ++j) {
-        double v = s.hu[q][i * 3 + j];
+        double v = c.hu[i * 3 + j];
 #pragma unroll
         for (int m = 0; m < 3; ++m) v += at[3 * m + i] * gt[j * 3 + m];
         h[i * 3 + j] = v;
@@ -446,7 +447,7 @@ __device__ __noinline__ int pass(const Ctx<G>& c, const double at[9]) {
       kbuf[idx % G] = v;
       if (idx % G == G - 1) {
         const double y = reduce_scatter<G>(kbuf, c.lane, c.mask);
-        s.kaa[(idx / G) * G + c.lane] = y;
+        s.kc[(idx / G) * G + c.lane] = y;
       }
     }
   }
@@ -454,7 +455,7 @@ __device__ __noinline__ int pass(const Ctx<G>& c, const double at[9]) {
 #pragma unroll
     for (int i = 81 % G; i < G; ++i) kbuf[i] = 0.0;
     const double y = reduce_scatter<G>(kbuf, c.lane, c.mask);
-    s.kaa[(81 / G) * G + c.lane] = y;
+    s.kc[(81 / G) * G + c.lane] = y;
   }
   c.sync();
   // The force and the scale sums over the points, in point order: lane a
@@ -518,15 +519,15 @@ __device__ __noinline__ int pass(const Ctx<G>& c, const double at[9]) {
 // ---- element-level helpers (lane 0, shared memory) ---------------------------
 
 // FullPivLU of a (9x9 row-major) into lu; true if invertible (Eigen's rank test).
-__device__ bool fullpiv_lu9(const double* a, double* lu, int* rowp, int* colp, double* maxpivot_out) {
-  for (int i = 0; i < 81; ++i) lu[i] = a[i];
+__device__ __noinline__ bool fullpiv_lu9(const double* a, double* lu, int* rowp, int* colp, double* maxpivot_out) {
+  _Pragma("unroll 1") for (int i = 0; i < 81; ++i) lu[i] = a[i];
   double maxpivot = 0.0;
   int nonzero = 9;
-  for (int k = 0; k < 9; ++k) {
+  _Pragma("unroll 1") for (int k = 0; k < 9; ++k) {
     int pr = k, pc = k;
     double big = -1.0;
-    for (int j = k; j < 9; ++j)
-      for (int i = k; i < 9; ++i) {
+    _Pragma("unroll 1") for (int j = k; j < 9; ++j)
+      _Pragma("unroll 1") for (int i = k; i < 9; ++i) {
         const double v = fabs(lu[i * 9 + j]);
         if (v > big) {
           big = v;
@@ -536,41 +537,41 @@ __device__ bool fullpiv_lu9(const double* a, double* lu, int* rowp, int* colp, d
       }
     if (big == 0.0) {
       nonzero = k;
-      for (int i = k; i < 9; ++i) rowp[i] = colp[i] = i;
+      _Pragma("unroll 1") for (int i = k; i < 9; ++i) rowp[i] = colp[i] = i;
       break;
     }
     if (big > maxpivot) maxpivot = big;
     rowp[k] = pr;
     colp[k] = pc;
     if (pr != k)
-      for (int j = 0; j < 9; ++j) {
+      _Pragma("unroll 1") for (int j = 0; j < 9; ++j) {
         const double t = lu[k * 9 + j];
         lu[k * 9 + j] = lu[pr * 9 + j];
         lu[pr * 9 + j] = t;
       }
     if (pc != k)
-      for (int i = 0; i < 9; ++i) {
+      _Pragma("unroll 1") for (int i = 0; i < 9; ++i) {
         const double t = lu[i * 9 + k];
         lu[i * 9 + k] = lu[i * 9 + pc];
         lu[i * 9 + pc] = t;
       }
     const double inv = 1.0 / lu[k * 9 + k];
-    for (int i = k + 1; i < 9; ++i) lu[i * 9 + k] *= inv;
-    for (int i = k + 1; i < 9; ++i) {
+    _Pragma("unroll 1") for (int i = k + 1; i < 9; ++i) lu[i * 9 + k] *= inv;
+    _Pragma("unroll 1") for (int i = k + 1; i < 9; ++i) {
       const double l = lu[i * 9 + k];
-      for (int j = k + 1; j < 9; ++j) lu[i * 9 + j] -= l * lu[k * 9 + j];
+      _Pragma("unroll 1") for (int j = k + 1; j < 9; ++j) lu[i * 9 + j] -= l * lu[k * 9 + j];
     }
   }
   *maxpivot_out = maxpivot;
   if (nonzero < 9) return false;
   const double threshold = kEps * 9.0 * maxpivot;
-  for (int i = 0; i < 9; ++i)
+  _Pragma("unroll 1") for (int i = 0; i < 9; ++i)
     if (!(fabs(lu[i * 9 + i]) > threshold)) return false;
   return true;
 }
 
 // x = A^-1 b with the FullPivLU factors (any lane; b and x may alias).
-__device__ __forceinline__ void fullpiv_solve9(const double* lu, const int* rowp, const int* colp, const double* b,
+__device__ __noinline__ void fullpiv_solve9(const double* lu, const int* rowp, const int* colp, const double* b,
                                                double* x) {
   double y[9];
 #pragma unroll
@@ -614,59 +615,59 @@ __device__ __forceinline__ void fullpiv_solve9(const double* lu, const int* rowp
 }
 
 // Cholesky (lower, in place); false at the first non-positive pivot.
-__device__ bool llt9(double* a) {
-  for (int k = 0; k < 9; ++k) {
+__device__ __noinline__ bool llt9(double* a) {
+  _Pragma("unroll 1") for (int k = 0; k < 9; ++k) {
     double x = a[k * 9 + k];
-    for (int j = 0; j < k; ++j) x -= a[k * 9 + j] * a[k * 9 + j];
+    _Pragma("unroll 1") for (int j = 0; j < k; ++j) x -= a[k * 9 + j] * a[k * 9 + j];
     if (x <= 0.0) return false;
     a[k * 9 + k] = sqrt(x);
-    for (int i = k + 1; i < 9; ++i) {
+    _Pragma("unroll 1") for (int i = k + 1; i < 9; ++i) {
       double v = a[i * 9 + k];
-      for (int j = 0; j < k; ++j) v -= a[i * 9 + j] * a[k * 9 + j];
+      _Pragma("unroll 1") for (int j = 0; j < k; ++j) v -= a[i * 9 + j] * a[k * 9 + j];
       a[i * 9 + k] = v / a[k * 9 + k];
     }
   }
   return true;
 }
-__device__ void llt9_solve(const double* l, const double* b, double* x) {
+__device__ __noinline__ void llt9_solve(const double* l, const double* b, double* x) {
   double y[9];
-  for (int i = 0; i < 9; ++i) {
+  _Pragma("unroll 1") for (int i = 0; i < 9; ++i) {
     double v = b[i];
-    for (int j = 0; j < i; ++j) v -= l[i * 9 + j] * y[j];
+    _Pragma("unroll 1") for (int j = 0; j < i; ++j) v -= l[i * 9 + j] * y[j];
     y[i] = v / l[i * 9 + i];
   }
-  for (int i = 8; i >= 0; --i) {
+  _Pragma("unroll 1") for (int i = 8; i >= 0; --i) {
     double v = y[i];
-    for (int j = i + 1; j < 9; ++j) v -= l[j * 9 + i] * y[j];
+    _Pragma("unroll 1") for (int j = i + 1; j < 9; ++j) v -= l[j * 9 + i] * y[j];
     y[i] = v / l[i * 9 + i];
   }
-  for (int i = 0; i < 9; ++i) x[i] = y[i];
+  _Pragma("unroll 1") for (int i = 0; i < 9; ++i) x[i] = y[i];
 }
 
 // Smallest eigenvalue and largest |eigenvalue| of a symmetric 9x9 (cyclic
 // Jacobi on a copy in `a`, destroyed).
-__device__ void sym_eig9(double* a, double* lo, double* top) {
-  for (int sweep = 0; sweep < 60; ++sweep) {
+__device__ __noinline__ void sym_eig9(double* a, double* lo, double* top) {
+  _Pragma("unroll 1") for (int sweep = 0; sweep < 60; ++sweep) {
     double off = 0.0, diag = 0.0;
-    for (int p = 0; p < 9; ++p) {
+    _Pragma("unroll 1") for (int p = 0; p < 9; ++p) {
       diag += a[p * 9 + p] * a[p * 9 + p];
-      for (int q = p + 1; q < 9; ++q) off += a[p * 9 + q] * a[p * 9 + q];
+      _Pragma("unroll 1") for (int q = p + 1; q < 9; ++q) off += a[p * 9 + q] * a[p * 9 + q];
     }
     if (off == 0.0 || off <= 1.0e-36 * diag) break;
-    for (int p = 0; p < 8; ++p)
-      for (int q = p + 1; q < 9; ++q) {
+    _Pragma("unroll 1") for (int p = 0; p < 8; ++p)
+      _Pragma("unroll 1") for (int q = p + 1; q < 9; ++q) {
         const double apq = a[p * 9 + q];
         if (apq == 0.0) continue;
         const double theta = (a[q * 9 + q] - a[p * 9 + p]) / (2.0 * apq);
         const double t = (theta >= 0.0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
         const double cs = 1.0 / sqrt(t * t + 1.0);
         const double sn = t * cs;
-        for (int k = 0; k < 9; ++k) {
+        _Pragma("unroll 1") for (int k = 0; k < 9; ++k) {
           const double akp = a[k * 9 + p], akq = a[k * 9 + q];
           a[k * 9 + p] = cs * akp - sn * akq;
           a[k * 9 + q] = sn * akp + cs * akq;
         }
-        for (int k = 0; k < 9; ++k) {
+        _Pragma("unroll 1") for (int k = 0; k < 9; ++k) {
           const double apk = a[p * 9 + k], aqk = a[q * 9 + k];
           a[p * 9 + k] = cs * apk - sn * aqk;
           a[q * 9 + k] = sn * apk + cs * aqk;
@@ -674,7 +675,7 @@ __device__ void sym_eig9(double* a, double* lo, double* top) {
       }
   }
   double mn = a[0], mx = fabs(a[0]);
-  for (int i = 1; i < 9; ++i) {
+  _Pragma("unroll 1") for (int i = 1; i < 9; ++i) {
     mn = fmin(mn, a[i * 9 + i]);
     mx = fmax(mx, fabs(a[i * 9 + i]));
   }
@@ -683,11 +684,11 @@ __device__ void sym_eig9(double* a, double* lo, double* top) {
 }
 
 // Partial-pivoting LU solve of a 9x9 (in place), x = A^-1 b.
-__device__ void plu9_solve(double* a, int* perm, const double* b, double* x) {
-  for (int k = 0; k < 9; ++k) {
+__device__ __noinline__ void plu9_solve(double* a, int* perm, const double* b, double* x) {
+  _Pragma("unroll 1") for (int k = 0; k < 9; ++k) {
     int p = k;
     double big = fabs(a[k * 9 + k]);
-    for (int i = k + 1; i < 9; ++i)
+    _Pragma("unroll 1") for (int i = k + 1; i < 9; ++i)
       if (fabs(a[i * 9 + k]) > big) {
         big = fabs(a[i * 9 + k]);
         p = i;
@@ -695,32 +696,32 @@ __device__ void plu9_solve(double* a, int* perm, const double* b, double* x) {
     perm[k] = p;
     if (big != 0.0) {
       if (p != k)
-        for (int j = 0; j < 9; ++j) {
+        _Pragma("unroll 1") for (int j = 0; j < 9; ++j) {
           const double t = a[k * 9 + j];
           a[k * 9 + j] = a[p * 9 + j];
           a[p * 9 + j] = t;
         }
       const double inv = 1.0 / a[k * 9 + k];
-      for (int i = k + 1; i < 9; ++i) a[i * 9 + k] *= inv;
+      _Pragma("unroll 1") for (int i = k + 1; i < 9; ++i) a[i * 9 + k] *= inv;
     }
-    for (int i = k + 1; i < 9; ++i)
-      for (int j = k + 1; j < 9; ++j) a[i * 9 + j] -= a[i * 9 + k] * a[k * 9 + j];
+    _Pragma("unroll 1") for (int i = k + 1; i < 9; ++i)
+      _Pragma("unroll 1") for (int j = k + 1; j < 9; ++j) a[i * 9 + j] -= a[i * 9 + k] * a[k * 9 + j];
   }
   double y[9];
-  for (int i = 0; i < 9; ++i) y[i] = b[i];
-  for (int k = 0; k < 9; ++k)
+  _Pragma("unroll 1") for (int i = 0; i < 9; ++i) y[i] = b[i];
+  _Pragma("unroll 1") for (int k = 0; k < 9; ++k)
     if (perm[k] != k) {
       const double t = y[k];
       y[k] = y[perm[k]];
       y[perm[k]] = t;
     }
-  for (int i = 1; i < 9; ++i)
-    for (int j = 0; j < i; ++j) y[i] -= a[i * 9 + j] * y[j];
-  for (int i = 8; i >= 0; --i) {
-    for (int j = i + 1; j < 9; ++j) y[i] -= a[i * 9 + j] * y[j];
+  _Pragma("unroll 1") for (int i = 1; i < 9; ++i)
+    _Pragma("unroll 1") for (int j = 0; j < i; ++j) y[i] -= a[i * 9 + j] * y[j];
+  _Pragma("unroll 1") for (int i = 8; i >= 0; --i) {
+    _Pragma("unroll 1") for (int j = i + 1; j < 9; ++j) y[i] -= a[i * 9 + j] * y[j];
     y[i] /= a[i * 9 + i];
   }
-  for (int i = 0; i < 9; ++i) x[i] = y[i];
+  _Pragma("unroll 1") for (int i = 0; i < 9; ++i) x[i] = y[i];
 }
 
 // ---- the local iteration -------------------------------------------------------
@@ -850,6 +851,8 @@ struct Local {
   // a failure code; on success the last pass is at s.alpha and s.lu holds
   // the factors of its K_aa.
   __device__ __noinline__ int run() {
+    // K_aa at alpha (k0), its symmetric part and scratch: lane 0's alone.
+    double work[243];
     {
       double at[9];
 #pragma unroll
@@ -863,9 +866,9 @@ struct Local {
       const double scale = vmax(s.scale);
       const double floor_ = kLocalRoundOff * vmax(s.flo);
       if (c.lane == 0) {
-        s.ival[0] = fullpiv_lu9(s.kaa, s.lu, s.rowp, s.colp, &s.maxpivot) ? 1 : 0;
+        s.ival[0] = fullpiv_lu9(s.kc, s.lu, s.rowp, s.colp, &s.maxpivot) ? 1 : 0;
         // k0 and r0 copies (the trial passes overwrite the sums).
-        for (int i = 0; i < 81; ++i) s.work[i] = s.kaa[i];
+        for (int i = 0; i < 81; ++i) work[i] = s.kc[i];
         for (int i = 0; i < 9; ++i) s.r0[i] = s.r[24 + i];
       }
       c.sync();
@@ -878,10 +881,10 @@ struct Local {
         double nw[9];
         fullpiv_solve9(s.lu, s.rowp, s.colp, s.r0, nw);
         for (int i = 0; i < 9; ++i) s.dir[i] = -nw[i];
-        double* sym = s.work + 81;
+        double* sym = work + 81;
         for (int i = 0; i < 9; ++i)
-          for (int j = 0; j < 9; ++j) sym[i * 9 + j] = 0.5 * (s.work[i * 9 + j] + s.work[j * 9 + i]);
-        double* chol = s.work + 162;
+          for (int j = 0; j < 9; ++j) sym[i * 9 + j] = 0.5 * (work[i * 9 + j] + work[j * 9 + i]);
+        double* chol = work + 162;
         for (int i = 0; i < 81; ++i) chol[i] = sym[i];
         s.ival[1] = llt9(chol) ? 1 : 0;
       }
@@ -899,13 +902,13 @@ struct Local {
         }
         if (c.lane == 0) {
           // The shifted direction (K_aa + mu I) d = -r_alpha.
-          double* sym = s.work + 81;
-          double* tmp = s.work + 162;
+          double* sym = work + 81;
+          double* tmp = work + 162;
           for (int i = 0; i < 81; ++i) tmp[i] = sym[i];
           double lo, top;
           sym_eig9(tmp, &lo, &top);
           const double mu = kLocalShift * top - lo;
-          for (int i = 0; i < 81; ++i) tmp[i] = s.work[i];
+          for (int i = 0; i < 81; ++i) tmp[i] = work[i];
           for (int i = 0; i < 9; ++i) tmp[i * 9 + i] += mu;
           double x[9];
           plu9_solve(tmp, s.perm, s.r0, x);
@@ -918,11 +921,11 @@ struct Local {
       // Levenberg-Marquardt (IncompatibleModes.cpp:522-545).
       double mu = 0.0;
       if (c.lane == 0) {
-        double* normal = s.work + 81;
+        double* normal = work + 81;
         for (int i = 0; i < 9; ++i)
           for (int j = 0; j < 9; ++j) {
             double v = 0.0;
-            for (int k = 0; k < 9; ++k) v += s.work[k * 9 + i] * s.work[k * 9 + j];
+            for (int k = 0; k < 9; ++k) v += work[k * 9 + i] * work[k * 9 + j];
             normal[i * 9 + j] = v;
           }
         double dmax = normal[0];
@@ -935,14 +938,14 @@ struct Local {
       for (int search = 0; search < kMaxLineSearch && !moved; ++search, mu *= 10.0) {
         c.sync();
         if (c.lane == 0) {
-          double* normal = s.work + 81;
-          double* a = s.work + 162;
+          double* normal = work + 81;
+          double* a = work + 162;
           for (int i = 0; i < 81; ++i) a[i] = normal[i];
           for (int i = 0; i < 9; ++i) a[i * 9 + i] += mu;
           double grad[9];
           for (int i = 0; i < 9; ++i) {
             double v = 0.0;
-            for (int j = 0; j < 9; ++j) v += s.work[j * 9 + i] * s.r0[j];
+            for (int j = 0; j < 9; ++j) v += work[j * 9 + i] * s.r0[j];
             grad[i] = v;
           }
           const bool ok = llt9(a);
@@ -990,7 +993,8 @@ __global__ void __launch_bounds__(128) element_kernel(const Params p, int64_t ne
   const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
   const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
   if (e >= ne) return;  // whole groups leave together
-  Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, trial, yield};
+  double hu_lane[9];
+  Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, trial, yield, hu_lane};
   ElemShared<G>& s = *sh;
   // Stage the element's coordinates and displacements (lane a: node a).
   if (lane < 8) {
@@ -1059,7 +1063,7 @@ __global__ void __launch_bounds__(128) element_kernel(const Params p, int64_t ne
     }
     // The coupling C = K_aa^-1 K_au, columns of node a, into shared memory
     // (K_au(3m+l, 3a+k) = kau[k][3m+l], or kua[k][3m+l] when symmetric).
-    double* C = s.work;  // 9 x 24, column-major by DOF: C[col * 9 + i]
+    double* C = s.kc;  // 9 x 24, column-major by DOF: C[col * 9 + i]
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       double b[9];
@@ -1085,7 +1089,7 @@ __global__ void __launch_bounds__(128) element_kernel(const Params p, int64_t ne
       force[e * 24 + 3 * a + k] = s.r[3 * a + k] - v;
     }
     if (want_tangent) {
-      const double* C = s.work;
+      const double* C = s.kc;
 #pragma unroll
       for (int chunk = 0; chunk < 2; ++chunk) {
         double acc[4][9];
