@@ -86,35 +86,52 @@ class Material:
     @classmethod
     def from_swift(cls, name: str, youngs_modulus: float, poisson_ratio: float, K: float, eps0: float, n: float,
                    fit_range: Tuple[float, float] = (0.0, 0.6), points: int = 200, **extra) -> "Material":
-        """Linear + Voce hardening fitted to sigma = K (eps0 + a)^n
-        (python/precomp/materials.py:204-254): the initial yield stress is
-        exact, H and Q >= 0 minimise the squared stress error over `points`
-        plastic strains in `fit_range` for each delta, delta by a bounded
-        scalar search on a log scale."""
-        import numpy as np
-        from scipy.optimize import minimize_scalar, nnls
-
+        """Linear + Voce hardening standing for the Swift law sigma = K (eps0
+        + a)^n, as python/precomp/materials.py:205-254 builds it (the
+        parameters must come out the same, so the fit is the same): sy0 =
+        K eps0^n exactly; H, Q >= 0 by non-negative least squares on the
+        Swift excess over sy0 at `points` equally spaced plastic strains of
+        `fit_range`; delta by a bounded scalar search over ln delta in
+        [ln 0.1, ln 500] (x tolerance 1e-6); delta = 0 when Q vanishes."""
+        if not (K > 0 and eps0 > 0 and n >= 0):
+            raise ValueError("from_swift needs K > 0, eps0 > 0 and n >= 0")
         lo, hi = float(fit_range[0]), float(fit_range[1])
-        a = np.linspace(lo, hi, points)
-        target = K * (eps0 + a) ** n
+        if not 0.0 <= lo < hi:
+            raise ValueError("fit_range must satisfy 0 <= low < high")
         sy0 = K * eps0 ** n
-        rhs = target - sy0
-
-        def solve(log_delta):
-            delta = math.exp(log_delta)
-            A = np.column_stack([a, 1.0 - np.exp(-delta * a)])
-            coef, res = nnls(A, rhs)
-            return coef, float(res)
-
-        best = minimize_scalar(lambda ld: solve(ld)[1], bounds=(math.log(0.1), math.log(500.0)), method="bounded",
-                               options={"xatol": 1e-6})
-        coef, _ = solve(best.x)
-        delta = math.exp(best.x)
-        H, Q = float(coef[0]), float(coef[1])
-        if Q <= 0.0:
-            delta = 0.0
+        H, Q, delta = _voce_fit(lo, hi, points, lambda a: K * (eps0 + a) ** n - sy0)
         return cls(name=name, youngs_modulus=youngs_modulus, poisson_ratio=poisson_ratio, yield_stress=sy0,
                    hardening_modulus=H, saturation_stress=Q, saturation_rate=delta, **extra)
+
+    @classmethod
+    def from_hollomon(cls, name: str, youngs_modulus: float, poisson_ratio: float, K: float, n: float,
+                      yield_stress: float, **extra) -> "Material":
+        """Hollomon sigma = K eps^n from the yield point on
+        (python/precomp/materials.py:256-270): the Swift law whose eps0 puts
+        its start at `yield_stress`, eps0 = (yield_stress / K)^(1/n)."""
+        if not (K > 0 and n > 0 and yield_stress > 0):
+            raise ValueError("from_hollomon needs K, n and yield_stress > 0")
+        return cls.from_swift(name, youngs_modulus, poisson_ratio, K, (yield_stress / K) ** (1.0 / n), n, **extra)
+
+
+def _voce_fit(lo: float, hi: float, points: int, excess):
+    """(H, Q, delta) of H a + Q (1 - exp(-delta a)) closest to excess(a) in
+    least squares over `points` plastic strains a in [lo, hi]."""
+    import numpy as np
+    from scipy.optimize import minimize_scalar, nnls
+
+    a = np.linspace(lo, hi, points)
+    y = excess(a)
+
+    def nnls_at(log_rate):
+        basis = np.column_stack([a, 1.0 - np.exp(-math.exp(log_rate) * a)])
+        return nnls(basis, y)
+
+    search = minimize_scalar(lambda t: float(nnls_at(t)[1]), bounds=(math.log(0.1), math.log(500.0)),
+                             method="bounded", options={"xatol": 1e-6})
+    (H, Q), _ = nnls_at(search.x)
+    H, Q = float(H), float(Q)
+    return H, Q, (math.exp(search.x) if Q > 0.0 else 0.0)
 
 
 def yield_matrix(m: Material):
@@ -155,6 +172,32 @@ def hill_chaboche_sheet() -> Material:
     base = aluminium_swift()
     return dataclasses.replace(base, name="hill_chaboche", criterion="hill48", r0=0.73, r45=0.80, r90=0.70,
                                backstresses=((8000.0e6, 200.0), (1200.0e6, 20.0)))
+
+
+# The built-in sheet materials of python/precomp/materials.py:272-299
+# (Hollomon K, n, yield stress; r-values; E, nu), by name.
+_HOLLOMON = {
+    "AA5754-O": (70.0e9, 0.33, 420e6, 0.30, 100e6, (0.75, 0.70, 0.80)),
+    "AA2024-O": (73.1e9, 0.33, 330e6, 0.20, 75e6, (0.70, 0.80, 0.70)),
+    "AA6061-T6": (68.9e9, 0.33, 410e6, 0.06, 276e6, (0.60, 0.70, 0.65)),
+    "AA7075-O": (71.7e9, 0.33, 400e6, 0.17, 103e6, (0.70, 0.90, 0.80)),
+    "DC04": (210.0e9, 0.30, 530e6, 0.22, 170e6, (1.90, 1.50, 2.20)),
+    "Ti-6Al-4V-annealed": (113.8e9, 0.342, 1100e6, 0.04, 880e6, None),
+}
+
+
+def library_material(name: str, anisotropic: bool = False) -> Material:
+    """A built-in material by name (case-insensitive), J2 with its linear +
+    Voce fit; with `anisotropic`, Hill48 from its r-values (RD = x, ND =
+    z). The reference stores the r-values beside a von Mises criterion
+    unless a deck asks for Hill48."""
+    for key, (E, nu, K, n, sy, r) in _HOLLOMON.items():
+        if key.lower() == name.lower():
+            m = Material.from_hollomon(key, E, nu, K, n, sy)
+            if anisotropic and r is not None:
+                m = dataclasses.replace(m, criterion="hill48", r0=r[0], r45=r[1], r90=r[2])
+            return m
+    raise KeyError(f"unknown material {name!r}; the library has {sorted(_HOLLOMON)}")
 
 
 def j2_steel() -> Material:

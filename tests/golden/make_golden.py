@@ -1,0 +1,49 @@
+"""Writes the golden fixtures of tests/golden from the reference itself.
+
+Run in a checkout that has the reference's sources (its Python package
+`precomp` imports without a build): ``python tests/golden/make_golden.py
+<reference root>``. The fixtures it writes are committed; the tests read
+only them, never the reference.
+
+materials.json: the hardening parameters the reference's own Python
+(python/precomp/materials.py) derives - its built-in library (Hollomon
+fits) and the Swift law of the 40x40x2 forming sheet - plus the material
+blocks of the committed forming decks under benchmarks/ that the
+reference's C++ runs read.
+"""
+from __future__ import annotations
+
+import glob
+import json
+import os
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+KEYS = ("youngs_modulus", "poisson_ratio", "yield_stress", "hardening_modulus", "saturation_stress",
+        "saturation_rate", "kinematic_hardening_modulus")
+
+
+def main(ref_root: str) -> None:
+    sys.path.insert(0, os.path.join(ref_root, "python"))
+    from precomp import materials  # the reference's own module
+
+    out = {"library": {}, "swift": [], "decks": {}}
+    for name, m in sorted(materials.library().items()):
+        out["library"][name] = {k: getattr(m, k) for k in KEYS}
+    for K, eps0, n in [(425e6, 0.003, 0.29), (530e6, 0.005, 0.22), (600e6, 0.01, 0.15)]:
+        m = materials.Material.from_swift("swift", 70e9, 0.33, 2700.0, K=K, eps0=eps0, n=n)
+        out["swift"].append({"K": K, "eps0": eps0, "n": n, **{k: getattr(m, k) for k in KEYS}})
+    for deck in sorted(glob.glob(os.path.join(ref_root, "benchmarks/physics_audit/calculix/punch/strip_h*_im_*/"
+                                                       "sparlab/deck.json")))[:4]:
+        d = json.load(open(deck))
+        mat = d["material"]
+        rel = os.path.relpath(deck, ref_root)
+        out["decks"][rel] = {"name": mat["name"], "youngs_modulus": mat["youngs_modulus"],
+                             "poisson_ratio": mat["poisson_ratio"], **mat["plasticity"]}
+    with open(os.path.join(HERE, "materials.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+        f.write("\n")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
