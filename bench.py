@@ -39,13 +39,6 @@ METRIC = "Hex8 tangent+residual+assembly elem/s (FP64)"
 UNIT = "elem/s"
 
 
-def env_int(name, default):
-    try:
-        return int(os.environ.get(name, default))
-    except ValueError:
-        return default
-
-
 def oracle_module():
     """The checker (test infrastructure), for the CPU-baseline legs only."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -237,29 +230,24 @@ def main():
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
 
-    rank = env_int("RANK", 0)
-    world = env_int("WORLD_SIZE", 1)
-    local = env_int("LOCAL_RANK", 0)
+    replicas = importlib.import_module(PKG + ".replicas")
+    rank, world, local = replicas.rank_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
     import torch
-    import torch.distributed as dist
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
+    replicas.init(world, "nccl", dev)
 
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
-
-    pkg = importlib.import_module(PKG)
     wl = importlib.import_module(PKG + ".workload")
     peaks = measured_peaks()
     fp64_peak = fp64_peak_tflops(torch, dev)
 
     t_setup = time.perf_counter()
-    sysm, u, s, mesh = wl.make_system_problem(args.nx, args.ny, args.nz, seed=7 + rank, device=dev)
+    sysm, u, s, mesh = wl.make_system_problem(args.nx, args.ny, args.nz, seed=replicas.replica_seed(7, rank),
+                                              device=dev)
     ne = mesh.num_elements
     if args.epb:
         sysm.set_elements_per_block(args.epb)
@@ -267,8 +255,7 @@ def main():
     setup_s = time.perf_counter() - t_setup
 
     def barrier():
-        if world > 1:
-            dist.barrier()
+        replicas.barrier(world)
 
     for _ in range(args.warmup):
         ev = sysm.evaluate(u, 0.0, True)
@@ -291,12 +278,8 @@ def main():
         torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
-    ms = start.elapsed_time(end) / args.steps
-    if world > 1:
-        m = torch.tensor([ms], device=dev)
-        dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        ms = float(m.item())
-    value = world * ne / (ms / 1e3)
+    ms = replicas.max_over_ranks(start.elapsed_time(end) / args.steps, world, dev)
+    value = replicas.job_rate(ne, world, ms / 1e3)
 
     # End to end through the C ABI with host buffers.
     e2e = None
@@ -317,12 +300,8 @@ def main():
         s1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        e_ms = s0.elapsed_time(s1) / args.steps
-        if world > 1:
-            m = torch.tensor([e_ms], device=dev)
-            dist.all_reduce(m, op=dist.ReduceOp.MAX)
-            e_ms = float(m.item())
-        e2e = {"value": world * ne / (e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 8 * sysm.num_dofs,
+        e_ms = replicas.max_over_ranks(s0.elapsed_time(s1) / args.steps, world, dev)
+        e2e = {"value": replicas.job_rate(ne, world, e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 8 * sysm.num_dofs,
                "d2h_bytes_per_step": 8 * (sysm.num_dofs + sysm.nnz), "ms_per_step": e_ms}
 
     line = None
@@ -371,9 +350,7 @@ def main():
                 "clocks": clocks.summary(), "yielding_fraction": yielding / (8.0 * ne), "increment_s": s,
                 "setup_s": setup_s}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.finish(world)
     return 0
 
 

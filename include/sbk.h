@@ -210,6 +210,16 @@ int sbk_system_plastic(const sbk_system* sys);
 int sbk_system_add_node_blocks(sbk_system* sys, int32_t n, const int32_t* nodes_dev,
                                const double* blocks_dev);
 
+/* stiffness_gross(K, u, free) (NonlinearSystem.hpp:49-67): the norm over the
+ * free DOFs of |K| |u|, with K the tangent values of the last evaluate (with
+ * any node blocks added since) and u_dev the displacement (num_dofs, device);
+ * free_dev lists num_free DOF indices (device, int32). Every row sum is the
+ * reference's to the bit (columns in ascending order); the squares of the
+ * free rows are summed by a fixed tree. Needs an evaluate with the tangent
+ * first (SBK_ERR_ARGUMENT otherwise). */
+int sbk_system_stiffness_gross(sbk_system* sys, const double* u_dev, int32_t num_free, const int32_t* free_dev,
+                               double* out);
+
 /* ---- contact: ToolContact ---------------------------------------------- */
 typedef struct sbk_contact sbk_contact;
 

@@ -255,6 +255,34 @@ def add_node_blocks(pat: dict, values, nodes, blocks) -> np.ndarray:
     return values
 
 
+def stiffness_product(pat: dict, values, u) -> np.ndarray:
+    """|K| |u| per row as stiffness_gross forms it
+    (src/fem/NonlinearSystem.hpp:55-67): the CSC columns in ascending order,
+    columns of zero displacement skipped, each column's |K(r, c)| |u(c)|
+    added to its rows."""
+    outer, inner = pat["outer"], pat["inner"]
+    values = np.asarray(values, dtype=np.float64)
+    u = np.asarray(u, dtype=np.float64)
+    product = np.zeros(len(outer) - 1)
+    for col in range(len(outer) - 1):
+        uc = abs(u[col])
+        if uc == 0.0:
+            continue
+        lo, hi = outer[col], outer[col + 1]
+        product[inner[lo:hi]] += np.abs(values[lo:hi]) * uc  # distinct rows within a column
+    return product
+
+
+def stiffness_gross(pat: dict, values, u, free) -> float:
+    """stiffness_gross(K, u, free): the norm of |K| |u| over the free DOFs,
+    summed in the order of `free` (NonlinearSystem.hpp:64-66)."""
+    product = stiffness_product(pat, values, u)
+    s = 0.0
+    for d in free:
+        s += product[d] * product[d]
+    return float(np.sqrt(s))
+
+
 class Contact:
     """ToolContact restated: tools = list of dicts with shape ('sphere',
     'plane', 'cylinder'), radius, friction, tangential_ratio, normal, axis,

@@ -145,7 +145,75 @@ __global__ void add_node_blocks_kernel(const int32_t* __restrict__ outer, const 
   }
 }
 
+// stiffness_gross (src/fem/NonlinearSystem.hpp:55-67), first half: |K| |u|
+// per row. The reference walks the CSC columns in ascending order and adds
+// |K(r, c)| |u(c)| to every row r of the column; here one thread owns a row
+// node A and visits its columns in the same ascending order (its neighbours
+// B, then the three columns of B), so every row sum is the reference's, bit
+// for bit. Column 3B's rows are sorted, so the entry (3A, 3B) is found by a
+// binary search over them; columns whose displacement is zero are skipped,
+// as there.
+__global__ void __launch_bounds__(256) stiffness_rows_kernel(int64_t nn, const int32_t* __restrict__ outer,
+                                                             const int32_t* __restrict__ inner,
+                                                             const double* __restrict__ values,
+                                                             const double* __restrict__ u,
+                                                             double* __restrict__ product) {
+  for (int64_t A = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; A < nn; A += (int64_t)gridDim.x * blockDim.x) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    const int32_t lo = outer[3 * A], count = (outer[3 * A + 1] - lo) / 3;
+    for (int32_t k = 0; k < count; ++k) {
+      const int32_t B = inner[lo + 3 * k] / 3;
+      const int32_t c0 = outer[3 * B], c1 = outer[3 * B + 1];
+      int32_t l = c0, h = c1;
+      while (l < h) {
+        const int32_t mid = l + (h - l) / 2;
+        if (inner[mid] < 3 * A) l = mid + 1; else h = mid;
+      }
+      const int64_t stride = (int64_t)c1 - c0;
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        const double uc = fabs(u[3 * B + j]);
+        if (uc == 0.0) continue;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) acc[i] += fabs(values[l + j * stride + i]) * uc;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) product[3 * A + i] = acc[i];
+  }
+}
+
+// Second half: the sum of squares over the listed free DOFs, per block.
+__global__ void __launch_bounds__(kReduceThreads) free_squares_kernel(int32_t n, const int32_t* __restrict__ free_dofs,
+                                                                      const double* __restrict__ product,
+                                                                      double* __restrict__ partial) {
+  __shared__ double sh[kReduceThreads];
+  double s = 0.0;
+  for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = product[free_dofs[i]];
+    s += v * v;
+  }
+  s = block_sum(s, sh);
+  if (threadIdx.x == 0) {
+    partial[3 * blockIdx.x + 0] = s;
+    partial[3 * blockIdx.x + 1] = 0.0;
+    partial[3 * blockIdx.x + 2] = 0.0;
+  }
+}
+
 }  // namespace
+
+int launch_stiffness_gross(int64_t nn, const int32_t* outer, const int32_t* inner, const double* values,
+                           const double* u, int32_t num_free, const int32_t* free_dofs, double* product,
+                           double* scratch, double* scalars, cudaStream_t stream) {
+  int64_t blocks = (nn + 255) / 256;
+  if (blocks > 148 * 32) blocks = 148 * 32;
+  if (blocks > 0)
+    stiffness_rows_kernel<<<(unsigned)blocks, 256, 0, stream>>>(nn, outer, inner, values, u, product);
+  free_squares_kernel<<<kReduceBlocks, kReduceThreads, 0, stream>>>(num_free, free_dofs, product, scratch);
+  finish_kernel<<<1, kReduceThreads, 0, stream>>>(kReduceBlocks, scratch, scalars);
+  return (int)cudaGetLastError();
+}
 
 int launch_assemble_values(const GatherMaps& m, const double* tangent, double* values, cudaStream_t stream) {
   if (m.num_blocks == 0) return 0;

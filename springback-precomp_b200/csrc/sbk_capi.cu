@@ -339,8 +339,10 @@ struct sbk_system {
   int32_t* block_src = nullptr;
   int32_t* node_ptr = nullptr;
   int32_t* node_src = nullptr;
+  double* product = nullptr;  // |K| |u| per DOF (stiffness_gross)
   int elements_per_block = 0;
   bool has_trial = false;
+  bool has_values = false;  // values hold the tangent of the last evaluate
   bool timing = false;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   double last_ms[3] = {0.0, 0.0, 0.0};
@@ -368,7 +370,7 @@ void free_system(sbk_system* s) {
   void* ptrs[] = {s->coords, s->conn, s->committed, s->trial, s->alpha_c, s->alpha_t, s->force,
                   s->tangent, s->energy_e, s->yield, s->iters, s->code, s->first_fail, s->outer,
                   s->inner, s->values, s->internal, s->scratch, s->scalars, s->missing, s->block_col,
-                  s->block_value, s->block_ptr, s->block_src, s->node_ptr, s->node_src};
+                  s->block_value, s->block_ptr, s->block_src, s->node_ptr, s->node_src, s->product};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : s->ev)
@@ -600,6 +602,7 @@ int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const 
   TRY(upload(&s->inner, hp.inner, nullptr));
   TRY(dalloc(&s->values, static_cast<size_t>(s->nnz)));
   TRY(dalloc(&s->internal, static_cast<size_t>(s->nn) * 3));
+  TRY(dalloc(&s->product, static_cast<size_t>(s->nn) * 3));
   TRY(dalloc(&s->scratch, sbk::assemble_scratch_doubles()));
   TRY(dalloc(&s->scalars, 4));
   TRY(dalloc(&s->missing, 1));
@@ -695,6 +698,7 @@ int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int
     out->failed_element = first;
     out->failure_code = code;
     sys->has_trial = false;
+    sys->has_values = false;
     char buf[160];
     std::snprintf(buf, sizeof(buf), "Hex8 element %d: SolverError (code %d)", first, code);
     return fail(SBK_ERR_SOLVER, buf);
@@ -706,6 +710,7 @@ int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int
   out->gross = std::sqrt(sc[1]);
   out->yielding_points = static_cast<int32_t>(sc[2]);
   sys->has_trial = true;
+  sys->has_values = want_tangent != 0;
   return SBK_OK;
 }
 
@@ -792,6 +797,22 @@ int sbk_system_add_node_blocks(sbk_system* sys, int32_t n, const int32_t* nodes_
   SBK_CUDA(cudaMemcpyAsync(&missing, sys->missing, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   SBK_CUDA(cudaStreamSynchronize(st));
   if (missing) return fail(SBK_ERR_ARGUMENT, "a node block lies outside the pattern");
+  return SBK_OK;
+}
+
+int sbk_system_stiffness_gross(sbk_system* sys, const double* u_dev, int32_t num_free, const int32_t* free_dev,
+                               double* out) {
+  if (!sys || !u_dev || !out || num_free < 0 || (num_free > 0 && !free_dev))
+    return fail(SBK_ERR_ARGUMENT, "null argument");
+  if (!sys->has_values) return fail(SBK_ERR_ARGUMENT, "stiffness_gross needs an evaluate with the tangent first");
+  cudaStream_t st = sys->stream;
+  int rc = sbk::launch_stiffness_gross(sys->nn, sys->outer, sys->inner, sys->values, u_dev, num_free, free_dev,
+                                       sys->product, sys->scratch, sys->scalars, st);
+  if (rc) return fail(SBK_ERR_CUDA, "stiffness_gross launch");
+  double sum = 0.0;
+  SBK_CUDA(cudaMemcpyAsync(&sum, sys->scalars, sizeof(double), cudaMemcpyDeviceToHost, st));
+  SBK_CUDA(cudaStreamSynchronize(st));
+  *out = std::sqrt(sum);
   return SBK_OK;
 }
 

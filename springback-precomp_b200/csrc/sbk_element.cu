@@ -974,7 +974,7 @@ struct Local {
 // ---- the condensation ---------------------------------------------------------
 
 template <int G>
-__global__ void __launch_bounds__(128) element_kernel(const Params p, int64_t ne, bool batch,
+__global__ void __launch_bounds__(128) element_kernel(const __grid_constant__ Params p, int64_t ne, bool batch,
                                                       const double* __restrict__ coords,
                                                       const int32_t* __restrict__ conn, const double* __restrict__ u,
                                                       const double* __restrict__ state,

@@ -52,6 +52,11 @@ int launch_assemble_forces(const GatherMaps& m, const double* force, const doubl
                            const uint8_t* yield, int nq, double* internal, double* scratch, double* scalars,
                            cudaStream_t stream);
 size_t assemble_scratch_doubles();
+// stiffness_gross: |K| |u| per row into `product` (3 nn), then the sum of
+// squares of its listed free DOFs into scalars[0] (scratch as for the forces).
+int launch_stiffness_gross(int64_t nn, const int32_t* outer, const int32_t* inner, const double* values,
+                           const double* u, int32_t num_free, const int32_t* free_dofs, double* product,
+                           double* scratch, double* scalars, cudaStream_t stream);
 // add_node_block for n blocks, in list order.
 int launch_add_node_blocks(const int32_t* outer, const int32_t* inner, double* values, int32_t n,
                            const int32_t* nodes, const double* blocks, int32_t* missing, cudaStream_t stream);

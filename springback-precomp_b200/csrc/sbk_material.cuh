@@ -82,7 +82,7 @@ __device__ __forceinline__ void elastic_C(const Params& p, double C[36]) {
 // J2 radial return (Plasticity.cpp:66-171). Returns 0 or a failure code;
 // writes the updated state through `st`.
 // ---------------------------------------------------------------------------
-__device__ __noinline__ int radial_return(const Params& p, const double strain[6], const PointState& st,
+__device__ __forceinline__ int radial_return(const Params& p, const double strain[6], const PointState& st,
                                           Response& out) {
   const double g = p.G, k = p.K, hk = p.Hkin;
   double ep[6], el[6], s[6], xi[6];
@@ -245,7 +245,7 @@ struct Terms {
   double a[SBK_MAX_BACKSTRESSES][6];
 };
 
-__device__ __noinline__ bool gr_evaluate(const Params& p, const double s_trial[6], const Terms& tn,
+__device__ __forceinline__ bool gr_evaluate(const Params& p, const double s_trial[6], const Terms& tn,
                                             double a_n, const double xi[6], double dl, GPoint& e) {
   double pxi[6];
 #pragma unroll
@@ -373,7 +373,7 @@ __device__ __forceinline__ void lu7_solve(const double A[49], const int piv[7], 
 
 // C_alg = C^e - 2G [m_t a^T + (dl / sigma_bar) S^-1 (P - m m^T) A] with
 // [A; a^T] = J^-1 [D_dev; 0] (Plasticity.cpp:299-311).
-__device__ __noinline__ void gr_tangent(const Params& p, const GPoint& e, double a_n, double dl, double C[36]) {
+__device__ __forceinline__ void gr_tangent(const Params& p, const GPoint& e, double a_n, double dl, double C[36]) {
   double J[49];
   int piv[7];
   gr_jacobian(p, e, a_n, dl, J);
@@ -407,7 +407,7 @@ __device__ __noinline__ void gr_tangent(const Params& p, const GPoint& e, double
 }
 
 // The Newton step of the closest-point equations: J step = -R.
-__device__ __noinline__ void gr_newton_step(const Params& p, const GPoint& e, double a_n, double dl, double step[7]) {
+__device__ __forceinline__ void gr_newton_step(const Params& p, const GPoint& e, double a_n, double dl, double step[7]) {
   double J[49];
   int piv[7];
   gr_jacobian(p, e, a_n, dl, J);
@@ -417,7 +417,7 @@ __device__ __noinline__ void gr_newton_step(const Params& p, const GPoint& e, do
   lu7_solve(J, piv, step);
 }
 
-__device__ __noinline__ int general_return(const Params& p, const double strain[6], const PointState& st,
+__device__ __forceinline__ int general_return(const Params& p, const double strain[6], const PointState& st,
                                            Response& out) {
   const double g = p.G, k = p.K;
   const int nt = p.nterms;
@@ -770,7 +770,7 @@ __device__ __forceinline__ double rot_m(const double q[9], int r, int c) {
 
 // S = P^T T, and material = P^T C P + T : L in global axes (engineering
 // strain columns, tensorial stress rows). C is overwritten by the material.
-__device__ __noinline__ void log_transform(const LogKin& L, const double t[6], double s_out[6], double C[36]) {
+__device__ __forceinline__ void log_transform(const LogKin& L, const double t[6], double s_out[6], double C[36]) {
   const int kr[6] = {0, 1, 2, 0, 1, 2};
   const int kc[6] = {0, 1, 2, 1, 2, 0};
   double M[36];

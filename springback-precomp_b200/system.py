@@ -298,3 +298,17 @@ class NonlinearSystem:
         n = int(nodes.numel())
         _capi.check(_capi.lib().sbk_system_add_node_blocks(self._h, n, _ptr(nodes.to(torch.int32).contiguous()),
                                                            _ptr(blocks.to(torch.float64).contiguous())))
+
+    def stiffness_gross(self, u: torch.Tensor, free: torch.Tensor) -> float:
+        """stiffness_gross (src/fem/NonlinearSystem.hpp:49-67): the norm over
+        the DOFs in `free` of |K| |u|, K the tangent of the last evaluate (with
+        any node blocks added since): the round-off floor the forming
+        driver's convergence test takes from the displacement's rounding."""
+        u = u.to(torch.float64).contiguous()
+        if u.numel() != self.num_dofs:
+            raise ValueError(f"u has {u.numel()} values, the system {self.num_dofs} DOFs")
+        free = free.to(device=u.device, dtype=torch.int32).contiguous()
+        out = ctypes.c_double(0.0)
+        _capi.check(_capi.lib().sbk_system_stiffness_gross(self._h, _ptr(u), int(free.numel()), _ptr(free),
+                                                           ctypes.byref(out)))
+        return out.value

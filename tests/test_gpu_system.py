@@ -112,3 +112,28 @@ def test_solver_error_names_the_element(pkg, problem, cuda):
     with pytest.raises(pkg.SolverError) as err:
         sys_.evaluate(u, 0.0, True)
     assert err.value.element >= 0
+
+
+def test_stiffness_gross_is_the_reference_norm(pkg, orc, problem, cuda):
+    """stiffness_gross (NonlinearSystem.hpp:49-67) of the assembled tangent
+    over a free-DOF list that leaves out a clamped edge, after node blocks
+    were added into it, against the oracle's column-ordered restatement."""
+    mesh = problem.mesh
+    sys_ = make_system(pkg, problem)
+    u = torch.tensor(problem.u, device=cuda)
+    ev = sys_.evaluate(u, 0.0, True)
+    nodes = torch.arange(0, mesh.num_nodes, 7, dtype=torch.int32, device=cuda)
+    blocks = torch.tensor(np.random.default_rng(3).uniform(-1e6, 1e6, (len(nodes), 3, 3)), device=cuda)
+    sys_.add_node_blocks(nodes, blocks)
+    x = mesh.coords[:, 0]
+    clamped = np.where(x <= x.min() + 1e-12)[0]
+    free = np.setdiff1d(np.arange(mesh.num_dofs), np.concatenate([3 * clamped, 3 * clamped + 1, 3 * clamped + 2]))
+    u_host = problem.u.copy()
+    u_host[3 * clamped] = 0.0  # columns of zero displacement are skipped
+    got = sys_.stiffness_gross(torch.tensor(u_host, device=cuda), torch.tensor(free, device=cuda))
+    pat = orc.pattern(mesh.num_nodes, mesh.connectivity)
+    ref = orc.stiffness_gross(pat, ev.tangent.cpu().numpy(), u_host, free)
+    assert abs(got - ref) <= 1e-14 * ref, (got, ref)
+    with pytest.raises(pkg.SbkError):
+        fresh = make_system(pkg, problem)
+        fresh.stiffness_gross(u, torch.tensor(free, device=cuda))
