@@ -243,6 +243,57 @@ int make_rule(const sbk_rule& rule, double pts[SBK_MAX_POINTS][4]) {
   return q;
 }
 
+// The generalised eigenvectors of the yield matrix, P v = l S^-1 v with
+// V^T S^-1 V = I (S = diag(1, 1, 1, 1/2, 1/2, 1/2)), through the ordinary
+// eigenproblem of Q = S^1/2 P S^1/2 = U diag(l) U^T by cyclic Jacobi
+// (V = S^1/2 U). The closest-point solves of the general return use them
+// (B^-1 = V (I + f diag(l))^-1 V^T).
+void yield_eigenbasis(const double* P, double* V, double* L) {
+  const double h = std::sqrt(0.5);
+  double s[6] = {1.0, 1.0, 1.0, h, h, h};
+  double a[6][6], u[6][6];
+  for (int i = 0; i < 6; ++i)
+    for (int j = 0; j < 6; ++j) {
+      a[i][j] = s[i] * P[i * 6 + j] * s[j];
+      u[i][j] = i == j ? 1.0 : 0.0;
+    }
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, diag = 0.0;
+    for (int i = 0; i < 6; ++i) {
+      diag += a[i][i] * a[i][i];
+      for (int j = i + 1; j < 6; ++j) off += a[i][j] * a[i][j];
+    }
+    if (off == 0.0 || off <= 1e-40 * diag) break;
+    for (int pp = 0; pp < 5; ++pp)
+      for (int q = pp + 1; q < 6; ++q) {
+        const double apq = a[pp][q];
+        if (apq == 0.0) continue;
+        const double theta = (a[q][q] - a[pp][pp]) / (2.0 * apq);
+        const double t = (theta >= 0.0 ? 1.0 : -1.0) / (std::fabs(theta) + std::sqrt(theta * theta + 1.0));
+        const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+        for (int k = 0; k < 6; ++k) {
+          const double akp = a[k][pp], akq = a[k][q];
+          a[k][pp] = c * akp - sn * akq;
+          a[k][q] = sn * akp + c * akq;
+        }
+        for (int k = 0; k < 6; ++k) {
+          const double apk = a[pp][k], aqk = a[q][k];
+          a[pp][k] = c * apk - sn * aqk;
+          a[q][k] = sn * apk + c * aqk;
+        }
+        for (int k = 0; k < 6; ++k) {
+          const double ukp = u[k][pp], ukq = u[k][q];
+          u[k][pp] = c * ukp - sn * ukq;
+          u[k][q] = sn * ukp + c * ukq;
+        }
+      }
+  }
+  for (int k = 0; k < 6; ++k) {
+    L[k] = std::max(a[k][k], 0.0);  // P is positive semi-definite; clip round-off below zero
+    for (int i = 0; i < 6; ++i) V[i * 6 + k] = s[i] * u[i][k];
+  }
+}
+
 int make_params(const sbk_material* mat, const sbk_rule* rule, int kinematics, Params& p) {
   if (!mat || !rule) return fail(SBK_ERR_ARGUMENT, "null material or rule");
   int rc = validate_material(*mat);
@@ -265,6 +316,7 @@ int make_params(const sbk_material* mat, const sbk_rule* rule, int kinematics, P
   p.delta = mat->saturation_rate;
   rc = yield_matrix(*mat, p.P);
   if (rc) return rc;
+  yield_eigenbasis(p.P, p.PV, p.PL);
   p.general = (mat->criterion == SBK_HILL48 || mat->num_backstresses > 0) ? 1 : 0;
   p.enabled = p.sy0 > 0.0 ? 1 : 0;
   p.integration = mat->kinematic_integration;

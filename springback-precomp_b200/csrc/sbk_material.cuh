@@ -293,113 +293,119 @@ __device__ __forceinline__ bool gr_evaluate(const Params& p, const double s_tria
   return true;
 }
 
-// J (7x7) of the closest-point equations, row-major.
-__device__ __forceinline__ void gr_jacobian(const Params& p, const GPoint& e, double a_n, double dl, double J[49]) {
-  const double f = e.b / e.eq;
-#pragma unroll
-  for (int r = 0; r < 6; ++r) {
-    const double sc = r < 3 ? 1.0 : 0.5;
-#pragma unroll
-    for (int c = 0; c < 6; ++c) J[r * 7 + c] = (r == c ? 1.0 : 0.0) + f * sc * (p.P[r * 6 + c] - e.m[r] * e.m[c]);
-    const double mt = r < 3 ? e.m[r] : 0.5 * e.m[r];
-    J[r * 7 + 6] = e.back_rate[r] + e.db * mt;
-  }
-#pragma unroll
-  for (int c = 0; c < 6; ++c) J[42 + c] = e.m[c];
-  J[48] = -yield_slope_of(p, a_n + dl);
-}
+// The closest-point Jacobian (Plasticity.cpp:246-311) has the block form
+//   J = [[A, j], [m^T, -h]],  A = I + f S (P - m m^T),  f = b / sigma_bar,
+//   j = back_rate + db S m,  h = sigma_y'(a_n + dl),
+// S = diag(1, 1, 1, 1/2, 1/2, 1/2). Writing A = S (B - f m m^T) with
+// B = S^-1 + f P, and P = S^-1 V L V^T S^-1 with V^T S^-1 V = I (the
+// generalised eigenvectors of the material's constant yield matrix, found
+// once on the host), B^-1 = V (I + f L)^-1 V^T: two 6x6 products. The rank
+// one term by Sherman-Morrison and the bordered row by its Schur complement
+// then solve J [x; y] = [r; s] without pivoting or branches. This is the
+// solution the reference's partial-pivoting LU of J gives, reached by a
+// factorisation that suits the GPU (no row exchanges, 3 small products per
+// Newton step); both agree to the round-off of J's conditioning.
+struct JFactor {
+  double f;      // b / sigma_bar
+  double d[6];   // 1 / (1 + f L_k)
+  double bm[6];  // B^-1 m
+  double c;      // f / (1 - f m^T B^-1 m)
+  double aj[6];  // A^-1 j
+  double s;      // m^T A^-1 j + h
+};
 
-// In-register LU with partial pivoting of a 7x7 matrix (row swaps done by
-// predicated exchanges, so that every index stays a compile-time constant).
-__device__ __forceinline__ void lu7(double A[49], int piv[7]) {
+// out = B^-1 w = PV diag(d) PV^T w.
+__device__ __forceinline__ void b_apply(const Params& p, const JFactor& jf, const double w[6], double out[6]) {
+  double t[6];
 #pragma unroll
-  for (int k = 0; k < 7; ++k) {
-    int p = k;
-    double big = fabs(A[k * 7 + k]);
+  for (int k = 0; k < 6; ++k) {
+    double a = 0.0;
 #pragma unroll
-    for (int i = k + 1; i < 7; ++i) {
-      const double v = fabs(A[i * 7 + k]);
-      if (v > big) {
-        big = v;
-        p = i;
-      }
-    }
-    piv[k] = p;
-#pragma unroll
-    for (int i = k + 1; i < 7; ++i) {
-      if (i == p) {
-#pragma unroll
-        for (int j = 0; j < 7; ++j) {
-          const double t = A[k * 7 + j];
-          A[k * 7 + j] = A[i * 7 + j];
-          A[i * 7 + j] = t;
-        }
-      }
-    }
-    if (big != 0.0) {
-      const double inv = 1.0 / A[k * 7 + k];
-#pragma unroll
-      for (int i = k + 1; i < 7; ++i) A[i * 7 + k] *= inv;
-    }
-#pragma unroll
-    for (int i = k + 1; i < 7; ++i)
-#pragma unroll
-      for (int j = k + 1; j < 7; ++j) A[i * 7 + j] -= A[i * 7 + k] * A[k * 7 + j];
-  }
-}
-__device__ __forceinline__ void lu7_solve(const double A[49], const int piv[7], double b[7]) {
-#pragma unroll
-  for (int k = 0; k < 7; ++k) {
-#pragma unroll
-    for (int i = k + 1; i < 7; ++i) {
-      if (i == piv[k]) {
-        const double t = b[k];
-        b[k] = b[i];
-        b[i] = t;
-      }
-    }
+    for (int i = 0; i < 6; ++i) a += p.PV[i * 6 + k] * w[i];
+    t[k] = a * jf.d[k];
   }
 #pragma unroll
-  for (int i = 1; i < 7; ++i)
+  for (int i = 0; i < 6; ++i) {
+    double a = 0.0;
 #pragma unroll
-    for (int j = 0; j < i; ++j) b[i] -= A[i * 7 + j] * b[j];
-#pragma unroll
-  for (int i = 6; i >= 0; --i) {
-#pragma unroll
-    for (int j = i + 1; j < 7; ++j) b[i] -= A[i * 7 + j] * b[j];
-    b[i] /= A[i * 7 + i];
+    for (int k = 0; k < 6; ++k) a += p.PV[i * 6 + k] * t[k];
+    out[i] = a;
   }
 }
 
-// C_alg = C^e - 2G [m_t a^T + (dl / sigma_bar) S^-1 (P - m m^T) A] with
+// out = A^-1 z = (B - f m m^T)^-1 w with w = S^-1 z (Sherman-Morrison).
+__device__ __forceinline__ void a_solve(const Params& p, const JFactor& jf, const double z[6], double out[6]) {
+  double w[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) w[i] = i < 3 ? z[i] : 2.0 * z[i];
+  b_apply(p, jf, w, out);
+  double bw = 0.0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) bw += jf.bm[i] * w[i];
+  const double g = jf.c * bw;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) out[i] += g * jf.bm[i];
+}
+
+__device__ __forceinline__ void j_factor(const Params& p, const GPoint& e, double a_n, double dl, JFactor& jf) {
+  jf.f = e.b / e.eq;
+#pragma unroll
+  for (int k = 0; k < 6; ++k) jf.d[k] = 1.0 / (1.0 + jf.f * p.PL[k]);
+  b_apply(p, jf, e.m, jf.bm);
+  double mbm = 0.0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) mbm += e.m[i] * jf.bm[i];
+  jf.c = jf.f / (1.0 - jf.f * mbm);
+  double jv[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) jv[i] = e.back_rate[i] + e.db * (i < 3 ? e.m[i] : 0.5 * e.m[i]);
+  a_solve(p, jf, jv, jf.aj);
+  double maj = 0.0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) maj += e.m[i] * jf.aj[i];
+  jf.s = maj + yield_slope_of(p, a_n + dl);
+}
+
+// J [x; y] = [r; rs]: y = (m^T A^-1 r - rs) / s, x = A^-1 r - A^-1 j y.
+__device__ __forceinline__ void j_solve(const Params& p, const GPoint& e, const JFactor& jf, const double r[6], double rs,
+                                        double x[7]) {
+  double ar[6];
+  a_solve(p, jf, r, ar);
+  double mar = 0.0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) mar += e.m[i] * ar[i];
+  const double y = (mar - rs) / jf.s;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) x[i] = ar[i] - jf.aj[i] * y;
+  x[6] = y;
+}
+
+// C_alg = C^e - 2G [m_t a^T + (dl / sigma_bar) S (P - m m^T) A] with
 // [A; a^T] = J^-1 [D_dev; 0] (Plasticity.cpp:299-311).
-__device__ __forceinline__ void gr_tangent(const Params& p, const GPoint& e, double a_n, double dl, double C[36]) {
-  double J[49];
-  int piv[7];
-  gr_jacobian(p, e, a_n, dl, J);
-  lu7(J, piv);
+__device__ __noinline__ void gr_tangent(const Params& p, const GPoint& e, double a_n, double dl, double C[36]) {
+  JFactor jf;
+  j_factor(p, e, a_n, dl, jf);
   const double g = p.G;
   elastic_C(p, C);
   const double f = (dl > 0.0) ? 2.0 * g * dl / e.eq : 0.0;
 #pragma unroll 1
   for (int col = 0; col < 6; ++col) {
-    double x[7];
+    double r[6], x[7];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) x[i] = col < 3 ? (i == col ? 4.0 * g / 3.0 : -2.0 * g / 3.0) : 0.0;
+    for (int i = 0; i < 3; ++i) r[i] = col < 3 ? (i == col ? 4.0 * g / 3.0 : -2.0 * g / 3.0) : 0.0;
 #pragma unroll
-    for (int i = 3; i < 6; ++i) x[i] = (i == col) ? g : 0.0;
-    x[6] = 0.0;
-    lu7_solve(J, piv, x);
+    for (int i = 3; i < 6; ++i) r[i] = (i == col) ? g : 0.0;
+    j_solve(p, e, jf, r, 0.0, x);
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
       const double mt = i < 3 ? e.m[i] : 0.5 * e.m[i];
       double v = 2.0 * g * (mt * x[6]);
       if (dl > 0.0) {
         const double sc = i < 3 ? 1.0 : 0.5;
-        double s = 0.0;
+        double sum = 0.0;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) s += sc * (p.P[i * 6 + k] - e.m[i] * e.m[k]) * x[k];
-        v += f * s;
+        for (int k = 0; k < 6; ++k) sum += sc * (p.P[i * 6 + k] - e.m[i] * e.m[k]) * x[k];
+        v += f * sum;
       }
       C[i * 6 + col] -= v;
     }
@@ -408,13 +414,12 @@ __device__ __forceinline__ void gr_tangent(const Params& p, const GPoint& e, dou
 
 // The Newton step of the closest-point equations: J step = -R.
 __device__ __forceinline__ void gr_newton_step(const Params& p, const GPoint& e, double a_n, double dl, double step[7]) {
-  double J[49];
-  int piv[7];
-  gr_jacobian(p, e, a_n, dl, J);
-  lu7(J, piv);
+  JFactor jf;
+  j_factor(p, e, a_n, dl, jf);
+  double r[6];
 #pragma unroll
-  for (int i = 0; i < 7; ++i) step[i] = -e.res[i];
-  lu7_solve(J, piv, step);
+  for (int i = 0; i < 6; ++i) r[i] = -e.res[i];
+  j_solve(p, e, jf, r, -e.res[6], step);
 }
 
 __device__ __forceinline__ int general_return(const Params& p, const double strain[6], const PointState& st,

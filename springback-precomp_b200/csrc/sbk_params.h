@@ -30,6 +30,11 @@ struct Params {
   double sy0, H, Hkin, Q, delta;
   // Yield matrix (tensorial Voigt, global axes), row-major.
   double P[36];
+  // P = S^-1 PV diag(PL) PV^T S^-1 with PV^T S^-1 PV = I, S = diag(1, 1, 1,
+  // 1/2, 1/2, 1/2): the generalised eigenvectors (columns, row-major) and
+  // eigenvalues of the yield matrix, for the closest-point solves.
+  double PV[36];
+  double PL[6];
   // Kinematic terms of the general return (Chaboche, then Prager).
   double termC[SBK_MAX_BACKSTRESSES], termG[SBK_MAX_BACKSTRESSES];
   int nterms;       // terms stored per point (0 for the radial return)
