@@ -211,7 +211,7 @@ __device__ __forceinline__ int radial_return(const Params& p, const double strai
 struct Decay {
   double theta, chi, dtheta, dchi;
 };
-__device__ __forceinline__ Decay decay_of(double gamma, double dl, int integration) {
+__device__ __noinline__ Decay decay_of(double gamma, double dl, int integration) {
   Decay d{1.0, 0.0, 0.0, 1.0};
   if (gamma == 0.0) {
     d.chi = dl;
@@ -245,7 +245,7 @@ struct Terms {
   double a[SBK_MAX_BACKSTRESSES][6];
 };
 
-__device__ __forceinline__ bool gr_evaluate(const Params& p, const double s_trial[6], const Terms& tn,
+__device__ __noinline__ bool gr_evaluate(const Params& p, const double s_trial[6], const Terms& tn,
                                             double a_n, const double xi[6], double dl, GPoint& e) {
   double pxi[6];
 #pragma unroll
@@ -651,7 +651,7 @@ __device__ __forceinline__ void jacobi_rotate(double a[9], double v[9], int p, i
   }
 }
 
-__device__ __forceinline__ double log_div(double mx, double my) {
+__device__ __noinline__ double log_div(double mx, double my) {
   if (mx > my) {
     const double t = mx;
     mx = my;
@@ -670,7 +670,7 @@ __device__ __forceinline__ double first_of(const double f[6], int a, int b) {
   return (lo == 0 && hi == 1) ? f[3] : ((lo == 1 && hi == 2) ? f[4] : f[5]);
 }
 
-__device__ __forceinline__ double log_div2(const LogKin& L, int a, int b, int c) {
+__device__ __noinline__ double log_div2(const LogKin& L, int a, int b, int c) {
   int i = a, j = b, k = c;
   if (L.mu[i] < L.mu[j]) { const int t = i; i = j; j = t; }
   if (L.mu[j] < L.mu[k]) { const int t = j; j = k; k = t; }
