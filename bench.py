@@ -346,7 +346,7 @@ def main():
                                       "kernel": "assemble_values (K2)", "kernel_ms": asm_ms,
                                       "traffic": None},
                 "phases_ms": {"element": el_ms, "forces": statistics.mean(force_ms), "values": asm_ms},
-                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 4 * args.steps,
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": 7 * args.steps,
                 "clocks": clocks.summary(), "yielding_fraction": yielding / (8.0 * ne), "increment_s": s,
                 "setup_s": setup_s}
         print(json.dumps(line), flush=True)

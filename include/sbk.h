@@ -145,6 +145,14 @@ int sbk_system_set_stream(sbk_system* sys, void* stream);
  * default; the autotuner sets it). */
 int sbk_system_set_elements_per_block(sbk_system* sys, int elements_per_block);
 
+/* The element schedule (no counterpart in the reference, whose OpenMP loop
+ * takes the elements in mesh order): with by_cost = 1 (the default) every
+ * evaluate after the first walks the elements grouped by the cost of their
+ * last evaluation (local iterations, yielding points), so that the elements
+ * sharing a warp take alike paths; 0 keeps the mesh order. No result depends
+ * on it. */
+int sbk_system_set_schedule(sbk_system* sys, int by_cost);
+
 /* Sizes and the pattern (device pointers owned by the system). The values
  * array is the reference's column-major (CSC) layout; the pattern is
  * structurally symmetric, so the same arrays read as CSR hold K^T. */

@@ -106,6 +106,7 @@ SIGNATURES = {
     "sbk_system_destroy": (_I, [_P]),
     "sbk_system_set_stream": (_I, [_P, _P]),
     "sbk_system_set_elements_per_block": (_I, [_P, _I]),
+    "sbk_system_set_schedule": (_I, [_P, _I]),
     "sbk_system_pattern": (_I, [_P, ctypes.POINTER(sbk_pattern)]),
     "sbk_system_evaluate": (_I, [_P, _P, _D, _I, ctypes.POINTER(sbk_evaluation)]),
     "sbk_system_commit": (_I, [_P]),

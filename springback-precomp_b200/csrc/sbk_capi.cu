@@ -392,6 +392,10 @@ struct sbk_system {
   int32_t* node_ptr = nullptr;
   int32_t* node_src = nullptr;
   double* product = nullptr;  // |K| |u| per DOF (stiffness_gross)
+  int32_t* order = nullptr;    // the element schedule of the next launch
+  int32_t* sched = nullptr;    // its bucket counters
+  bool order_valid = false;
+  bool schedule = true;
   int elements_per_block = 0;
   bool has_trial = false;
   bool has_values = false;  // values hold the tangent of the last evaluate
@@ -422,7 +426,8 @@ void free_system(sbk_system* s) {
   void* ptrs[] = {s->coords, s->conn, s->committed, s->trial, s->alpha_c, s->alpha_t, s->force,
                   s->tangent, s->energy_e, s->yield, s->iters, s->code, s->first_fail, s->outer,
                   s->inner, s->values, s->internal, s->scratch, s->scalars, s->missing, s->block_col,
-                  s->block_value, s->block_ptr, s->block_src, s->node_ptr, s->node_src, s->product};
+                  s->block_value, s->block_ptr, s->block_src, s->node_ptr, s->node_src, s->product,
+                  s->order, s->sched};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : s->ev)
@@ -592,7 +597,7 @@ int sbk_element_batch(const sbk_material* material, const sbk_rule* rule, int ki
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   rc = sbk::launch_elements(p, ne, x_dev, nullptr, u_dev, state_dev, alpha_dev, tangent_dev != nullptr, force_dev,
                             tangent_dev, energy_dev, trial_dev, alpha_out_dev, yield_dev, iterations_dev, code_dev,
-                            nullptr, true, 0, s);
+                            nullptr, true, 0, nullptr, s);
   if (rc) return fail(SBK_ERR_CUDA, std::string("element kernel launch: ") + cudaGetErrorString((cudaError_t)rc));
   return SBK_OK;
 }
@@ -655,6 +660,8 @@ int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const 
   TRY(dalloc(&s->values, static_cast<size_t>(s->nnz)));
   TRY(dalloc(&s->internal, static_cast<size_t>(s->nn) * 3));
   TRY(dalloc(&s->product, static_cast<size_t>(s->nn) * 3));
+  TRY(dalloc(&s->order, static_cast<size_t>(s->ne)));
+  TRY(dalloc(&s->sched, sbk::schedule_scratch_ints()));
   TRY(dalloc(&s->scratch, sbk::assemble_scratch_doubles()));
   TRY(dalloc(&s->scalars, 4));
   TRY(dalloc(&s->missing, 1));
@@ -690,6 +697,13 @@ int sbk_system_set_stream(sbk_system* sys, void* stream) {
   return SBK_OK;
 }
 
+int sbk_system_set_schedule(sbk_system* sys, int by_cost) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  sys->schedule = by_cost != 0;
+  if (!sys->schedule) sys->order_valid = false;
+  return SBK_OK;
+}
+
 int sbk_system_set_elements_per_block(sbk_system* sys, int epb) {
   if (!sys || epb < 0 || epb > 16) return fail(SBK_ERR_ARGUMENT, "bad elements per block");
   sys->elements_per_block = epb;
@@ -717,7 +731,8 @@ int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int
   int rc = sbk::launch_elements(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c,
                                 want_tangent, sys->force, sys->tangent, sys->energy_e, sys->trial, sys->alpha_t,
                                 sys->yield, sys->iters, sys->code, sys->first_fail, false,
-                                sys->elements_per_block, st);
+                                sys->elements_per_block, sys->schedule && sys->order_valid ? sys->order : nullptr,
+                                st);
   if (rc) return fail(SBK_ERR_CUDA, std::string("element kernel: ") + cudaGetErrorString((cudaError_t)rc));
   if (sys->timing) SBK_CUDA(cudaEventRecord(sys->ev[1], st));
   // The assembly runs unconditionally; a failed element is reported after
@@ -732,6 +747,11 @@ int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int
     if (rc) return fail(SBK_ERR_CUDA, std::string("assembly: ") + cudaGetErrorString((cudaError_t)rc));
   }
   if (sys->timing) SBK_CUDA(cudaEventRecord(sys->ev[3], st));
+  if (sys->schedule) {
+    rc = sbk::launch_schedule(sys->ne, sys->p.nq, sys->iters, sys->yield, sys->sched, sys->order, st);
+    if (rc) return fail(SBK_ERR_CUDA, std::string("schedule: ") + cudaGetErrorString((cudaError_t)rc));
+    sys->order_valid = true;
+  }
   double sc[3];
   int32_t first = 0;
   SBK_CUDA(cudaMemcpyAsync(sc, sys->scalars, sizeof(sc), cudaMemcpyDeviceToHost, st));

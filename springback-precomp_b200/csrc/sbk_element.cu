@@ -983,16 +983,22 @@ __global__ void __launch_bounds__(128) element_kernel(const __grid_constant__ Pa
                                                       double* __restrict__ energy, double* __restrict__ trial,
                                                       double* __restrict__ alpha_out, uint8_t* __restrict__ yield,
                                                       int32_t* __restrict__ iterations, int32_t* __restrict__ code,
-                                                      int32_t* __restrict__ first_failure) {
+                                                      int32_t* __restrict__ first_failure,
+                                                      const int32_t* __restrict__ order) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int epb = blockDim.x / G;
   const int slot_in_block = threadIdx.x / G;
   const int lane = threadIdx.x % G;
-  const int64_t e = (int64_t)blockIdx.x * epb + slot_in_block;
+  const int64_t slot = (int64_t)blockIdx.x * epb + slot_in_block;
   ElemShared<G>* sh = reinterpret_cast<ElemShared<G>*>(smem_raw) + slot_in_block;
   const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
   const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
-  if (e >= ne) return;  // whole groups leave together
+  if (slot >= ne) return;  // whole groups leave together
+  // The element of this slot: the schedule's order (elements of alike cost
+  // side by side, so that the groups sharing a warp take alike paths), or
+  // the mesh order. Every output is indexed by the element, so the order
+  // changes no result.
+  const int64_t e = order ? (int64_t)order[slot] : slot;
   double hu_lane[9];
   Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, trial, yield, hu_lane};
   ElemShared<G>& s = *sh;
@@ -1162,7 +1168,7 @@ template <int G>
 int launch_g(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
              const double* state, const double* alpha_n, int want_tangent, double* force, double* tangent,
              double* energy, double* trial, double* alpha_out, uint8_t* yield, int32_t* iterations, int32_t* code,
-             int32_t* first_failure, bool batch, int epb, cudaStream_t stream) {
+             int32_t* first_failure, bool batch, int epb, const int32_t* order, cudaStream_t stream) {
   const int threads = epb * G;
   const size_t smem = sizeof(ElemShared<G>) * epb;
   const int64_t blocks = (ne + epb - 1) / epb;
@@ -1172,7 +1178,7 @@ int launch_g(const Params& p, int64_t ne, const double* coords, const int32_t* c
   if (err != cudaSuccess) return (int)err;
   kern<<<(unsigned)blocks, threads, smem, stream>>>(p, ne, batch, coords, conn, u, state, alpha_n, want_tangent,
                                                      force, tangent, energy, trial, alpha_out, yield, iterations,
-                                                     code, first_failure);
+                                                     code, first_failure, order);
   return (int)cudaGetLastError();
 }
 
@@ -1191,16 +1197,16 @@ int launch_elements(const Params& p, int64_t ne, const double* coords, const int
                     const double* state, const double* alpha_n, int want_tangent, double* force, double* tangent,
                     double* energy, double* trial, double* alpha_out, uint8_t* yield, int32_t* iterations,
                     int32_t* code, int32_t* first_failure, bool batch, int elements_per_block,
-                    cudaStream_t stream) {
+                    const int32_t* order, cudaStream_t stream) {
   if (p.nq <= 8) {
     const int epb = elements_per_block > 0 ? elements_per_block : 4;
     return launch_g<8>(p, ne, coords, conn, u, state, alpha_n, want_tangent, force, tangent, energy, trial,
-                       alpha_out, yield, iterations, code, first_failure, batch, epb, stream);
+                       alpha_out, yield, iterations, code, first_failure, batch, epb, order, stream);
   }
 #ifdef SBK_WIDE_RULES
   const int epb = elements_per_block > 0 ? elements_per_block : 1;
   return launch_g<32>(p, ne, coords, conn, u, state, alpha_n, want_tangent, force, tangent, energy, trial,
-                      alpha_out, yield, iterations, code, first_failure, batch, epb, stream);
+                      alpha_out, yield, iterations, code, first_failure, batch, epb, order, stream);
 #else
   return -1;  // rules of more than 8 points: not in this build
 #endif

@@ -18,13 +18,13 @@ int set_error(int code, const std::string& what);
 // allocation).
 int make_launch_params(const sbk_material* material, const sbk_rule* rule, int kinematics, Params& p);
 
-// K1: ne elements. Mesh mode (batch = false): coords 3 per node, conn 8 per
+// K1: ne elements (slot i evaluates element order[i]; order NULL: i). Mesh mode (batch = false): coords 3 per node, conn 8 per
 // element, u 3 per node. Batch mode: coords and u hold 24 per element.
 int launch_elements(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
                     const double* state, const double* alpha_n, int want_tangent, double* force, double* tangent,
                     double* energy, double* trial, double* alpha_out, uint8_t* yield, int32_t* iterations,
                     int32_t* code, int32_t* first_failure, bool batch, int elements_per_block,
-                    cudaStream_t stream);
+                    const int32_t* order, cudaStream_t stream);
 size_t element_smem_bytes(int group);
 
 // The gather maps of the assembly (built once on the host).
@@ -57,6 +57,12 @@ size_t assemble_scratch_doubles();
 int launch_stiffness_gross(int64_t nn, const int32_t* outer, const int32_t* inner, const double* values,
                            const double* u, int32_t num_free, const int32_t* free_dofs, double* product,
                            double* scratch, double* scalars, cudaStream_t stream);
+// The schedule of the next element launch: the elements bucketed by the
+// cost of their last evaluation (local iterations, yielding points), so
+// that elements of alike cost share a warp. scratch: schedule_scratch_ints().
+int launch_schedule(int64_t ne, int nq, const int32_t* iterations, const uint8_t* yield, int32_t* scratch,
+                    int32_t* order, cudaStream_t stream);
+size_t schedule_scratch_ints();
 // add_node_block for n blocks, in list order.
 int launch_add_node_blocks(const int32_t* outer, const int32_t* inner, double* values, int32_t n,
                            const int32_t* nodes, const double* blocks, int32_t* missing, cudaStream_t stream);

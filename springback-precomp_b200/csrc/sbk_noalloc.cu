@@ -153,7 +153,7 @@ extern "C" int sbk_evaluate_noalloc(const sbk_material* material, const sbk_rule
   if (err != cudaSuccess) return sbk::set_error(SBK_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(err));
   rc = sbk::launch_elements(p, num_elements, coords_dev, connectivity_dev, u_dev, state_dev, alpha_dev,
                             values_dev != nullptr, s->force, s->tangent, s->energy, trial_dev, alpha_out_dev,
-                            yield_dev, s->iterations, s->code, &s->first_failure, false, 0, st);
+                            yield_dev, s->iterations, s->code, &s->first_failure, false, 0, nullptr, st);
   if (rc) return sbk::set_error(SBK_ERR_CUDA, std::string("element kernel: ") + cudaGetErrorString((cudaError_t)rc));
   scatter_small_kernel<<<1, 576, 0, st>>>(num_nodes, num_elements, p.nq, connectivity_dev, outer_dev, inner_dev, nnz,
                                           s, s->gross, internal_dev, values_dev, yield_dev, summary_dev);

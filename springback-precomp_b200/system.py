@@ -204,6 +204,11 @@ class NonlinearSystem:
     def set_stream(self, stream=None):
         _capi.check(_capi.lib().sbk_system_set_stream(self._h, _stream_ptr(stream)))
 
+    def set_schedule(self, by_cost: bool = True):
+        """Walk the elements grouped by the cost of their last evaluation (the
+        default) or in mesh order; no result depends on it."""
+        _capi.check(_capi.lib().sbk_system_set_schedule(self._h, 1 if by_cost else 0))
+
     def set_elements_per_block(self, epb: int):
         _capi.check(_capi.lib().sbk_system_set_elements_per_block(self._h, int(epb)))
 

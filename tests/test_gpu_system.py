@@ -137,3 +137,23 @@ def test_stiffness_gross_is_the_reference_norm(pkg, orc, problem, cuda):
     with pytest.raises(pkg.SbkError):
         fresh = make_system(pkg, problem)
         fresh.stiffness_gross(u, torch.tensor(free, device=cuda))
+
+
+def test_schedule_changes_no_result(pkg, problem, cuda):
+    """The element schedule (elements grouped by the cost of their last
+    evaluation) reorders only which warp evaluates which element: two
+    evaluations with it equal, bit for bit, the same two in mesh order."""
+    u = torch.tensor(problem.u, device=cuda)
+    outs = []
+    for by_cost in (False, True):
+        sys_ = make_system(pkg, problem)
+        sys_.set_schedule(by_cost)
+        for _ in range(2):  # the second evaluation runs on the schedule of the first
+            ev = sys_.evaluate(u, 0.0, True)
+        outs.append((ev.internal.clone(), ev.tangent.clone(), ev.energy, ev.gross,
+                     torch.tensor(sys_.trial_states()), torch.tensor(sys_.trial_modes())))
+    for a, b in zip(*outs):
+        if isinstance(a, torch.Tensor):
+            assert torch.equal(a, b)
+        else:
+            assert a == b
