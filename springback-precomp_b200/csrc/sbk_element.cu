@@ -195,7 +195,8 @@ struct Ctx {
   const double* state;
   double* trial;
   uint8_t* yield;
-  double* hu;  // this lane's U G^T (per-lane memory)
+  double* hu;    // this lane's U G^T (per-lane memory)
+  double* warm;  // this lane's last converged closest point (general return)
   __device__ __forceinline__ void sync() const { __syncwarp(mask); }
 };
 
@@ -353,7 +354,7 @@ __device__ __noinline__ int pass(const Ctx<G>& c, const double at[9]) {
     if (!fail) {
       PointState st{c.state + c.e * p.nq + q, c.trial + c.e * p.nq + q, c.npts};
       Response r;
-      code = p.general ? general_return(p, strain, st, r) : radial_return(p, strain, st, r);
+      code = p.general ? general_return(p, strain, st, r, c.warm) : radial_return(p, strain, st, r);
       if (code) {
         fail = (2 << 8) | q;
       } else {
@@ -1000,7 +1001,9 @@ __global__ void __launch_bounds__(128) element_kernel(const __grid_constant__ Pa
   // changes no result.
   const int64_t e = order ? (int64_t)order[slot] : slot;
   double hu_lane[9];
-  Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, trial, yield, hu_lane};
+  double warm_lane[8];
+  warm_lane[7] = 0.0;  // no closest point yet
+  Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, trial, yield, hu_lane, warm_lane};
   ElemShared<G>& s = *sh;
   // Stage the element's coordinates and displacements (lane a: node a).
   if (lane < 8) {

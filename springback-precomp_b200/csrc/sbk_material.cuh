@@ -422,8 +422,15 @@ __device__ __forceinline__ void gr_newton_step(const Params& p, const GPoint& e,
   j_solve(p, e, jf, r, -e.res[6], step);
 }
 
+// warm: the point's last converged closest point (xi 6, dl, valid flag) in
+// this element's local iteration, or NULL. The Newton iteration starts from
+// whichever of it and the trial state has the smaller residual; the converged
+// point is the same either way (to the return's tolerance), and from within
+// one local iteration the warm start takes fewer steps. If a warm start does
+// not converge, the return runs again from the trial state, as the
+// reference's always does.
 __device__ __forceinline__ int general_return(const Params& p, const double strain[6], const PointState& st,
-                                           Response& out) {
+                                           Response& out, double* warm = nullptr) {
   const double g = p.G, k = p.K;
   const int nt = p.nterms;
   double ep[6], el[6], s_trial[6];
@@ -495,12 +502,6 @@ __device__ __forceinline__ int general_return(const Params& p, const double stra
     st.put(field_loading(nt), loading ? 1.0 : 0.0);
     return 0;
   }
-  double xi[6];
-#pragma unroll
-  for (int i = 0; i < 6; ++i) xi[i] = xi_tr[i];
-  double dl = 0.0;
-  GPoint e;
-  gr_evaluate(p, s_trial, tn, a_n, xi, dl, e);
   double scale = sy_n;
 #pragma unroll
   for (int i = 0; i < 6; ++i) scale = fmax(scale, fmax(fabs(s_trial[i]), fabs(xi_tr[i])));
@@ -518,37 +519,58 @@ __device__ __forceinline__ int general_return(const Params& p, const double stra
     for (int i = 0; i < 7; ++i) s += x.res[i] * x.res[i];
     return sqrt(s);
   };
+  double xi[6], dl = 0.0;
+  GPoint e;
   bool converged = false;
-  for (int it = 0; it < 50; ++it) {
-    const double r_inf = rinf(e);
-    if (r_inf <= tol) {
-      converged = true;
-      break;
+  // Attempt 0 starts warm (when that start has the smaller residual),
+  // attempt 1 from the trial state (Plasticity.cpp:353-430).
+  for (int attempt = (warm != nullptr && warm[7] != 0.0) ? 0 : 1; attempt < 2 && !converged; ++attempt) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) xi[i] = xi_tr[i];
+    dl = 0.0;
+    gr_evaluate(p, s_trial, tn, a_n, xi, dl, e);
+    if (attempt == 0) {
+      double xw[6];
+#pragma unroll
+      for (int i = 0; i < 6; ++i) xw[i] = warm[i];
+      GPoint ew;
+      if (!gr_evaluate(p, s_trial, tn, a_n, xw, warm[6], ew) || !(rnorm(ew) < rnorm(e))) continue;
+#pragma unroll
+      for (int i = 0; i < 6; ++i) xi[i] = xw[i];
+      dl = warm[6];
+      e = ew;
     }
-    double step[7];
-    gr_newton_step(p, e, a_n, dl, step);
-    const double r0 = rnorm(e);
-    double t = 1.0;
-    bool accepted = false;
-    for (int ls = 0; ls < 40; ++ls) {
-      double xt[6];
-#pragma unroll
-      for (int i = 0; i < 6; ++i) xt[i] = xi[i] + t * step[i];
-      const double dlt = fmax(dl + t * step[6], 0.0);
-      GPoint tr;
-      if (gr_evaluate(p, s_trial, tn, a_n, xt, dlt, tr) && rnorm(tr) <= (1.0 - 1.0e-4 * t) * r0) {
-#pragma unroll
-        for (int i = 0; i < 6; ++i) xi[i] = xt[i];
-        dl = dlt;
-        e = tr;
-        accepted = true;
+    for (int it = 0; it < 50; ++it) {
+      const double r_inf = rinf(e);
+      if (r_inf <= tol) {
+        converged = true;
         break;
       }
-      t *= 0.5;
-    }
-    if (!accepted) {
-      converged = r_inf <= 4.0 * tol;
-      break;
+      double step[7];
+      gr_newton_step(p, e, a_n, dl, step);
+      const double r0 = rnorm(e);
+      double t = 1.0;
+      bool accepted = false;
+      for (int ls = 0; ls < 40; ++ls) {
+        double xt[6];
+#pragma unroll
+        for (int i = 0; i < 6; ++i) xt[i] = xi[i] + t * step[i];
+        const double dlt = fmax(dl + t * step[6], 0.0);
+        GPoint tr;
+        if (gr_evaluate(p, s_trial, tn, a_n, xt, dlt, tr) && rnorm(tr) <= (1.0 - 1.0e-4 * t) * r0) {
+#pragma unroll
+          for (int i = 0; i < 6; ++i) xi[i] = xt[i];
+          dl = dlt;
+          e = tr;
+          accepted = true;
+          break;
+        }
+        t *= 0.5;
+      }
+      if (!accepted) {
+        converged = r_inf <= 4.0 * tol;
+        break;
+      }
     }
   }
   if (!converged) return kFailReturn;
@@ -567,6 +589,12 @@ __device__ __forceinline__ int general_return(const Params& p, const double stra
       dl = dlp;
       e = po;
     }
+  }
+  if (warm != nullptr) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) warm[i] = xi[i];
+    warm[6] = dl;
+    warm[7] = 1.0;
   }
   out.yielding = true;
 #pragma unroll
