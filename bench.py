@@ -36,6 +36,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 PKG = "springback-precomp_b200"
 METRIC = "Hex8 tangent+residual+assembly elem/s (FP64)"
+# DRAM bytes (read + write) per element of one element-kernel launch, from
+# the ncu capture of the same construction at 80,000 elements
+# (profiles/element_kernel_microbench.md: 29.16 GB / 80,000); the traffic
+# grows with the elements, so a launch of ne elements moves about ne times
+# this.
+K1_DRAM_BYTES_PER_ELEMENT = 29.16e9 / 80000
 UNIT = "elem/s"
 
 
@@ -327,7 +333,10 @@ def main():
         if flops_per_element:
             achieved = flops_per_element * ne / (el_ms / 1e3) / 1e12
             roofline = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                        "frac": achieved / fp64_peak, "traffic": None,
+                        "frac": achieved / fp64_peak, "traffic": K1_DRAM_BYTES_PER_ELEMENT * ne,
+                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one element_kernel "
+                                          "launch on the 200x200x2 case, scaled by elements "
+                                          "(profiles/element_kernel_microbench.md)",
                         "kernel": "element_kernel (K1)", "kernel_ms": el_ms,
                         "flops_per_element": flops_per_element,
                         "peak_source": "measured in this run: cuBLAS FP64 GEMM 8192^3 burst (FP64 has no entry in "
