@@ -1188,12 +1188,7 @@ int launch_g(const Params& p, int64_t ne, const double* coords, const int32_t* c
 }  // namespace
 
 size_t element_smem_bytes(int group) {
-  if (group == 8) return sizeof(ElemShared<8>);
-#ifdef SBK_WIDE_RULES
-  return sizeof(ElemShared<32>);
-#else
-  return 0;
-#endif
+  return group == 8 ? sizeof(ElemShared<8>) : sizeof(ElemShared<32>);
 }
 
 int launch_elements(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
@@ -1206,13 +1201,11 @@ int launch_elements(const Params& p, int64_t ne, const double* coords, const int
     return launch_g<8>(p, ne, coords, conn, u, state, alpha_n, want_tangent, force, tangent, energy, trial,
                        alpha_out, yield, iterations, code, first_failure, batch, epb, order, stream);
   }
-#ifdef SBK_WIDE_RULES
-  const int epb = elements_per_block > 0 ? elements_per_block : 1;
+  // Rules of 9 to 32 points (the sheet rules 2 x 2 x 3..7, the 3 x 3 x 3
+  // cube): a warp per element, lane = point.
+  const int epb = elements_per_block > 0 ? (elements_per_block < 4 ? elements_per_block : 4) : 1;
   return launch_g<32>(p, ne, coords, conn, u, state, alpha_n, want_tangent, force, tangent, energy, trial,
                       alpha_out, yield, iterations, code, first_failure, batch, epb, order, stream);
-#else
-  return -1;  // rules of more than 8 points: not in this build
-#endif
 }
 
 }  // namespace sbk

@@ -31,12 +31,13 @@ def material(pkg, law):
             "hill_chaboche": m.hill_chaboche_sheet, "perfect": m.perfectly_plastic}[law]()
 
 
-def run_gpu(pkg, mat, X, ue, state_dev, alpha, kin, cuda, want_tangent=True):
+def run_gpu(pkg, mat, X, ue, state_dev, alpha, kin, cuda, want_tangent=True, rule=(2, 0)):
     x = torch.tensor(np.asarray(X).reshape(-1, 24), device=cuda)
     u = torch.tensor(np.asarray(ue).reshape(-1, 24), device=cuda)
     st = torch.tensor(np.ascontiguousarray(state_dev), device=cuda) if state_dev is not None else None
     al = torch.tensor(np.asarray(alpha).reshape(-1, 9), device=cuda) if alpha is not None else None
-    r = pkg.element_batch(mat, x, u, st, al, kinematics=kin, want_tangent=want_tangent)
+    r = pkg.element_batch(mat, x, u, st, al, kinematics=kin, want_tangent=want_tangent, stiffness_points=rule[0],
+                          thickness_points=rule[1])
     torch.cuda.synchronize()
     return r
 
@@ -167,3 +168,56 @@ def test_deterministic(pkg, cuda):
     a = run_gpu(pkg, mat, X, ue, None, None, "logarithmic", cuda)
     b = run_gpu(pkg, mat, X, ue, None, None, "logarithmic", cuda)
     assert torch.equal(a.force, b.force) and torch.equal(a.tangent, b.tangent)
+
+
+RULES = [(2, 3), (2, 5), (2, 7), (3, 0)]
+
+
+@pytest.mark.parametrize("rule", RULES, ids=lambda r: f"{r[0]}x{r[0]}x{r[1] or r[0]}")
+@pytest.mark.parametrize("law", ["j2", "hill", "chaboche"])
+def test_rules_beyond_eight_points(pkg, orc, cuda, law, rule):
+    """The sheet rules with thickness points (2 x 2 x 3, 5, 7: 12 to 28
+    points, the production rule being 2 x 2 x 5) and the 3 x 3 x 3 cube, a
+    warp per element: the reference's condensed-tangent case
+    (test_incompatible_modes.cpp:433-508) under logarithmic strain."""
+    mat = material(pkg, law)
+    X = X_DISTORTED.reshape(1, 24)
+    kw = dict(kinematics="logarithmic", in_plane=rule[0], thickness=rule[1])
+    first = orc.elements(mat.as_dict(), X, deformation(X_DISTORTED, 0.1).reshape(1, 24), want_tangent=False, **kw)
+    ue = deformation(X_DISTORTED, 0.13)
+    for a in range(8):
+        ue[3 * a + 2] += 0.02 * X_DISTORTED[a, 0] * X_DISTORTED[a, 1]
+    ref = orc.elements(mat.as_dict(), X, ue.reshape(1, 24), first["states"], first["alpha"], **kw)
+    nt = mat.kinematic_terms
+    r = run_gpu(pkg, mat, X, ue, oracle_to_device(first["states"], nt), first["alpha"], "logarithmic", cuda,
+                rule=rule)
+    compare(ref, r, nt)
+    assert int(r.yielding.sum()) == orc.rule_size(*rule, 2)
+
+
+@pytest.mark.parametrize("law", ["perfect", "j2", "chaboche", "hill"])
+@pytest.mark.parametrize("tp", [5, 7])
+@pytest.mark.parametrize("factor", [-6.0, -10.0, -15.0])
+def test_reversal_with_thickness_points(pkg, orc, cuda, law, tp, factor):
+    """Reversals of 6 to 15 times a 2 % logarithmic strain with 5 and 7
+    thickness points (test_incompatible_modes.cpp:549-595), where K_aa turns
+    indefinite and the shifted and Levenberg-Marquardt steps act."""
+    mat = material(pkg, law)
+    X = X_DISTORTED.reshape(1, 24)
+    kw = dict(kinematics="logarithmic", in_plane=2, thickness=tp)
+    first = orc.elements(mat.as_dict(), X, deformation(X_DISTORTED, 0.02).reshape(1, 24), want_tangent=False, **kw)
+    ue = deformation(X_DISTORTED, factor * 0.02)
+    ref = orc.elements(mat.as_dict(), X, ue.reshape(1, 24), first["states"], first["alpha"], **kw)
+    assert ref["status"][0] == 0
+    nt = mat.kinematic_terms
+    r = run_gpu(pkg, mat, X, ue, oracle_to_device(first["states"], nt), first["alpha"], "logarithmic", cuda,
+                rule=(2, tp))
+    compare(ref, r, nt, tol_k=1e-9, tol_f=1e-9)
+
+
+def test_rules_beyond_thirty_two_points_are_refused(pkg, cuda):
+    mat = pkg.material.j2_steel()
+    X = torch.tensor(X_DISTORTED.reshape(1, 24), device=cuda)
+    with pytest.raises(pkg.SbkError) as e:
+        pkg.element_batch(mat, X, torch.zeros_like(X), stiffness_points=4)  # 64 points
+    assert e.value.status == 6

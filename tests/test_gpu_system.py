@@ -157,3 +157,29 @@ def test_schedule_changes_no_result(pkg, problem, cuda):
             assert torch.equal(a, b)
         else:
             assert a == b
+
+
+def test_production_rule_system(pkg, orc, cuda):
+    """A sheet with the production rule 2 x 2 x 5 (20 points per element;
+    python/precomp/fea/setup.py:142-144), Hill48 + Chaboche, logarithmic
+    strain, from virgin points: the system's f_int and assembled tangent
+    against the oracle's."""
+    mesh = pkg.structured_hex_mesh(8, 4, 1, 4e-3, 2e-3, 1e-3)
+    mat = pkg.material.hill_chaboche_sheet()
+    x = mesh.coords
+    u = np.zeros_like(x)
+    u[:, 2] = -0.005 * (x[:, 0] - x[:, 0].mean()) ** 2 / 4e-3  # bending: the outer points of the rule yield
+    u[:, 0] = 0.0005 * (x[:, 2] - x[:, 2].mean()) * (x[:, 0] - x[:, 0].mean()) / 4e-3
+    u = u.reshape(-1)
+    sys_ = pkg.NonlinearSystem(mesh, mat, kinematics="logarithmic", thickness_points=5)
+    assert sys_.nq == 20
+    ev = sys_.evaluate(torch.tensor(u, device=cuda), 0.0, True)
+    ref = orc.system_evaluate(mat.as_dict(), mesh.coords, mesh.connectivity, u, kinematics="logarithmic",
+                              in_plane=2, thickness=5)
+    assert ref["code"] == 0
+    assert 0 < ref["yielding_points"] < 20 * mesh.num_elements
+    assert ev.yielding_points == ref["yielding_points"]
+    f = ev.internal.cpu().numpy()
+    assert np.abs(f - ref["internal"]).max() <= 1e-11 * ref["gross"]
+    v = ev.tangent.cpu().numpy()
+    assert np.linalg.norm(v - ref["values"]) <= 1e-11 * np.linalg.norm(ref["values"])
