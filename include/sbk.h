@@ -218,6 +218,19 @@ int sbk_system_plastic(const sbk_system* sys);
 int sbk_system_add_node_blocks(sbk_system* sys, int32_t n, const int32_t* nodes_dev,
                                const double* blocks_dev);
 
+/* Stress recovery at the end of a step: elastoplastic_stress for every
+ * element (IncompatibleModes.cpp:602-664, as the forming driver calls it at
+ * Forming.cpp:1266-1281) at the displacement u_dev (num_dofs, device), from
+ * the committed points and modes - call it after sbk_system_commit. out_dev
+ * (device) receives 28 doubles per element: the point averages of the Cauchy
+ * stress (6) and the second Piola-Kirchhoff stress (6), the von Mises stress
+ * of the average Cauchy stress, the largest accumulated plastic strain, the
+ * largest strain component, the smallest det F, the averages of the
+ * Kirchhoff stress (6) and of the log strain (6, tensor components; zero
+ * unless logarithmic). SBK_ERR_SOLVER names the lowest failing element.
+ * The trial state of the last evaluate is overwritten. */
+int sbk_system_stress(sbk_system* sys, const double* u_dev, double* out_dev);
+
 /* stiffness_gross(K, u, free) (NonlinearSystem.hpp:49-67): the norm over the
  * free DOFs of |K| |u|, with K the tangent values of the last evaluate (with
  * any node blocks added since) and u_dev the displacement (num_dofs, device);

@@ -50,6 +50,7 @@ def _declare(L):
     L.orc_log_strain.argtypes = [_d, _d, _d, _d, _d, _d]
     L.orc_elements.argtypes = ([_d] + [ctypes.c_int] * 4 + [_ll, _d, _d, _d, _d, ctypes.c_int, ctypes.c_int]
                                + [_d, _d, _d, _d, _d, _i, _i, _i, ctypes.c_void_p])
+    L.orc_element_stress.argtypes = [_d] + [ctypes.c_int] * 4 + [_ll, _d, _d, _d, _d, ctypes.c_int, _d, _i]
     L.orc_count_flops.restype = _ll
     L.orc_count_flops.argtypes = [_d] + [ctypes.c_int] * 4 + [_ll, _d, _d, _d, _d, ctypes.c_int]
     L.orc_pattern_nnz.restype = _ll
@@ -177,6 +178,27 @@ def elements(m: dict, X, ue, committed=None, alpha_n=None, kinematics="logarithm
                        _p(y, _i), _p(it, _i), _p(st, _i), yf.ctypes.data_as(ctypes.c_void_p))
     return dict(force=f, tangent=K, energy=energy, states=trial, alpha=alpha, yielding=y, iterations=it, status=st,
                 yield_flags=yf.astype(bool))
+
+
+def element_stress(m: dict, X, ue, committed=None, alpha=None, kinematics="logarithmic", in_plane=2, thickness=0,
+                   axis=2, threads=0):
+    """incompatible_elastoplastic_stress (IncompatibleModes.cpp:602-664) of
+    a batch: (ne, 28) - Cauchy 6, second Piola-Kirchhoff 6, von Mises, max
+    eqps, max strain, min det F, Kirchhoff 6, log strain 6 - and a status
+    per element."""
+    rec = material_record(m)
+    X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 24)
+    ne = X.shape[0]
+    ue = np.ascontiguousarray(ue, dtype=np.float64).reshape(ne, 24)
+    nq = lib().orc_rule_size(in_plane, thickness, axis)
+    committed = (np.zeros((ne, nq, NF)) if committed is None
+                 else np.ascontiguousarray(committed, dtype=np.float64).reshape(ne, nq, NF))
+    out = np.zeros((ne, 28))
+    st = np.zeros(ne, dtype=np.int32)
+    al = None if alpha is None else np.ascontiguousarray(alpha, dtype=np.float64).reshape(ne, 9)
+    lib().orc_element_stress(_p(rec), in_plane, thickness, axis, KIN[kinematics], ne, _p(X), _p(ue), _p(committed),
+                             _p(al) if al is not None else None, threads, _p(out), _p(st, _i))
+    return out, st
 
 
 def count_flops(m: dict, X, ue, committed=None, alpha_n=None, kinematics="logarithmic", in_plane=2, thickness=0,

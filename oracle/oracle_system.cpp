@@ -299,6 +299,45 @@ int orc_elements(const double* material, int in_plane, int thickness, int axis, 
   return static_cast<int>(failed);
 }
 
+/// incompatible_elastoplastic_stress (IncompatibleModes.cpp:602-664) for a
+/// batch: 28 doubles per element - Cauchy 6, second Piola-Kirchhoff 6, von
+/// Mises, max eqps, max strain, min det F, Kirchhoff 6, log strain 6.
+int orc_element_stress(const double* material, int in_plane, int thickness, int axis, int kinematics,
+                       long long ne, const double* X, const double* ue, const double* committed,
+                       const double* alpha, int threads, double* out, int* status) {
+  Material mat;
+  if (!make_material(material, mat)) return -1;
+  const std::vector<QPoint> rule = hex8_rule(in_plane, thickness, axis);
+  const int nq = static_cast<int>(rule.size());
+  const int nt = set_threads(threads);
+  long long failed = 0;
+#pragma omp parallel for schedule(static) num_threads(nt) reduction(+ : failed)
+  for (long long e = 0; e < ne; ++e) {
+    IMElement<double> el(mat, rule, kinematics);
+    std::vector<State<double>> c(static_cast<std::size_t>(nq));
+    for (int q = 0; q < nq; ++q) c[q] = load_state<double>(committed + (e * nq + q) * kNF);
+    try {
+      const ElementStress st = el.stress(X + e * 24, ue + e * 24, c, alpha ? alpha + e * 9 : nullptr);
+      double* o = out + e * 28;
+      for (int i = 0; i < 6; ++i) {
+        o[i] = st.cauchy[i];
+        o[6 + i] = st.piola_kirchhoff[i];
+        o[16 + i] = st.kirchhoff[i];
+        o[22 + i] = st.log_strain[i];
+      }
+      o[12] = st.von_mises;
+      o[13] = st.max_eqps;
+      o[14] = st.max_strain;
+      o[15] = st.min_jacobian;
+      status[e] = 0;
+    } catch (const Failure& f) {
+      status[e] = f.code;
+      ++failed;
+    }
+  }
+  return static_cast<int>(failed);
+}
+
 /// The algorithmic flop count of the same batch (counting scalar, one
 /// thread): +, -, *, / and each sqrt/log1p/exp/expm1 count one.
 long long orc_count_flops(const double* material, int in_plane, int thickness, int axis,

@@ -872,6 +872,29 @@ int sbk_system_add_node_blocks(sbk_system* sys, int32_t n, const int32_t* nodes_
   return SBK_OK;
 }
 
+int sbk_system_stress(sbk_system* sys, const double* u_dev, double* out_dev) {
+  if (!sys || !u_dev || !out_dev) return fail(SBK_ERR_ARGUMENT, "null argument");
+  cudaStream_t st = sys->stream;
+  SBK_CUDA(cudaMemsetAsync(sys->first_fail, 0x7f, sizeof(int32_t), st));
+  // The returns reproduce the committed states into the trial buffer, which
+  // the last evaluate's trial state no longer occupies after a commit.
+  sys->has_trial = false;
+  int rc = sbk::launch_stress(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c, sys->trial,
+                              out_dev, sys->code, sys->first_fail, st);
+  if (rc) return fail(SBK_ERR_CUDA, std::string("stress kernel: ") + cudaGetErrorString((cudaError_t)rc));
+  int32_t first = 0;
+  SBK_CUDA(cudaMemcpyAsync(&first, sys->first_fail, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  SBK_CUDA(cudaStreamSynchronize(st));
+  if (first != 0x7f7f7f7f) {
+    int32_t code = 0;
+    SBK_CUDA(cudaMemcpy(&code, sys->code + first, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    char buf[160];
+    std::snprintf(buf, sizeof(buf), "Hex8 element %d: SolverError in stress recovery (code %d)", first, code);
+    return fail(SBK_ERR_SOLVER, buf);
+  }
+  return SBK_OK;
+}
+
 int sbk_system_stiffness_gross(sbk_system* sys, const double* u_dev, int32_t num_free, const int32_t* free_dev,
                                double* out) {
   if (!sys || !u_dev || !out || num_free < 0 || (num_free > 0 && !free_dev))

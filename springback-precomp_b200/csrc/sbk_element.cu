@@ -1167,6 +1167,231 @@ __global__ void __launch_bounds__(128) element_kernel(const __grid_constant__ Pa
   for (int i = lane; i < 9; i += G) alpha_out[e * 9 + i] = s.alpha[i];
 }
 
+// Stress recovery at the end of a step (incompatible_elastoplastic_stress,
+// IncompatibleModes.cpp:602-664, called for every element by the forming
+// driver, Forming.cpp:1266-1281): the kinematics at the committed modes
+// without a local iteration, every point's return from its committed state
+// (an elastic check that reproduces it), and per element the point averages
+// of the Cauchy, second Piola-Kirchhoff and Kirchhoff stresses and the log
+// strain, the von Mises stress of the average Cauchy stress, the largest
+// accumulated plastic strain and strain component and the smallest det F.
+// The point values go through shared memory and lane 0 sums them in point
+// order, as the reference does. out: 28 per element (cauchy 6, pk2 6, von
+// Mises, max eqps, max strain, min det F, kirchhoff 6, log strain 6).
+template <int G>
+__global__ void __launch_bounds__(128) stress_kernel(const __grid_constant__ Params p, int64_t ne,
+                                                     const double* __restrict__ coords,
+                                                     const int32_t* __restrict__ conn, const double* __restrict__ u,
+                                                     const double* __restrict__ state,
+                                                     const double* __restrict__ alpha_n, double* __restrict__ scratch,
+                                                     double* __restrict__ out, int32_t* __restrict__ code,
+                                                     int32_t* __restrict__ first_failure) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int epb = blockDim.x / G;
+  const int slot_in_block = threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  const int64_t e = (int64_t)blockIdx.x * epb + slot_in_block;
+  ElemShared<G>* sh = reinterpret_cast<ElemShared<G>*>(smem_raw) + slot_in_block;
+  const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+  const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
+  if (e >= ne) return;
+  double hu_lane[9];
+  Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, scratch, nullptr, hu_lane, nullptr};
+  ElemShared<G>& s = *sh;
+  if (lane < 8) {
+    const int64_t node = conn[e * 8 + lane];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      s.X[3 * lane + k] = coords[node * 3 + k];
+      s.U[3 * lane + k] = u[node * 3 + k];
+    }
+  }
+  for (int i = lane; i < 9; i += G) s.alpha[i] = alpha_n ? alpha_n[e * 9 + i] : 0.0;
+  c.sync();
+  int status = set_up<G>(c);
+  if (status) {
+    if (lane == 0) {
+      code[e] = status;
+      atomicMin(first_failure, (int32_t)e);
+    }
+    return;
+  }
+  const int q = lane;
+  int fail = 0, fcode = 0;
+  if (q < p.nq) {
+    double gt[9], h[9], F[9];
+    mode_grads(c, q, gt);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) {
+        double v = c.hu[i * 3 + j];
+#pragma unroll
+        for (int m = 0; m < 3; ++m) v += s.alpha[3 * m + i] * gt[j * 3 + m];
+        h[i * 3 + j] = v;
+      }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) F[i] = h[i] + ((i % 4) == 0 ? 1.0 : 0.0);
+    double sym[9];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) sym[i * 3 + j] = 0.5 * (h[i * 3 + j] + h[j * 3 + i]);
+    double strain[6];
+    LogKin L;
+    if (p.kinematics == SBK_SMALL_STRAIN) {
+      strain[0] = h[0];
+      strain[1] = h[4];
+      strain[2] = h[8];
+      strain[3] = h[1] + h[3];
+      strain[4] = h[5] + h[7];
+      strain[5] = h[6] + h[2];
+    } else {
+      double E[9];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          E[i * 3 + j] = 0.5 * (h[i * 3 + j] + h[j * 3 + i] + h[0 * 3 + i] * h[0 * 3 + j] +
+                                h[1 * 3 + i] * h[1 * 3 + j] + h[2 * 3 + i] * h[2 * 3 + j]);
+      const double green[6] = {E[0], E[4], E[8], 2.0 * E[1], 2.0 * E[5], 2.0 * E[6]};
+      if (p.kinematics == SBK_FINITE) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) strain[i] = green[i];
+      } else if (!(det3(F) > 0.0)) {
+        fcode = SBK_EL_INVERTED_POINT;
+      } else {
+        fcode = log_strain(green, L, strain);
+      }
+      if (fcode) fail = (1 << 8) | q;
+    }
+    if (!fail) {
+      PointState st{c.state + c.e * p.nq + q, c.trial + c.e * p.nq + q, c.npts};
+      Response r;
+      fcode = p.general ? general_return(p, strain, st, r) : radial_return(p, strain, st, r);
+      if (fcode) {
+        fail = (2 << 8) | q;
+      } else {
+        double* o = s.slot[q];
+        double pk[6], cauchy[6], tau[6] = {0, 0, 0, 0, 0, 0}, lstr[6] = {0, 0, 0, 0, 0, 0};
+        double max_strain = 0.0, jac = 1.0;
+#pragma unroll
+        for (int i = 0; i < 6; ++i) cauchy[i] = pk[i] = r.stress[i];
+        // F T F^T of a tensorial Voigt T, as a tensorial Voigt vector.
+        auto push = [&](const double t[6], double res[6]) {
+          const double T3[9] = {t[0], t[3], t[5], t[3], t[1], t[4], t[5], t[4], t[2]};
+          double FT[9], R[9];
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+              FT[i * 3 + j] = F[i * 3 + 0] * T3[0 * 3 + j] + F[i * 3 + 1] * T3[1 * 3 + j] + F[i * 3 + 2] * T3[2 * 3 + j];
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+              R[i * 3 + j] = FT[i * 3 + 0] * F[j * 3 + 0] + FT[i * 3 + 1] * F[j * 3 + 1] + FT[i * 3 + 2] * F[j * 3 + 2];
+          res[0] = R[0], res[1] = R[4], res[2] = R[8], res[3] = R[1], res[4] = R[5], res[5] = R[6];
+        };
+        if (p.kinematics == SBK_FINITE_LOGARITHMIC) {
+          log_stress(L, r.stress, pk);
+          push(pk, tau);
+#pragma unroll
+          for (int i = 0; i < 6; ++i) lstr[i] = i < 3 ? strain[i] : 0.5 * strain[i];
+          const double vol = exp(lstr[0] + lstr[1] + lstr[2]);
+#pragma unroll
+          for (int i = 0; i < 6; ++i) {
+            cauchy[i] = tau[i] / vol;
+            max_strain = fmax(max_strain, fabs(lstr[i]));
+          }
+          jac = det3(F);
+        } else if (p.kinematics == SBK_FINITE) {
+          jac = det3(F);
+          double ft[6];
+          push(r.stress, ft);
+#pragma unroll
+          for (int i = 0; i < 6; ++i) cauchy[i] = ft[i] / jac;
+#pragma unroll
+          for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+              const double g = sym[i * 3 + j] + 0.5 * (h[0 * 3 + i] * h[0 * 3 + j] + h[1 * 3 + i] * h[1 * 3 + j] +
+                                                       h[2 * 3 + i] * h[2 * 3 + j]);
+              max_strain = fmax(max_strain, fabs(g));
+            }
+        } else {
+#pragma unroll
+          for (int i = 0; i < 9; ++i) max_strain = fmax(max_strain, fabs(sym[i]));
+        }
+#pragma unroll
+        for (int i = 0; i < 6; ++i) {
+          o[i] = cauchy[i];
+          o[6 + i] = pk[i];
+          o[12 + i] = tau[i];
+          o[18 + i] = lstr[i];
+        }
+        o[24] = max_strain;
+        o[25] = jac;
+        o[26] = st.out[field_eqps(p.nterms) * st.stride];
+      }
+    }
+  }
+  int key = fail ? fail : 0x7fffffff;
+#pragma unroll
+  for (int o = G / 2; o >= 1; o >>= 1) key = min(key, __shfl_xor_sync(c.mask, key, o, G));
+  const int owner = key & 0xff;
+  const int fcode_g = __shfl_sync(c.mask, fcode, key != 0x7fffffff ? owner : 0, G);
+  c.sync();
+  if (lane != 0) return;
+  if (key != 0x7fffffff) {
+    code[e] = fcode_g;
+    atomicMin(first_failure, (int32_t)e);
+    return;
+  }
+  double acc[24];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) acc[i] = 0.0;
+  double max_eqps = 0.0, max_strain = 0.0, min_jac = __longlong_as_double(0x7ff0000000000000LL);
+  for (int qq = 0; qq < p.nq; ++qq) {
+    const double* o = s.slot[qq];
+#pragma unroll
+    for (int i = 0; i < 24; ++i) acc[i] += o[i];
+    max_strain = fmax(max_strain, o[24]);
+    min_jac = fmin(min_jac, o[25]);
+    max_eqps = fmax(max_eqps, o[26]);
+  }
+  const double count = (double)p.nq;
+  double* res = out + e * 28;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    res[i] = acc[i] / count;
+    res[6 + i] = acc[6 + i] / count;
+    res[16 + i] = acc[12 + i] / count;
+    res[22 + i] = acc[18 + i] / count;
+  }
+  const double a0 = res[0] - res[1], a1 = res[1] - res[2], a2 = res[2] - res[0];
+  res[12] = sqrt(0.5 * (a0 * a0 + a1 * a1 + a2 * a2) + 3.0 * (res[3] * res[3] + res[4] * res[4] + res[5] * res[5]));
+  res[13] = max_eqps;
+  res[14] = max_strain;
+  res[15] = p.kinematics == SBK_SMALL_STRAIN ? 1.0 : min_jac;
+  code[e] = 0;
+}
+
+template <int G>
+int launch_stress_g(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
+                    const double* state, const double* alpha_n, double* scratch, double* out, int32_t* code,
+                    int32_t* first_failure, int epb, cudaStream_t stream) {
+  const size_t smem = sizeof(ElemShared<G>) * epb;
+  const int64_t blocks = (ne + epb - 1) / epb;
+  if (blocks == 0) return 0;
+  auto kern = stress_kernel<G>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return (int)err;
+  kern<<<(unsigned)blocks, epb * G, smem, stream>>>(p, ne, coords, conn, u, state, alpha_n, scratch, out, code,
+                                                    first_failure);
+  return (int)cudaGetLastError();
+}
+
 template <int G>
 int launch_g(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
              const double* state, const double* alpha_n, int want_tangent, double* force, double* tangent,
@@ -1186,6 +1411,14 @@ int launch_g(const Params& p, int64_t ne, const double* coords, const int32_t* c
 }
 
 }  // namespace
+
+int launch_stress(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
+                  const double* state, const double* alpha_n, double* scratch, double* out, int32_t* code,
+                  int32_t* first_failure, cudaStream_t stream) {
+  if (p.nq <= 8)
+    return launch_stress_g<8>(p, ne, coords, conn, u, state, alpha_n, scratch, out, code, first_failure, 4, stream);
+  return launch_stress_g<32>(p, ne, coords, conn, u, state, alpha_n, scratch, out, code, first_failure, 1, stream);
+}
 
 size_t element_smem_bytes(int group) {
   return group == 8 ? sizeof(ElemShared<8>) : sizeof(ElemShared<32>);

@@ -26,6 +26,12 @@ int launch_elements(const Params& p, int64_t ne, const double* coords, const int
                     int32_t* code, int32_t* first_failure, bool batch, int elements_per_block,
                     const int32_t* order, cudaStream_t stream);
 size_t element_smem_bytes(int group);
+// Stress recovery of ne mesh elements at u from the committed points and
+// modes: 28 doubles per element into out (see stress_kernel); the returns
+// write their (reproduced) states into scratch (the state layout).
+int launch_stress(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
+                  const double* state, const double* alpha_n, double* scratch, double* out, int32_t* code,
+                  int32_t* first_failure, cudaStream_t stream);
 
 // The gather maps of the assembly (built once on the host).
 struct GatherMaps {

@@ -801,6 +801,29 @@ __device__ __forceinline__ double rot_m(const double q[9], int r, int c) {
   return i == j ? q[i * 3 + a] * q[i * 3 + b] : q[i * 3 + a] * q[j * 3 + b] + q[j * 3 + a] * q[i * 3 + b];
 }
 
+// S = P^T T alone (LogarithmicStrain.cpp:144-149): the second
+// Piola-Kirchhoff stress of the Kirchhoff-like stress T work-conjugate to
+// E_log, for stress recovery.
+__device__ __noinline__ void log_stress(const LogKin& L, const double t[6], double s_out[6]) {
+  const int kr[6] = {0, 1, 2, 0, 1, 2};
+  const int kc[6] = {0, 1, 2, 1, 2, 0};
+  double tpv[6];
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    double v = 0.0;
+#pragma unroll
+    for (int c = 0; c < 6; ++c) v += rot_m(L.q, r, c) * t[c];
+    tpv[r] = v;
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    double v = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) v += rot_m(L.q, k, i) * ((k < 3 ? 1.0 : 2.0) * first_of(L.first, kr[k], kc[k])) * tpv[k];
+    s_out[i] = i < 3 ? v : 0.5 * v;
+  }
+}
+
 // S = P^T T, and material = P^T C P + T : L in global axes (engineering
 // strain columns, tensorial stress rows). C is overwritten by the material.
 __device__ __forceinline__ void log_transform(const LogKin& L, const double t[6], double s_out[6], double C[36]) {

@@ -140,6 +140,25 @@ def evaluate_noalloc(material: Material, coords: torch.Tensor, connectivity: tor
 
 
 @dataclasses.dataclass
+class ElementStresses:
+    """ElastoplasticStress (include/sparlab/fem/Elastoplastic.hpp:206-221)
+    of every element: point averages, [Pa] and [-]."""
+
+    cauchy: torch.Tensor            # (ne, 6) tensorial Voigt
+    piola_kirchhoff: torch.Tensor   # (ne, 6)
+    von_mises: torch.Tensor         # (ne,) of the average Cauchy stress
+    max_plastic_strain: torch.Tensor  # (ne,) largest accumulated plastic strain
+    max_strain: torch.Tensor        # (ne,) largest strain component
+    min_jacobian: torch.Tensor      # (ne,) smallest det F
+    kirchhoff: torch.Tensor         # (ne, 6) logarithmic kinematics, else 0
+    log_strain: torch.Tensor        # (ne, 6) tensor components, logarithmic, else 0
+
+    @classmethod
+    def from_packed(cls, t: torch.Tensor) -> "ElementStresses":
+        return cls(t[:, 0:6], t[:, 6:12], t[:, 12], t[:, 13], t[:, 14], t[:, 15], t[:, 16:22], t[:, 22:28])
+
+
+@dataclasses.dataclass
 class Evaluation:
     """NonlinearSystem.hpp:27-47. Tensors are views of the system's buffers,
     valid until its next evaluate (clone to keep them)."""
@@ -303,6 +322,21 @@ class NonlinearSystem:
         n = int(nodes.numel())
         _capi.check(_capi.lib().sbk_system_add_node_blocks(self._h, n, _ptr(nodes.to(torch.int32).contiguous()),
                                                            _ptr(blocks.to(torch.float64).contiguous())))
+
+    def stress(self, u: torch.Tensor) -> ElementStresses:
+        """elastoplastic_stress of every element at u from the committed
+        points and modes (IncompatibleModes.cpp:602-664), the step-end stress
+        recovery of the forming driver (Forming.cpp:1266-1281): call after
+        commit(). Overwrites the trial state of the last evaluate."""
+        u = u.to(torch.float64).contiguous()
+        if u.numel() != self.num_dofs:
+            raise ValueError(f"u has {u.numel()} values, the system {self.num_dofs} DOFs")
+        out = torch.empty((self.mesh.num_elements, 28), dtype=torch.float64, device=u.device)
+        st = _capi.lib().sbk_system_stress(self._h, _ptr(u), _ptr(out))
+        if st == 4:
+            raise _capi.SolverError(st, _capi.last_error())
+        _capi.check(st)
+        return ElementStresses.from_packed(out)
 
     def stiffness_gross(self, u: torch.Tensor, free: torch.Tensor) -> float:
         """stiffness_gross (src/fem/NonlinearSystem.hpp:49-67): the norm over

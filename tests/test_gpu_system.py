@@ -183,3 +183,34 @@ def test_production_rule_system(pkg, orc, cuda):
     assert np.abs(f - ref["internal"]).max() <= 1e-11 * ref["gross"]
     v = ev.tangent.cpu().numpy()
     assert np.linalg.norm(v - ref["values"]) <= 1e-11 * np.linalg.norm(ref["values"])
+
+
+@pytest.mark.parametrize("kin", ["logarithmic", "finite", "small"])
+def test_stress_recovery_matches_oracle(pkg, orc, problem, cuda, kin):
+    """Step-end stress recovery (elastoplastic_stress, IncompatibleModes.cpp
+    :602-664) after a commit: every element's averages against the oracle's
+    restatement at the committed points and modes."""
+    mesh, mat = problem.mesh, problem.material
+    sys_ = pkg.NonlinearSystem(mesh, mat, kinematics=kin)
+    if kin == "logarithmic":
+        sys_.set_committed(problem.state)
+        sys_.set_internal(problem.alpha)
+    u = torch.tensor(problem.u if kin == "logarithmic" else 0.5 * problem.u, device=cuda)
+    sys_.evaluate(u, 0.0, False)
+    sys_.commit()
+    st, al = sys_.committed_views()
+    committed = device_to_oracle(st.cpu().numpy(), mat.kinematic_terms)
+    alpha = al.cpu().numpy()
+    got = sys_.stress(u)
+    X = mesh.element_coordinates()
+    ue = mesh.gather(u.cpu().numpy())
+    ref, status = orc.element_stress(mat.as_dict(), X, ue, committed, alpha, kinematics=kin)
+    assert (status == 0).all()
+    packed = torch.cat([got.cauchy, got.piola_kirchhoff, got.von_mises[:, None], got.max_plastic_strain[:, None],
+                        got.max_strain[:, None], got.min_jacobian[:, None], got.kirchhoff, got.log_strain],
+                       dim=1).cpu().numpy()
+    for lo, hi in [(0, 6), (6, 12), (12, 13), (13, 14), (14, 15), (15, 16), (16, 22), (22, 28)]:
+        scale = max(np.abs(ref[:, lo:hi]).max(), 1e-300)
+        assert np.abs(packed[:, lo:hi] - ref[:, lo:hi]).max() <= 1e-11 * scale, (lo, hi)
+    if kin == "logarithmic":
+        assert ref[:, 13].max() > 0.0

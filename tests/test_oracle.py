@@ -685,3 +685,43 @@ def test_contact_tangent_is_the_derivative(orc, shape, friction):
             exact.commit()
             exact.begin_increment(u1, 0.2, 0.25, [True], 1e-3)
             assert np.array_equal(exact.evaluate(u2, 0.25, False)["residual"], ev["residual"])
+
+
+def test_stress_recovery_is_objective_and_reproduces_the_state(orc, pkg):
+    """Stress recovery (incompatible_elastoplastic_stress,
+    IncompatibleModes.cpp:602-664) at the converged state of a plastic step:
+    the recovered second Piola-Kirchhoff stress and log strain are unchanged
+    by a superposed rotation, the Kirchhoff and Cauchy stresses rotate
+    (tests/test_logarithmic.cpp:329-383), the largest accumulated plastic
+    strain is the committed one (the return from it is an elastic check),
+    and at rest every stress is zero."""
+    import scipy.spatial.transform  # noqa: F401
+
+    m = dict(materials(pkg)["hill"], backstresses=[(30.0e9, 300.0)])
+    x = X_DISTORTED
+    R = rotation(0.9, (0.2, 1.0, -0.4))
+    ue = deformation(x, 0.08)
+    turned = np.concatenate([R @ (x[a] + ue[3 * a:3 * a + 3]) - x[a] for a in range(8)])
+    el = one(orc, m, ue, tangent=False)
+    er = one(orc, m, turned, tangent=False)
+    assert el["yielding"] > 0
+    s1, st1 = orc.element_stress(m, x.reshape(1, 24), ue.reshape(1, 24), el["states"][None], el["alpha"][None])
+    s2, st2 = orc.element_stress(m, x.reshape(1, 24), turned.reshape(1, 24), er["states"][None], er["alpha"][None])
+    assert st1[0] == 0 and st2[0] == 0
+    s1, s2 = s1[0], s2[0]
+
+    def tens(v):
+        return np.array([[v[0], v[3], v[5]], [v[3], v[1], v[4]], [v[5], v[4], v[2]]])
+
+    def voigt(t):
+        return np.array([t[0, 0], t[1, 1], t[2, 2], t[0, 1], t[1, 2], t[2, 0]])
+
+    assert relative(s2[6:12], s1[6:12]) <= 1e-11  # second Piola-Kirchhoff
+    assert relative(s2[22:28], s1[22:28]) <= 1e-12  # log strain
+    assert relative(s2[16:22], voigt(R @ tens(s1[16:22]) @ R.T)) <= 1e-11  # Kirchhoff
+    assert relative(s2[0:6], voigt(R @ tens(s1[0:6]) @ R.T)) <= 1e-11  # Cauchy
+    assert s2[12] == pytest.approx(s1[12], rel=1e-11)  # von Mises
+    assert s2[15] == pytest.approx(s1[15], rel=1e-13)  # min det F
+    assert s1[13] == pytest.approx(el["states"][:, 36].max(), rel=1e-15)
+    rest, st = orc.element_stress(m, x.reshape(1, 24), np.zeros((1, 24)))
+    assert st[0] == 0 and np.abs(rest[0][:13]).max() == 0.0 and rest[0][15] == 1.0
