@@ -1,0 +1,228 @@
+"""A forming driver for the end-to-end tests - test infrastructure, not part
+of the product. It stands in for the reference's FormingAnalysis::run
+(src/fem/Forming.cpp:686-1262), which calls the element loop and the contact
+every Newton iteration: it runs a committed forming deck of the reference
+through this package's NonlinearSystem and ToolContact on the GPU, solving
+the linear systems on the host with scipy (the reference's own sparse solver
+is outside the graft).
+
+What it restates of the driver, because the converged states depend on it:
+the step partition (prescribed DOFs held at their values, Forming.cpp:804-821),
+the start imbalance r0 ramped out over the step (:829-846, :890-897), the
+increment schedule (the tool travel per increment and the stations,
+:1149-1163) and the commit of every converged increment (:1208-1215). What
+it does not restate, because it only changes the path to the same converged
+state: the predictor, the energy line search (a residual backtracking here),
+the semismooth anticipation and the tolerances (the iteration here runs to
+a correction of 1e-13 m (1e-11 m after 40 iterations), well inside the reference's
+relative 1e-6).
+"""
+from __future__ import annotations
+
+import dataclasses
+
+import numpy as np
+import scipy.sparse
+import scipy.sparse.linalg
+import torch
+
+
+def in_region(x: np.ndarray, region: dict, tol: float) -> np.ndarray:
+    """Selector::contains (src/fem/Selector.cpp:49-56) of a deck region:
+    boxes inclusive with the tolerance, `all`, `any_of`."""
+    if region.get("all"):
+        return np.ones(len(x), dtype=bool)
+    if "any_of" in region:
+        out = np.zeros(len(x), dtype=bool)
+        for r in region["any_of"]:
+            out |= in_region(x, r, tol)
+        return out
+    box = region["box"]
+    inf = np.inf
+    lo = [box.get("xmin", -inf), box.get("ymin", -inf), box.get("zmin", -inf)]
+    hi = [box.get("xmax", inf), box.get("ymax", inf), box.get("zmax", inf)]
+    ok = np.ones(len(x), dtype=bool)
+    for k in range(3):
+        ok &= (x[:, k] >= lo[k] - tol) & (x[:, k] <= hi[k] + tol)
+    return ok
+
+
+def top_face_slaves(nodes: np.ndarray, elements: np.ndarray, region: dict, tol: float):
+    """The slave nodes of a tool and their tributary areas: the boundary
+    faces whose every node lies in the tool's surface region, each face's
+    shape-function integrals added to its nodes (ToolContact's constructor,
+    src/fem/RigidTool.cpp:292-321). For the flat quadrilateral faces of a
+    structured sheet every node of a face takes a quarter of its area."""
+    faces = {}
+    local = [(0, 3, 2, 1), (4, 5, 6, 7), (0, 1, 5, 4), (1, 2, 6, 5), (2, 3, 7, 6), (3, 0, 4, 7)]
+    for e, conn in enumerate(elements):
+        for f in local:
+            key = tuple(sorted(conn[list(f)]))
+            faces.setdefault(key, []).append((e, [conn[i] for i in f]))
+    inside = in_region(nodes, region, tol)
+    area = {}
+    for key, owners in sorted(faces.items()):
+        if len(owners) != 1:
+            continue  # an interior face
+        quad = owners[0][1]
+        if not all(inside[n] for n in quad):
+            continue
+        p = nodes[quad]
+        a = 0.5 * np.linalg.norm(np.cross(p[2] - p[0], p[3] - p[1]))  # a planar quadrilateral
+        for n in quad:
+            area[n] = area.get(n, 0.0) + 0.25 * a
+    ids = np.array(sorted(area), dtype=np.int32)
+    return ids, np.array([area[i] for i in ids])
+
+
+@dataclasses.dataclass
+class StepResult:
+    u: np.ndarray
+    increments: int
+    tool_fz: list
+
+
+class FormingRun:
+    def __init__(self, pkg, fixture: dict, device):
+        self.pkg = pkg
+        self.fx = fixture
+        self.dev = device
+        self.nodes = np.array(fixture["nodes"], dtype=np.float64)
+        self.elements = np.array(fixture["elements"], dtype=np.int32)
+        self.mesh = pkg.HexMesh(self.nodes, self.elements)
+        m = fixture["material"]
+        pl = m["plasticity"]
+        self.material = pkg.Material(m["youngs_modulus"], m["poisson_ratio"], yield_stress=pl["yield_stress"],
+                                     hardening_modulus=pl["hardening_modulus"],
+                                     kinematic_hardening_modulus=pl.get("kinematic_hardening_modulus", 0.0),
+                                     saturation_stress=pl["saturation_stress"],
+                                     saturation_rate=pl["saturation_rate"], name=m["name"])
+        kin = {"finite_logarithmic": "logarithmic", "finite": "finite", "small_strain": "small"}[fixture["kinematics"]]
+        self.system = pkg.NonlinearSystem(self.mesh, self.material, kinematics=kin)
+        extent = self.nodes.max(0) - self.nodes.min(0)
+        self.tol = 1e-9 * float(np.linalg.norm(extent))
+        self.tools = []
+        self.paths = []
+        for t in fixture["tools"]:
+            ids, area = top_face_slaves(self.nodes, self.elements, t["surface"], self.tol)
+            kappa = t.get("penalty", 10.0) * self.material.youngs_modulus / np.sqrt(area)
+            tr = t["trajectory"]
+            self.paths.append((np.array(tr["times"], float), np.array(tr["points"], float)))
+            self.tools.append(pkg.Tool(shape=t["shape"], times=tr["times"], points=tr["points"], nodes=ids,
+                                       area=area, kappa=kappa, radius=t.get("radius", 0.0),
+                                       friction=t.get("friction", 0.0), axis=t.get("axis", (0.0, 0.0, 1.0)),
+                                       normal=t.get("normal", (0.0, 0.0, 1.0)), name=t["name"]))
+        self.min_size = float(np.sqrt(min(tl.area.min() for tl in self.tools))) if self.tools else 1.0
+        self.contact = pkg.ToolContact(self.mesh, self.tools, friction_tangent="exact") if self.tools else None
+        self.u = np.zeros(self.mesh.num_dofs)
+        self.t = 0.0
+        self.last_du = 0.0
+
+    # -- pieces of one Newton iteration -------------------------------------
+    def _residual(self, u, t, active, tangent):
+        """f_int + the contact residual, with the contact node blocks added
+        into the system tangent (Forming.cpp:986-990)."""
+        ev = self.system.evaluate(torch.tensor(u, device=self.dev), 0.0, tangent)
+        r = ev.residual.double().cpu().numpy().copy()
+        fz = 0.0
+        if self.contact is not None and any(active):
+            cev = self.contact.evaluate(torch.tensor(u, device=self.dev), t, tangent)
+            r += cev.residual.cpu().numpy()
+            fz = float(sum(cev.tools[k][5] for k in range(len(active)) if active[k]))
+            if tangent and len(cev.nodes):
+                self.system.add_node_blocks(cev.nodes, cev.blocks)
+        return ev, r, fz
+
+    def _matrix(self, ev, free):
+        n = self.mesh.num_dofs
+        k = scipy.sparse.csc_matrix((ev.tangent.cpu().numpy(), self.system.inner.cpu().numpy(),
+                                     self.system.outer.cpu().numpy()), shape=(n, n))
+        return k[free][:, free].tocsc()
+
+    def _speed(self, t, active):
+        v = 0.0
+        for k, (times, pts) in enumerate(self.paths):
+            if not active[k]:
+                continue
+            i = min(max(np.searchsorted(times, t, side="right") - 1, 0), len(times) - 2)
+            v = max(v, np.linalg.norm(pts[i + 1] - pts[i]) / (times[i + 1] - times[i]))
+        return v
+
+    def run_step(self, k: int) -> StepResult:
+        st = self.fx["steps"][k]["deck"]
+        names = [t["name"] for t in self.fx["tools"]]
+        active = [n in st.get("tools", []) for n in names]
+        release = st["type"] == "release"
+        tb, te = (st["time"] if "time" in st else (self.t, self.t + 1.0))
+        duration = te - tb
+        fixed = np.zeros(self.mesh.num_dofs, dtype=bool)
+        for bc in st["boundary_conditions"]:
+            sel = in_region(self.nodes, bc["region"], self.tol)
+            for comp in bc["fix"]:
+                fixed[3 * np.where(sel)[0] + "xyz".index(comp)] = True
+        free = np.where(~fixed)[0]
+        # The start imbalance on the step's free DOFs.
+        if self.contact is not None:
+            self.contact.begin_increment(torch.tensor(self.u, device=self.dev), tb, tb, active, np.inf)
+        _, r, _ = self._residual(self.u, tb, active, False)
+        r0 = r[free]
+        stations = sorted({tt for kk, (times, _) in enumerate(self.paths) if active[kk]
+                           for tt in times if tb < tt <= te} | {te})
+        parts = st.get("increments", 0) or (10 if release else 1)
+        dt_max = duration / parts
+        travel = st.get("max_tool_travel", 0.0) or 0.5 * self.min_size
+        t, dt, count, fz_list = tb, dt_max, 0, []
+        while True:
+            station = next(s for s in stations if s > t)
+            h = min(dt, dt_max)
+            speed = self._speed(t, active)
+            if speed > 0:
+                h = min(h, travel / speed)
+            reach = station - t <= h * (1.0 + 1.0e-6)
+            t1 = station if reach else t + h
+            s1 = 1.0 if (reach and station == te) else (t1 - tb) / duration
+            fz = self._newton(t, t1, s1, free, r0, active)
+            fz_list.append(fz)
+            count += 1
+            t = t1
+            if s1 >= 1.0:
+                break
+        self.t = te
+        return StepResult(u=self.u.copy(), increments=count, tool_fz=fz_list)
+
+    def _newton(self, t0, t1, s1, free, r0, active):
+        ramp = 1.0 - s1
+        trial = self.u.copy()
+        if self.contact is not None:
+            self.contact.begin_increment(torch.tensor(self.u, device=self.dev), t0, t1, active,
+                                         2.0 * 1e-3 + 2.0 * self.last_du + self.min_size)
+        for it in range(60):
+            ev, r, _ = self._residual(trial, t1, active, True)
+            rf = r[free] - ramp * r0
+            du = scipy.sparse.linalg.spsolve(self._matrix(ev, free), -rf)
+            norm0 = np.linalg.norm(rf)
+            alpha = 1.0
+            for _ in range(12):  # backtrack on |R| where a full step overshoots
+                probe = trial.copy()
+                probe[free] += alpha * du
+                try:
+                    _, rp, _ = self._residual(probe, t1, active, False)
+                    if np.linalg.norm(rp[free] - ramp * r0) <= max(norm0, 1e-6) * 1.0001 or alpha < 1e-3:
+                        break
+                except self.pkg.SolverError:
+                    pass
+                alpha *= 0.5
+            trial[free] += alpha * du
+            step = alpha * np.abs(du).max()
+            if (alpha == 1.0 and step <= 1e-13) or (it >= 40 and step <= 1e-11):
+                break
+        else:
+            raise AssertionError(f"the increment to t = {t1} did not converge")
+        # The accepted state's own evaluation makes its trial history the one committed.
+        _, _, fz = self._residual(trial, t1, active, False)
+        self.system.commit()
+        if self.contact is not None:
+            self.contact.commit()
+        self.last_du = float(np.abs((trial - self.u).reshape(-1, 3)).max())
+        self.u = trial
+        return fz

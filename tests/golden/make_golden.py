@@ -5,6 +5,13 @@ Run in a checkout that has the reference's sources (its Python package
 <reference root>``. The fixtures it writes are committed; the tests read
 only them, never the reference.
 
+strip_h2_im_nz4.json: one committed forming run of the reference
+(benchmarks/physics_audit/calculix/punch/strip_h2_im_nz4/sparlab): its mesh,
+the parts of its deck the element loop and the contact read (material,
+kinematics, tool, steps and their boundary regions), the nodal
+displacements at the end of each step (17 significant digits in the
+reference's CSV output) and the tool force of every forming increment.
+
 materials.json: the hardening parameters the reference's own Python
 (python/precomp/materials.py) derives - its built-in library (Hollomon
 fits) and the Swift law of the 40x40x2 forming sheet - plus the material
@@ -45,5 +52,31 @@ def main(ref_root: str) -> None:
         f.write("\n")
 
 
+def strip(ref_root: str, case: str = "strip_h2_im_nz4") -> None:
+    import csv
+
+    base = os.path.join(ref_root, "benchmarks/physics_audit/calculix/punch", case, "sparlab")
+    deck = json.load(open(os.path.join(base, "deck.json")))
+    mesh = json.load(open(os.path.join(base, "out", "mesh.json")))
+    summary = json.load(open(os.path.join(base, "out", "summary.json")))
+    steps = []
+    for k, st in enumerate(deck["forming"]["steps"], start=1):
+        rows = list(csv.DictReader(open(os.path.join(base, "out", f"step_{k}_{st['name']}_nodes.csv"))))
+        steps.append({"deck": st, "u": [[float(r["ux"]), float(r["uy"]), float(r["uz"])] for r in rows],
+                      "increments": summary["steps"][k - 1]["increments"],
+                      "cuts": summary["steps"][k - 1]["cuts"]})
+    forces = [{k: r[k] for k in ("step", "increment", "t", "cz", "fx", "fz", "active_nodes")}
+              for r in csv.DictReader(open(os.path.join(base, "out", "tool_forces.csv")))]
+    out = {"source": os.path.relpath(base, ref_root), "nodes": mesh["nodes_m"], "elements": mesh["elements"],
+           "material": deck["material"], "kinematics": deck["forming"]["kinematics"],
+           "tools": deck["forming"]["tools"], "steps": steps, "tool_forces": forces,
+           "analysis": summary["analysis"]}
+    with open(os.path.join(HERE, f"{case}.json"), "w") as f:
+        json.dump(out, f, separators=(",", ":"))
+        f.write("\n")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    main(root)
+    strip(root)
