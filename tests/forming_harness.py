@@ -32,6 +32,10 @@ def in_region(x: np.ndarray, region: dict, tol: float) -> np.ndarray:
     boxes inclusive with the tolerance, `all`, `any_of`."""
     if region.get("all"):
         return np.ones(len(x), dtype=bool)
+    if "nearest_node" in region:  # the node nearest a point (the first of equals)
+        out = np.zeros(len(x), dtype=bool)
+        out[int(np.argmin(np.linalg.norm(x - np.asarray(region["nearest_node"], float), axis=1)))] = True
+        return out
     if "any_of" in region:
         out = np.zeros(len(x), dtype=bool)
         for r in region["any_of"]:
@@ -148,7 +152,11 @@ class FormingRun:
             v = max(v, np.linalg.norm(pts[i + 1] - pts[i]) / (times[i + 1] - times[i]))
         return v
 
-    def run_step(self, k: int) -> StepResult:
+    def run_step(self, k: int, times=None) -> StepResult:
+        """Step k of the deck. `times`: the end times of the increments the
+        reference accepted (its tool_forces.csv), to follow its increment
+        sequence through the cuts its own Newton iterations made; else the
+        schedule of Forming.cpp:1149-1163 without cuts."""
         st = self.fx["steps"][k]["deck"]
         names = [t["name"] for t in self.fx["tools"]]
         active = [n in st.get("tools", []) for n in names]
@@ -172,6 +180,14 @@ class FormingRun:
         dt_max = duration / parts
         travel = st.get("max_tool_travel", 0.0) or 0.5 * self.min_size
         t, dt, count, fz_list = tb, dt_max, 0, []
+        if times is not None:
+            for t1 in times:
+                s1 = 1.0 if t1 == te else (t1 - tb) / duration
+                fz_list.append(self._newton(t, t1, s1, free, r0, active))
+                t = t1
+            assert t == te, (t, te)
+            self.t = te
+            return StepResult(u=self.u.copy(), increments=len(times), tool_fz=fz_list)
         while True:
             station = next(s for s in stations if s > t)
             h = min(dt, dt_max)

@@ -5,8 +5,9 @@ Run in a checkout that has the reference's sources (its Python package
 <reference root>``. The fixtures it writes are committed; the tests read
 only them, never the reference.
 
-strip_h2_im_nz4.json: one committed forming run of the reference
-(benchmarks/physics_audit/calculix/punch/strip_h2_im_nz4/sparlab): its mesh,
+strip_h2_im_nz4.json, strip_h1_im_nz4.json, plate_h2_im_mu0.1_drag3.json:
+committed forming runs of the reference
+(benchmarks/physics_audit/calculix/punch/<case>/sparlab): the mesh,
 the parts of its deck the element loop and the contact read (material,
 kinematics, tool, steps and their boundary regions), the nodal
 displacements at the end of each step (17 significant digits in the
@@ -65,7 +66,7 @@ def strip(ref_root: str, case: str = "strip_h2_im_nz4") -> None:
         steps.append({"deck": st, "u": [[float(r["ux"]), float(r["uy"]), float(r["uz"])] for r in rows],
                       "increments": summary["steps"][k - 1]["increments"],
                       "cuts": summary["steps"][k - 1]["cuts"]})
-    forces = [{k: r[k] for k in ("step", "increment", "t", "cz", "fx", "fz", "active_nodes")}
+    forces = [{k: r[k] for k in ("step", "increment", "t", "cx", "cz", "fx", "fz", "active_nodes")}
               for r in csv.DictReader(open(os.path.join(base, "out", "tool_forces.csv")))]
     out = {"source": os.path.relpath(base, ref_root), "nodes": mesh["nodes_m"], "elements": mesh["elements"],
            "material": deck["material"], "kinematics": deck["forming"]["kinematics"],
@@ -79,4 +80,5 @@ def strip(ref_root: str, case: str = "strip_h2_im_nz4") -> None:
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     main(root)
-    strip(root)
+    for case in ("strip_h2_im_nz4", "strip_h1_im_nz4", "plate_h2_im_mu0.1_drag3"):
+        strip(root, case)

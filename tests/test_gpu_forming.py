@@ -1,12 +1,23 @@
-"""End to end against a forming run the reference committed
-(benchmarks/physics_audit/calculix/punch/strip_h2_im_nz4: a 20 x 1 x 4
-incompatible-mode Hex8 strip, logarithmic strain, J2 with Voce hardening,
-a cylindrical punch with Coulomb friction 0.1 pressed 4 mm into it, then
-the tool taken away over 20 increments and the clamps released onto
-supports). The element loop and the contact are this package's, on the
-GPU; the Newton driver around them is the test harness in
-forming_harness.py. The formed, unloaded and released nodal displacements
-must agree with the reference's within 1e-5 mm (1e-8 m)."""
+"""End to end against forming runs the reference committed
+(benchmarks/physics_audit/calculix/punch/<case>/sparlab), all
+incompatible-mode Hex8 under logarithmic strain with J2 and Voce hardening
+and Coulomb friction 0.1:
+
+- strip_h2_im_nz4: a 20 x 1 x 4 strip under a cylindrical punch pressed
+  4 mm into it, the tool taken away over 20 increments and the clamps
+  released onto supports;
+- strip_h1_im_nz4: the same strip at 40 x 1 x 4, whose forming step the
+  reference's Newton iterations cut four times;
+- plate_h2_im_mu0.1_drag3: a clamped 20 x 20 x 2 plate under a spherical
+  punch pressed 3 mm in and dragged 3 mm sideways, released onto 3-2-1
+  supports (two cuts).
+
+The element loop and the contact are this package's, on the GPU; the
+Newton driver around them is the test harness in forming_harness.py, which
+takes the reference's accepted increments (their times in its
+tool_forces.csv) through the forming step. The formed, unloaded and
+released nodal displacements must agree with the reference's within 1e-5 mm
+(1e-8 m), the north star's bar."""
 from __future__ import annotations
 
 import json
@@ -19,15 +30,19 @@ from forming_harness import FormingRun
 
 pytestmark = pytest.mark.gpu
 
-FIXTURE = os.path.join(os.path.dirname(__file__), "golden", "strip_h2_im_nz4.json")
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+CASES = ["strip_h2_im_nz4", "strip_h1_im_nz4", "plate_h2_im_mu0.1_drag3"]
 HEIGHT_TOL = 1.0e-8  # [m]: 1e-5 mm
 
 
-@pytest.fixture(scope="module")
-def run(pkg, cuda):
-    fx = json.load(open(FIXTURE))
+@pytest.fixture(scope="module", params=CASES)
+def run(request, pkg, cuda):
+    fx = json.load(open(os.path.join(GOLDEN, request.param + ".json")))
     r = FormingRun(pkg, fx, cuda)
-    results = [r.run_step(k) for k in range(len(fx["steps"]))]
+    results = []
+    for k in range(len(fx["steps"])):
+        times = [float(f["t"]) for f in fx["tool_forces"] if int(f["step"]) == k + 1]
+        results.append(r.run_step(k, times if times else None))
     return fx, results
 
 
