@@ -184,6 +184,25 @@ typedef struct sbk_evaluation {
 int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int want_tangent,
                         sbk_evaluation* out);
 
+/* sbk_system_evaluate without a synchronisation, for stream capture (a CUDA
+ * graph of a Newton iteration, replayed every iteration): enqueues the
+ * element kernel, the gathers and the schedule on the system's stream and
+ * writes a 5-double summary to summary_dev (device): energy, gross,
+ * yielding points, the lowest failing element (-1: none) and its code. The
+ * schedule is used in the captured launch only if an evaluate ran before
+ * the capture. The caller checks summary_dev[3] before it commits. (No
+ * counterpart in the reference, whose evaluate returns its Evaluation.) */
+int sbk_system_enqueue(sbk_system* sys, const double* u_dev, int want_tangent, double* summary_dev);
+
+/* With stable = 1, sbk_system_commit copies the trial points and modes into
+ * the committed buffers on the device instead of exchanging the two, so
+ * that every device pointer of the system - and so a captured graph - stays
+ * valid across commits. It then commits whatever the last evaluation left
+ * in the trial buffers - an evaluate, an enqueue or a replay of a captured
+ * enqueue, which the library does not see - so the caller checks that
+ * evaluation's summary first. */
+int sbk_system_set_stable_buffers(sbk_system* sys, int stable);
+
 /* Device time of each phase of the last evaluate, in ms, recorded with CUDA
  * events on the system's stream when timing is on: [0] the element kernel,
  * [1] the force gather and reductions, [2] the tangent value gather (the

@@ -110,6 +110,8 @@ SIGNATURES = {
     "sbk_system_pattern": (_I, [_P, ctypes.POINTER(sbk_pattern)]),
     "sbk_system_evaluate": (_I, [_P, _P, _D, _I, ctypes.POINTER(sbk_evaluation)]),
     "sbk_system_commit": (_I, [_P]),
+    "sbk_system_enqueue": (_I, [_P, _P, _I, _P]),
+    "sbk_system_set_stable_buffers": (_I, [_P, _I]),
     "sbk_system_set_timing": (_I, [_P, _I]),
     "sbk_system_last_timings": (_I, [_P, ctypes.POINTER(_D)]),
     "sbk_system_get_committed": (_I, [_P, _P, _P]),

@@ -201,7 +201,28 @@ __global__ void __launch_bounds__(kReduceThreads) free_squares_kernel(int32_t n,
   }
 }
 
+// The summary of an evaluation for a caller that does not synchronise:
+// energy, gross, yielding points, the lowest failing element (-1: none) and
+// its code.
+__global__ void summary_kernel(const double* __restrict__ scalars, const int32_t* __restrict__ first_failure,
+                               const int32_t* __restrict__ code, double* __restrict__ summary) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  summary[0] = scalars[0];
+  summary[1] = sqrt(scalars[1]);
+  summary[2] = scalars[2];
+  const int32_t first = *first_failure;
+  const bool failed = first != 0x7f7f7f7f;
+  summary[3] = failed ? (double)first : -1.0;
+  summary[4] = failed ? (double)code[first] : 0.0;
+}
+
 }  // namespace
+
+int launch_summary(const double* scalars, const int32_t* first_failure, const int32_t* code, double* summary,
+                   cudaStream_t stream) {
+  summary_kernel<<<1, 32, 0, stream>>>(scalars, first_failure, code, summary);
+  return (int)cudaGetLastError();
+}
 
 int launch_stiffness_gross(int64_t nn, const int32_t* outer, const int32_t* inner, const double* values,
                            const double* u, int32_t num_free, const int32_t* free_dofs, double* product,

@@ -396,6 +396,7 @@ struct sbk_system {
   int32_t* sched = nullptr;    // its bucket counters
   bool order_valid = false;
   bool schedule = true;
+  bool stable = false;  // commit copies instead of swapping (captured graphs stay valid)
   int elements_per_block = 0;
   bool has_trial = false;
   bool has_values = false;  // values hold the tangent of the last evaluate
@@ -802,10 +803,49 @@ int sbk_system_last_timings(const sbk_system* sys, double* ms3) {
 
 int sbk_system_commit(sbk_system* sys) {
   if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
-  if (!sys->has_trial) return fail(SBK_ERR_ARGUMENT, "no successful evaluation to commit");
-  std::swap(sys->committed, sys->trial);
-  std::swap(sys->alpha_c, sys->alpha_t);
+  // With stable buffers the trial state may come from a replayed graph,
+  // which the host does not see: the caller checked its summary.
+  if (!sys->has_trial && !sys->stable) return fail(SBK_ERR_ARGUMENT, "no successful evaluation to commit");
+  if (sys->stable) {
+    const size_t ns = static_cast<size_t>(sys->ne) * sys->p.nq * sys->p.nfields;
+    SBK_CUDA(cudaMemcpyAsync(sys->committed, sys->trial, ns * sizeof(double), cudaMemcpyDeviceToDevice, sys->stream));
+    SBK_CUDA(cudaMemcpyAsync(sys->alpha_c, sys->alpha_t, static_cast<size_t>(sys->ne) * 9 * sizeof(double),
+                             cudaMemcpyDeviceToDevice, sys->stream));
+  } else {
+    std::swap(sys->committed, sys->trial);
+    std::swap(sys->alpha_c, sys->alpha_t);
+  }
   sys->has_trial = false;
+  return SBK_OK;
+}
+
+int sbk_system_set_stable_buffers(sbk_system* sys, int stable) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  sys->stable = stable != 0;
+  return SBK_OK;
+}
+
+int sbk_system_enqueue(sbk_system* sys, const double* u_dev, int want_tangent, double* summary_dev) {
+  if (!sys || !u_dev || !summary_dev) return fail(SBK_ERR_ARGUMENT, "null argument");
+  cudaStream_t st = sys->stream;
+  SBK_CUDA(cudaMemsetAsync(sys->first_fail, 0x7f, sizeof(int32_t), st));
+  int rc = sbk::launch_elements(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c,
+                                want_tangent, sys->force, sys->tangent, sys->energy_e, sys->trial, sys->alpha_t,
+                                sys->yield, sys->iters, sys->code, sys->first_fail, false,
+                                sys->elements_per_block, sys->schedule && sys->order_valid ? sys->order : nullptr,
+                                st);
+  if (rc) return fail(SBK_ERR_CUDA, std::string("element kernel: ") + cudaGetErrorString((cudaError_t)rc));
+  rc = sbk::launch_assemble_forces(sys->maps(), sys->force, sys->energy_e, sys->yield, sys->p.nq, sys->internal,
+                                   sys->scratch, sys->scalars, st);
+  if (!rc && want_tangent) rc = sbk::launch_assemble_values(sys->maps(), sys->tangent, sys->values, st);
+  if (!rc && sys->schedule && sys->order_valid)
+    rc = sbk::launch_schedule(sys->ne, sys->p.nq, sys->iters, sys->yield, sys->sched, sys->order, st);
+  if (!rc) rc = sbk::launch_summary(sys->scalars, sys->first_fail, sys->code, summary_dev, st);
+  if (rc) return fail(SBK_ERR_CUDA, std::string("enqueue: ") + cudaGetErrorString((cudaError_t)rc));
+  // The caller reads the summary after its own synchronisation; a commit
+  // then takes this evaluation's trial state.
+  sys->has_trial = true;
+  sys->has_values = want_tangent != 0;
   return SBK_OK;
 }
 

@@ -1402,8 +1402,17 @@ int launch_g(const Params& p, int64_t ne, const double* coords, const int32_t* c
   const int64_t blocks = (ne + epb - 1) / epb;
   if (blocks == 0) return 0;
   auto kern = element_kernel<G>;
-  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (err != cudaSuccess) return (int)err;
+  // The shared-memory limit is raised once per device and size, so that a
+  // launch inside a stream capture (a CUDA graph of an evaluation) makes no
+  // attribute call.
+  static size_t raised[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || raised[dev] < smem) {
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return (int)err;
+    if (dev >= 0 && dev < 64) raised[dev] = smem;
+  }
   kern<<<(unsigned)blocks, threads, smem, stream>>>(p, ne, batch, coords, conn, u, state, alpha_n, want_tangent,
                                                      force, tangent, energy, trial, alpha_out, yield, iterations,
                                                      code, first_failure, order);

@@ -58,6 +58,10 @@ int launch_assemble_forces(const GatherMaps& m, const double* force, const doubl
                            const uint8_t* yield, int nq, double* internal, double* scratch, double* scalars,
                            cudaStream_t stream);
 size_t assemble_scratch_doubles();
+// Energy, gross, yielding points, lowest failing element (-1) and its code
+// into summary (5 doubles, device), from the reductions' scalars.
+int launch_summary(const double* scalars, const int32_t* first_failure, const int32_t* code, double* summary,
+                   cudaStream_t stream);
 // stiffness_gross: |K| |u| per row into `product` (3 nn), then the sum of
 // squares of its listed free DOFs into scalars[0] (scratch as for the forces).
 int launch_stiffness_gross(int64_t nn, const int32_t* outer, const int32_t* inner, const double* values,

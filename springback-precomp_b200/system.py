@@ -223,6 +223,28 @@ class NonlinearSystem:
     def set_stream(self, stream=None):
         _capi.check(_capi.lib().sbk_system_set_stream(self._h, _stream_ptr(stream)))
 
+    def set_stable_buffers(self, stable: bool = True):
+        """Commit by copying on the device instead of exchanging buffers, so
+        that a captured graph of evaluate stays valid across commits."""
+        _capi.check(_capi.lib().sbk_system_set_stable_buffers(self._h, 1 if stable else 0))
+
+    def enqueue(self, u: torch.Tensor, want_tangent: bool, summary: torch.Tensor):
+        """evaluate without a host synchronisation (capturable in a CUDA
+        graph): results in internal_view() / values_view(), and summary (5
+        doubles on the device): energy, gross, yielding points, lowest
+        failing element (-1: none), its code."""
+        _capi.check(_capi.lib().sbk_system_enqueue(self._h, _ptr(u), int(want_tangent), _ptr(summary)))
+
+    def internal_view(self) -> torch.Tensor:
+        """The f_int buffer (num_dofs) every evaluation writes (known after
+        the first evaluate)."""
+        return self._internal_view
+
+    def values_view(self) -> torch.Tensor:
+        """The tangent value buffer (nnz, CSC) every evaluation with the
+        tangent writes (known after the first evaluate with the tangent)."""
+        return self._values_view
+
     def set_schedule(self, by_cost: bool = True):
         """Walk the elements grouped by the cost of their last evaluation (the
         default) or in mesh order; no result depends on it."""
@@ -257,6 +279,9 @@ class NonlinearSystem:
         _capi.check(st)
         internal = device_view(ev.internal_dev, (self.num_dofs,))
         values = device_view(ev.values_dev, (self.nnz,)) if want_tangent else None
+        self._internal_view = internal
+        if values is not None:
+            self._values_view = values
         return Evaluation(internal=internal, residual=internal, tangent=values, energy=float(ev.energy),
                           gross=float(ev.gross), yielding_points=int(ev.yielding_points), system=self)
 
