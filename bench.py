@@ -32,6 +32,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 PKG = "springback-precomp_b200"
@@ -209,6 +211,85 @@ def run_reference(args, rank, world):
     return 0
 
 
+def run_batched(args, rank, world):
+    """The batched design sweep (the 64 uneven parts of the sweep
+    configuration: 20k-150k elements each, material of the microbenchmark):
+    one evaluation of all parts as one system, plain and as a replayed CUDA
+    graph, against the same parts evaluated one system at a time (each
+    evaluate followed by its host read, as a per-part driver does). Parts are
+    seeded sheets of 2 layers with aspect ratios 1.0-1.6 under a bending
+    field; their points start virgin."""
+    import torch
+
+    if world > 1 and rank != 0:
+        return 0
+    pkg = importlib.import_module(PKG)
+    batch_mod = importlib.import_module(PKG + ".batch")
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(20260)
+    mat = pkg.material.hill_chaboche_sheet()
+    meshes, us = [], []
+    for _ in range(args.parts):
+        ne = int(rng.uniform(20000, 150000))
+        aspect = rng.uniform(1.0, 1.6)
+        ny = max(1, int(round(np.sqrt(ne / 2 / aspect))))
+        nx = max(1, int(round(ne / 2 / ny)))
+        m = pkg.structured_hex_mesh(nx, ny, 2, nx * 4e-5, ny * 4e-5, 1e-3)
+        x = m.coords
+        u = np.zeros_like(x)
+        span = x[:, 0].max() - x[:, 0].min()
+        u[:, 2] = -0.02 * (x[:, 0] - x[:, 0].mean()) ** 2 / span
+        u[:, 0] = 0.002 * (x[:, 2] - x[:, 2].mean()) * (x[:, 0] - x[:, 0].mean()) / span
+        meshes.append(m)
+        us.append(u.reshape(-1))
+    total = sum(m.num_elements for m in meshes)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(reps):
+            fn()
+        s1.record()
+        torch.cuda.synchronize()
+        return s0.elapsed_time(s1) / reps
+
+    # One part at a time.
+    systems = [pkg.NonlinearSystem(m, mat) for m in meshes]
+    u_dev = [torch.tensor(u, device=dev) for u in us]
+
+    def sequential():
+        for sy, u in zip(systems, u_dev):
+            sy.evaluate(u, 0.0, True)
+
+    seq_ms = timed(sequential, max(1, args.steps // 4))
+    yielding = sum(sy.evaluate(u, 0.0, True).yielding_points for sy, u in zip(systems, u_dev))
+    del systems
+    torch.cuda.empty_cache()
+    batch = batch_mod.PartBatch(meshes, mat)
+    ub = torch.tensor(np.concatenate(us), device=dev)
+    tune = batch.autotune(ub, candidates=(2, 4, 8))
+    bat_ms = timed(lambda: batch.evaluate(ub, True), max(1, args.steps // 4))
+    graph = batch_mod.GraphedEvaluation(batch.system, ub)
+    gr_ms = timed(graph.replay, max(1, args.steps // 4))
+    line = {"metric": "batched design sweep: part evaluations/s (FP64)", "value": args.parts / (gr_ms / 1e3),
+            "unit": "parts/s", "n_gpus": 1, "steps": max(1, args.steps // 4), "warmup": 1,
+            "ms_per_step": gr_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"{args.parts} sheet parts of 20k-150k IM Hex8 ({total} elements), Hill48 + "
+                                   f"Chaboche + Voce, logarithmic strain, bending from virgin points; one step = "
+                                   f"one evaluation of every part with its tangent"},
+            "sequential_ms": seq_ms, "batched_ms": bat_ms, "graph_ms": gr_ms,
+            "speedup_batched": seq_ms / bat_ms, "speedup_graph": seq_ms / gr_ms,
+            "elements_per_s_graph": total / (gr_ms / 1e3), "autotune_ms": tune,
+            "chosen_elements_per_block": batch.chosen_elements_per_block,
+            "yielding_fraction": yielding / (8.0 * total)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def config(args, world):
     return {"workload": f"element-kernel microbenchmark: {args.nx}x{args.ny}x{args.nz} IM Hex8 sheet "
                         f"(0.04x0.04x0.5 mm cells), 2x2x2 points, Hill48 r=(0.73,0.80,0.70) + Chaboche "
@@ -233,6 +314,10 @@ def main():
     p.add_argument("--epb", type=int, default=0, help="elements per block of the element kernel (0: default)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--workload", default="microbench", choices=["microbench", "batched"],
+                   help="batched: the design-sweep batch (64 parts of 20k-150k elements) in one launch against the "
+                        "same parts evaluated one at a time")
+    p.add_argument("--parts", type=int, default=64)
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -240,6 +325,8 @@ def main():
     rank, world, local = replicas.rank_env()
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "batched":
+        return run_batched(args, rank, world)
 
     import torch
 

@@ -662,7 +662,7 @@ int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const 
   TRY(dalloc(&s->internal, static_cast<size_t>(s->nn) * 3));
   TRY(dalloc(&s->product, static_cast<size_t>(s->nn) * 3));
   TRY(dalloc(&s->order, static_cast<size_t>(s->ne)));
-  TRY(dalloc(&s->sched, sbk::schedule_scratch_ints()));
+  TRY(dalloc(&s->sched, sbk::schedule_scratch_ints(s->ne)));
   TRY(dalloc(&s->scratch, sbk::assemble_scratch_doubles()));
   TRY(dalloc(&s->scalars, 4));
   TRY(dalloc(&s->missing, 1));

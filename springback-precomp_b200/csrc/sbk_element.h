@@ -72,7 +72,7 @@ int launch_stiffness_gross(int64_t nn, const int32_t* outer, const int32_t* inne
 // that elements of alike cost share a warp. scratch: schedule_scratch_ints().
 int launch_schedule(int64_t ne, int nq, const int32_t* iterations, const uint8_t* yield, int32_t* scratch,
                     int32_t* order, cudaStream_t stream);
-size_t schedule_scratch_ints();
+size_t schedule_scratch_ints(int64_t ne);
 // add_node_block for n blocks, in list order.
 int launch_add_node_blocks(const int32_t* outer, const int32_t* inner, double* values, int32_t n,
                            const int32_t* nodes, const double* blocks, int32_t* missing, cudaStream_t stream);

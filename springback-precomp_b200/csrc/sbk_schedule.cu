@@ -8,10 +8,12 @@
 // much of their behaviour from one Newton iteration to the next, so after
 // each evaluation the elements are bucketed by what their last evaluation
 // cost (local iterations, yielding points) and the next launch walks them
-// bucket by bucket. No result depends on the order: every output of the
-// element kernel is indexed by the element, and the assembly sums in
-// element order. Within a bucket the order is that of the atomic
-// reservations, which may vary from run to run; the results do not.
+// bucket by bucket. The bucketing is a stable counting sort: within a
+// bucket the elements keep their mesh order, so that a warp's elements stay
+// neighbours where their costs agree (their nodes are then shared in cache),
+// and the order is the same on every run. No result depends on the order:
+// every output of the element kernel is indexed by the element, and the
+// assembly sums in element order.
 #include <cuda_runtime.h>
 
 #include "sbk_element.h"
@@ -22,6 +24,7 @@ namespace {
 constexpr int kIterationBuckets = 32;             // local iterations 0..31 (the limit is 25)
 constexpr int kYieldBuckets = SBK_MAX_POINTS + 1;  // yielding points 0..32
 constexpr int kBuckets = kIterationBuckets * kYieldBuckets;
+constexpr int kChunk = 1024;                       // elements per block, in mesh order
 
 __device__ __forceinline__ int bucket_of(int64_t e, int nq, const int32_t* iterations, const uint8_t* yield) {
   int it = iterations[e];
@@ -31,54 +34,84 @@ __device__ __forceinline__ int bucket_of(int64_t e, int nq, const int32_t* itera
   return it * kYieldBuckets + y;
 }
 
-__global__ void __launch_bounds__(256) schedule_count_kernel(int64_t ne, int nq, const int32_t* __restrict__ iterations,
+// Pass 1: the bucket counts of every chunk, bucket-major (count[k * nb + b]).
+__global__ void __launch_bounds__(256) schedule_count_kernel(int64_t ne, int nq, int64_t nb,
+                                                             const int32_t* __restrict__ iterations,
                                                              const uint8_t* __restrict__ yield,
-                                                             int32_t* __restrict__ count) {
+                                                             int32_t* __restrict__ count, int16_t* __restrict__ keys) {
   __shared__ int32_t h[kBuckets];
   for (int i = threadIdx.x; i < kBuckets; i += blockDim.x) h[i] = 0;
   __syncthreads();
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x)
-    atomicAdd(&h[bucket_of(e, nq, iterations, yield)], 1);
+  const int64_t b = blockIdx.x;
+  const int64_t lo = b * kChunk, hi = lo + kChunk < ne ? lo + kChunk : ne;
+  for (int64_t e = lo + threadIdx.x; e < hi; e += blockDim.x) {
+    const int k = bucket_of(e, nq, iterations, yield);
+    keys[e] = (int16_t)k;
+    atomicAdd(&h[k], 1);
+  }
   __syncthreads();
-  for (int i = threadIdx.x; i < kBuckets; i += blockDim.x)
-    if (h[i]) atomicAdd(&count[i], h[i]);
+  for (int i = threadIdx.x; i < kBuckets; i += blockDim.x) count[(int64_t)i * nb + b] = h[i];
 }
 
-// Exclusive prefix sum of the bucket counts into the bucket cursors.
-__global__ void schedule_scan_kernel(const int32_t* __restrict__ count, int32_t* __restrict__ cursor) {
-  if (threadIdx.x != 0) return;
-  int32_t run = 0;
-  for (int i = 0; i < kBuckets; ++i) {
-    cursor[i] = run;
-    run += count[i];
+// Pass 2: exclusive prefix sum of the counts in bucket-major order, by one
+// block: each thread sums a contiguous stretch, then the stretches' totals
+// are scanned.
+__global__ void __launch_bounds__(1024) schedule_scan_kernel(int64_t n, int32_t* __restrict__ count) {
+  __shared__ int32_t part[1024];
+  const int64_t per = (n + blockDim.x - 1) / blockDim.x;
+  const int64_t lo = threadIdx.x * per, hi = lo + per < n ? lo + per : n;
+  int32_t s = 0;
+  for (int64_t i = lo; i < hi; ++i) s += count[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int32_t run = 0;
+    for (int i = 0; i < (int)blockDim.x; ++i) {
+      const int32_t v = part[i];
+      part[i] = run;
+      run += v;
+    }
+  }
+  __syncthreads();
+  int32_t run = part[threadIdx.x];
+  for (int64_t i = lo; i < hi; ++i) {
+    const int32_t v = count[i];
+    count[i] = run;
+    run += v;
   }
 }
 
-__global__ void __launch_bounds__(256) schedule_place_kernel(int64_t ne, int nq, const int32_t* __restrict__ iterations,
-                                                             const uint8_t* __restrict__ yield,
-                                                             int32_t* __restrict__ cursor, int32_t* __restrict__ order) {
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < ne; e += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t pos = atomicAdd(&cursor[bucket_of(e, nq, iterations, yield)], 1);
-    order[pos] = (int32_t)e;
+// Pass 3: each chunk places its elements in mesh order at its buckets'
+// offsets (one thread walks the chunk, so the order within a bucket is the
+// mesh order).
+__global__ void schedule_place_kernel(int64_t ne, int64_t nb, const int16_t* __restrict__ keys,
+                                      const int32_t* __restrict__ start, int32_t* __restrict__ order) {
+  if (threadIdx.x != 0) return;
+  const int64_t b = blockIdx.x;
+  const int64_t lo = b * kChunk, hi = lo + kChunk < ne ? lo + kChunk : ne;
+  int32_t used[kBuckets];
+  for (int i = 0; i < kBuckets; ++i) used[i] = 0;
+  for (int64_t e = lo; e < hi; ++e) {
+    const int k = keys[e];
+    order[start[(int64_t)k * nb + b] + used[k]++] = (int32_t)e;
   }
 }
 
 }  // namespace
 
-size_t schedule_scratch_ints() { return 2 * kBuckets; }
+size_t schedule_scratch_ints(int64_t ne) {
+  const int64_t nb = (ne + kChunk - 1) / kChunk;
+  return (size_t)(kBuckets * (nb > 0 ? nb : 1)) + (size_t)(ne + 1) / 2;  // the counts, then int16 keys
+}
 
 int launch_schedule(int64_t ne, int nq, const int32_t* iterations, const uint8_t* yield, int32_t* scratch,
                     int32_t* order, cudaStream_t stream) {
   if (ne <= 0) return 0;
-  int32_t* count = scratch;
-  int32_t* cursor = scratch + kBuckets;
-  cudaError_t err = cudaMemsetAsync(count, 0, kBuckets * sizeof(int32_t), stream);
-  if (err != cudaSuccess) return (int)err;
-  int64_t blocks = (ne + 255) / 256;
-  if (blocks > 148 * 4) blocks = 148 * 4;
-  schedule_count_kernel<<<(unsigned)blocks, 256, 0, stream>>>(ne, nq, iterations, yield, count);
-  schedule_scan_kernel<<<1, 32, 0, stream>>>(count, cursor);
-  schedule_place_kernel<<<(unsigned)blocks, 256, 0, stream>>>(ne, nq, iterations, yield, cursor, order);
+  const int64_t nb = (ne + kChunk - 1) / kChunk;
+  int16_t* keys = reinterpret_cast<int16_t*>(scratch + (int64_t)kBuckets * nb);
+  schedule_count_kernel<<<(unsigned)nb, 256, 0, stream>>>(ne, nq, nb, iterations, yield, scratch, keys);
+  schedule_scan_kernel<<<1, 1024, 0, stream>>>((int64_t)kBuckets * nb, scratch);
+  schedule_place_kernel<<<(unsigned)nb, 32, 0, stream>>>(ne, nb, keys, scratch, order);
   return (int)cudaGetLastError();
 }
 
