@@ -270,7 +270,7 @@ def run_batched(args, rank, world):
     torch.cuda.empty_cache()
     batch = batch_mod.PartBatch(meshes, mat)
     ub = torch.tensor(np.concatenate(us), device=dev)
-    tune = batch.autotune(ub, candidates=(2, 4, 8))
+    tune = batch.autotune(ub, candidates=(4, 8, 16))
     bat_ms = timed(lambda: batch.evaluate(ub, True), max(1, args.steps // 4))
     graph = batch_mod.GraphedEvaluation(batch.system, ub)
     gr_ms = timed(graph.replay, max(1, args.steps // 4))

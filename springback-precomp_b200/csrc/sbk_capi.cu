@@ -706,7 +706,7 @@ int sbk_system_set_schedule(sbk_system* sys, int by_cost) {
 }
 
 int sbk_system_set_elements_per_block(sbk_system* sys, int epb) {
-  if (!sys || epb < 0 || epb > 16) return fail(SBK_ERR_ARGUMENT, "bad elements per block");
+  if (!sys || epb < 0 || epb > 32) return fail(SBK_ERR_ARGUMENT, "bad elements per block");
   sys->elements_per_block = epb;
   return SBK_OK;
 }

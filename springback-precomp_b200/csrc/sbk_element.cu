@@ -975,7 +975,7 @@ struct Local {
 // ---- the condensation ---------------------------------------------------------
 
 template <int G>
-__global__ void __launch_bounds__(128) element_kernel(const __grid_constant__ Params p, int64_t ne, bool batch,
+__global__ void __launch_bounds__(256) element_kernel(const __grid_constant__ Params p, int64_t ne, bool batch,
                                                       const double* __restrict__ coords,
                                                       const int32_t* __restrict__ conn, const double* __restrict__ u,
                                                       const double* __restrict__ state,
@@ -1439,13 +1439,21 @@ int launch_elements(const Params& p, int64_t ne, const double* coords, const int
                     int32_t* code, int32_t* first_failure, bool batch, int elements_per_block,
                     const int32_t* order, cudaStream_t stream) {
   if (p.nq <= 8) {
-    const int epb = elements_per_block > 0 ? elements_per_block : 4;
+    // At most what 227 KB of shared memory and 256 threads hold.
+    const int most = (int)((227 * 1024) / sizeof(ElemShared<8>)) < 32 ? (int)((227 * 1024) / sizeof(ElemShared<8>)) : 32;
+    // The default, 16 elements (4 warps) per block and so one block per SM:
+    // the four warps of a block start together and, their elements being
+    // alike under the schedule, stay close enough in the code to share its
+    // instruction fetches (1.8x over one-warp blocks on the sheet
+    // microbenchmark; 5 to 7 warps per block are slower).
+    int epb = elements_per_block > 0 ? elements_per_block : 16;
+    if (epb > most) epb = most;
     return launch_g<8>(p, ne, coords, conn, u, state, alpha_n, want_tangent, force, tangent, energy, trial,
                        alpha_out, yield, iterations, code, first_failure, batch, epb, order, stream);
   }
   // Rules of 9 to 32 points (the sheet rules 2 x 2 x 3..7, the 3 x 3 x 3
   // cube): a warp per element, lane = point.
-  const int epb = elements_per_block > 0 ? (elements_per_block < 4 ? elements_per_block : 4) : 1;
+  const int epb = elements_per_block > 0 ? (elements_per_block < 8 ? elements_per_block : 8) : 4;
   return launch_g<32>(p, ne, coords, conn, u, state, alpha_n, want_tangent, force, tangent, energy, trial,
                       alpha_out, yield, iterations, code, first_failure, batch, epb, order, stream);
 }
