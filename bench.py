@@ -40,10 +40,10 @@ PKG = "springback-precomp_b200"
 METRIC = "Hex8 tangent+residual+assembly elem/s (FP64)"
 # DRAM bytes (read + write) per element of one element-kernel launch, from
 # the ncu capture of the same construction at 80,000 elements
-# (profiles/element_kernel_microbench.md: 29.16 GB / 80,000); the traffic
+# (profiles/element_kernel_microbench.md: 16.11 GB / 80,000); the traffic
 # grows with the elements, so a launch of ne elements moves about ne times
 # this.
-K1_DRAM_BYTES_PER_ELEMENT = 29.16e9 / 80000
+K1_DRAM_BYTES_PER_ELEMENT = 16.11e9 / 80000
 UNIT = "elem/s"
 
 
