@@ -1,7 +1,8 @@
 // K1: the incompatible-mode Hex8 element on the GPU.
 //
-// One group of G lanes (G = 8 for rules of up to 8 points, 16 or 32 for
-// larger ones) evaluates one element; a 32-lane warp holds 32 / G elements.
+// One group of G lanes (G = 8 for rules of up to 8 points, 32 for rules of
+// 9 to 32 points) evaluates one element; a 32-lane warp holds 32 / G
+// elements, and a block of four warps 16 (or 4) elements by default.
 // Lane q owns integration point q: its kinematics, its return map and its
 // share of K_aa, which a shuffle reduce-scatter sums over the group into
 // shared memory. The element-level work of the local Newton iteration - the
