@@ -3,8 +3,8 @@ of the product. It stands in for the reference's FormingAnalysis::run
 (src/fem/Forming.cpp:686-1262), which calls the element loop and the contact
 every Newton iteration: it runs a committed forming deck of the reference
 through this package's NonlinearSystem and ToolContact on the GPU, solving
-the linear systems on the host with scipy (the reference's own sparse solver
-is outside the graft).
+the linear systems with scipy on the host, or densely on the GPU for a
+larger sheet (the reference's own sparse solver is outside the graft).
 
 What it restates of the driver, because the converged states depend on it:
 the step partition (prescribed DOFs held at their values, Forming.cpp:804-821),
@@ -96,13 +96,25 @@ class FormingRun:
         self.mesh = pkg.HexMesh(self.nodes, self.elements)
         m = fixture["material"]
         pl = m["plasticity"]
+        extra = {}
+        if pl.get("yield_criterion") == "hill48":
+            an = pl["anisotropy"]
+            extra.update(criterion="hill48", r0=an["r0"], r45=an["r45"], r90=an["r90"],
+                         rolling_direction=tuple(an.get("rolling_direction", (1.0, 0.0, 0.0))),
+                         sheet_normal=tuple(an.get("sheet_normal", (0.0, 0.0, 1.0))))
+        if pl.get("backstresses"):
+            extra["backstresses"] = tuple((b["modulus"], b["recovery"]) for b in pl["backstresses"])
         self.material = pkg.Material(m["youngs_modulus"], m["poisson_ratio"], yield_stress=pl["yield_stress"],
                                      hardening_modulus=pl["hardening_modulus"],
                                      kinematic_hardening_modulus=pl.get("kinematic_hardening_modulus", 0.0),
                                      saturation_stress=pl["saturation_stress"],
-                                     saturation_rate=pl["saturation_rate"], name=m["name"])
+                                     saturation_rate=pl["saturation_rate"], name=m["name"], **extra)
         kin = {"finite_logarithmic": "logarithmic", "finite": "finite", "small_strain": "small"}[fixture["kinematics"]]
-        self.system = pkg.NonlinearSystem(self.mesh, self.material, kinematics=kin)
+        integ = fixture.get("model", {}).get("integration", {})
+        tp = int(integ.get("thickness_points", 0))
+        axis = "xyz".index(integ.get("thickness_direction", "z"))
+        self.system = pkg.NonlinearSystem(self.mesh, self.material, kinematics=kin, thickness_points=tp,
+                                          thickness_axis=axis)
         extent = self.nodes.max(0) - self.nodes.min(0)
         self.tol = 1e-9 * float(np.linalg.norm(extent))
         self.tools = []
@@ -137,11 +149,18 @@ class FormingRun:
                 self.system.add_node_blocks(cev.nodes, cev.blocks)
         return ev, r, fz
 
-    def _matrix(self, ev, free):
+    def _solve(self, ev, free, rhs):
+        """K_ff x = rhs: scipy's sparse LU on the host, or for a larger sheet
+        a dense LU on the GPU (torch)."""
         n = self.mesh.num_dofs
-        k = scipy.sparse.csc_matrix((ev.tangent.cpu().numpy(), self.system.inner.cpu().numpy(),
-                                     self.system.outer.cpu().numpy()), shape=(n, n))
-        return k[free][:, free].tocsc()
+        if len(free) <= 3000:
+            k = scipy.sparse.csc_matrix((ev.tangent.cpu().numpy(), self.system.inner.cpu().numpy(),
+                                         self.system.outer.cpu().numpy()), shape=(n, n))
+            return scipy.sparse.linalg.spsolve(k[free][:, free].tocsc(), rhs)
+        k = torch.sparse_csc_tensor(self.system.outer.long(), self.system.inner.long(), ev.tangent, (n, n))
+        f = torch.as_tensor(free, device=self.dev)
+        kff = k.to_dense()[f][:, f]
+        return torch.linalg.solve(kff, torch.as_tensor(rhs, device=self.dev)).cpu().numpy()
 
     def _speed(self, t, active):
         v = 0.0
@@ -215,7 +234,7 @@ class FormingRun:
         for it in range(60):
             ev, r, _ = self._residual(trial, t1, active, True)
             rf = r[free] - ramp * r0
-            du = scipy.sparse.linalg.spsolve(self._matrix(ev, free), -rf)
+            du = self._solve(ev, free, -rf)
             norm0 = np.linalg.norm(rf)
             alpha = 1.0
             for _ in range(12):  # backtrack on |R| where a full step overshoots

@@ -13,6 +13,13 @@ kinematics, tool, steps and their boundary regions), the nodal
 displacements at the end of each step (17 significant digits in the
 reference's CSV output) and the tool force of every forming increment.
 
+kin_h0833.json + kin_h0833.npz: the reference's forming run
+benchmarks/physics_audit/challenge/cases/kin_h0833 - a 48 x 48 x 1
+incompatible-mode sheet with the 2 x 2 x 5 rule, Hill48 with two Chaboche
+backstresses and Voce hardening, a spherical tool on a 113-knot spiral
+path - the deck's parts in the JSON (the tool path read from its CSV), the
+mesh and the step-end displacements in the npz.
+
 materials.json: the hardening parameters the reference's own Python
 (python/precomp/materials.py) derives - its built-in library (Hollomon
 fits) and the Swift law of the 40x40x2 forming sheet - plus the material
@@ -77,8 +84,45 @@ def strip(ref_root: str, case: str = "strip_h2_im_nz4") -> None:
         f.write("\n")
 
 
+def challenge(ref_root: str, case: str = "kin_h0833") -> None:
+    import csv
+
+    import numpy as np
+
+    base = os.path.join(ref_root, "benchmarks/physics_audit/challenge/cases", case)
+    deck = json.load(open(os.path.join(base, "deck", "deck.json")))
+    mesh = json.load(open(os.path.join(base, "output", "mesh.json")))
+    summary = json.load(open(os.path.join(base, "output", "summary.json")))
+    tools = []
+    for t in deck["forming"]["tools"]:
+        t = dict(t)
+        tr = t["trajectory"]
+        if "file" in tr:
+            rows = list(csv.DictReader(open(os.path.join(base, "deck", tr["file"]))))
+            t["trajectory"] = {"times": [float(r["t"]) for r in rows],
+                               "points": [[float(r["x"]), float(r["y"]), float(r["z"])] for r in rows]}
+        tools.append(t)
+    steps, us = [], []
+    for k, st in enumerate(deck["forming"]["steps"], start=1):
+        rows = list(csv.DictReader(open(os.path.join(base, "output", f"step_{k}_{st['name']}_nodes.csv"))))
+        us.append([[float(r["ux"]), float(r["uy"]), float(r["uz"])] for r in rows])
+        steps.append({"deck": st, "increments": summary["steps"][k - 1]["increments"],
+                      "cuts": summary["steps"][k - 1]["cuts"]})
+    forces = [{k: r[k] for k in ("step", "increment", "t", "cx", "cz", "fx", "fz", "active_nodes")}
+              for r in csv.DictReader(open(os.path.join(base, "output", "tool_forces.csv")))]
+    out = {"source": os.path.relpath(base, ref_root), "material": deck["material"], "model": deck["model"],
+           "kinematics": deck["forming"]["kinematics"], "tools": tools, "steps": steps, "tool_forces": forces,
+           "analysis": summary["analysis"], "arrays": case + ".npz"}
+    with open(os.path.join(HERE, f"{case}.json"), "w") as f:
+        json.dump(out, f, separators=(",", ":"))
+        f.write("\n")
+    np.savez_compressed(os.path.join(HERE, f"{case}.npz"), nodes=np.array(mesh["nodes_m"], dtype=np.float64),
+                        elements=np.array(mesh["elements"], dtype=np.int32), u=np.array(us, dtype=np.float64))
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     main(root)
     for case in ("strip_h2_im_nz4", "strip_h1_im_nz4", "plate_h2_im_mu0.1_drag3"):
         strip(root, case)
+    challenge(root)

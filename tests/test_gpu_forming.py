@@ -35,9 +35,21 @@ CASES = ["strip_h2_im_nz4", "strip_h1_im_nz4", "plate_h2_im_mu0.1_drag3"]
 HEIGHT_TOL = 1.0e-8  # [m]: 1e-5 mm
 
 
+def load_fixture(case):
+    """A reference run's fixture; the larger ones keep their mesh and step
+    displacements in an npz beside the JSON."""
+    fx = json.load(open(os.path.join(GOLDEN, case + ".json")))
+    if "arrays" in fx:
+        a = np.load(os.path.join(GOLDEN, fx["arrays"]))
+        fx["nodes"], fx["elements"] = a["nodes"], a["elements"]
+        for k, st in enumerate(fx["steps"]):
+            st["u"] = a["u"][k]
+    return fx
+
+
 @pytest.fixture(scope="module", params=CASES)
 def run(request, pkg, cuda):
-    fx = json.load(open(os.path.join(GOLDEN, request.param + ".json")))
+    fx = load_fixture(request.param)
     r = FormingRun(pkg, fx, cuda)
     results = []
     for k in range(len(fx["steps"])):
