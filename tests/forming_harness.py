@@ -13,9 +13,11 @@ increment schedule (the tool travel per increment and the stations,
 :1149-1163) and the commit of every converged increment (:1208-1215). What
 it does not restate, because it only changes the path to the same converged
 state: the predictor, the energy line search (a residual backtracking here),
-the semismooth anticipation and the tolerances (the iteration here runs to
-a correction of 1e-13 m (1e-11 m after 40 iterations), well inside the reference's
-relative 1e-6).
+and the tolerances (the iteration here runs to a correction of 1e-13 m,
+1e-11 m after 40 iterations, well inside the reference's relative 1e-6). Its
+Newton iteration follows the reference's: the semismooth anticipation of
+contact and the line search on du . R, which keep the iterates where every
+element's local iteration converges.
 """
 from __future__ import annotations
 
@@ -226,33 +228,90 @@ class FormingRun:
         return StepResult(u=self.u.copy(), increments=count, tool_fz=fz_list)
 
     def _newton(self, t0, t1, s1, free, r0, active):
+        """One increment: Newton's method as Forming.cpp:900-1135 runs it -
+        the semismooth anticipation of nodes the correction drives into a
+        tool (:1017-1046), the line search on the energy du . R(a) with the
+        full step's evaluation kept (:916-960, :1057-1075) - iterated here to
+        a correction of 1e-13 m."""
         ramp = 1.0 - s1
         trial = self.u.copy()
+        any_tool = self.contact is not None and any(active)
         if self.contact is not None:
             self.contact.begin_increment(torch.tensor(self.u, device=self.dev), t0, t1, active,
                                          2.0 * 1e-3 + 2.0 * self.last_du + self.min_size)
-        for it in range(60):
-            ev, r, _ = self._residual(trial, t1, active, True)
+
+        def g_at(x, du, tangent):
+            try:
+                ev, r, _ = self._residual(x, t1, active, tangent)
+            except self.pkg.SolverError:
+                return None, None, np.nan
+            return ev, r, float(du @ (r[free] - ramp * r0))
+
+        history = []
+        have = None  # the full step's evaluation with its tangent, when kept
+        for it in range(300):
+            if have is None:
+                ev, r, _ = self._residual(trial, t1, active, True)
+            else:
+                ev, r = have
+            have = None
             rf = r[free] - ramp * r0
             du = self._solve(ev, free, -rf)
-            norm0 = np.linalg.norm(rf)
+            if any_tool:
+                du_full = np.zeros(self.mesh.num_dofs)
+                du_full[free] = du
+                extra = torch.zeros(self.mesh.num_dofs, dtype=torch.float64, device=self.dev)
+                added, nodes, blocks = self.contact.anticipate(torch.tensor(trial, device=self.dev),
+                                                               torch.tensor(du_full, device=self.dev), t1, extra)
+                if added > 0:
+                    n0 = len(nodes) - added
+                    self.system.add_node_blocks(nodes[n0:], blocks[n0:])
+                    again = self._solve(ev, free, -(rf + extra.cpu().numpy()[free]))
+                    if np.all(np.isfinite(again)):
+                        du = again
+            g0 = float(du @ rf)
             alpha = 1.0
-            for _ in range(12):  # backtrack on |R| where a full step overshoots
+            if g0 < 0.0:
                 probe = trial.copy()
-                probe[free] += alpha * du
-                try:
-                    _, rp, _ = self._residual(probe, t1, active, False)
-                    if np.linalg.norm(rp[free] - ramp * r0) <= max(norm0, 1e-6) * 1.0001 or alpha < 1e-3:
+                probe[free] += du
+                nxt, r_next, g1 = g_at(probe, du, True)
+                a_hi, g_hi = 1.0, g1
+                for _ in range(6):
+                    if np.isfinite(g_hi):
                         break
-                except self.pkg.SolverError:
-                    pass
-                alpha *= 0.5
+                    a_hi *= 0.5
+                    probe = trial.copy()
+                    probe[free] += a_hi * du
+                    nxt, r_next, g_hi = None, None, g_at(probe, du, False)[2]
+                if not np.isfinite(g_hi) or abs(g_hi) <= 0.8 * abs(g0) or g_hi < 0.0:
+                    alpha = a_hi
+                else:
+                    a_lo, g_lo, best = 0.0, g0, a_hi
+                    for _ in range(5):
+                        a = min(max(a_lo - g_lo * (a_hi - a_lo) / (g_hi - g_lo), 0.1 * a_hi), a_hi)
+                        probe = trial.copy()
+                        probe[free] += a * du
+                        nxt, ga = None, g_at(probe, du, False)[2]
+                        if not np.isfinite(ga):
+                            a_hi, g_hi = a, abs(g0)
+                            continue
+                        best = a
+                        if abs(ga) <= 0.8 * abs(g0):
+                            break
+                        if ga < 0.0:
+                            a_lo, g_lo = a, ga
+                        else:
+                            a_hi, g_hi = a, ga
+                    alpha = best
+                if alpha == 1.0 and nxt is not None:
+                    have = (nxt, r_next)  # the full step's evaluation, with its tangent: the next iteration's
             trial[free] += alpha * du
             step = alpha * np.abs(du).max()
+            history.append((float(np.linalg.norm(rf)), float(step), alpha))
             if (alpha == 1.0 and step <= 1e-13) or (it >= 40 and step <= 1e-11):
                 break
         else:
-            raise AssertionError(f"the increment to t = {t1} did not converge")
+            raise AssertionError(f"the increment to t = {t1} did not converge: (|R|, step, alpha) {history[-8:]}")
         # The accepted state's own evaluation makes its trial history the one committed.
         _, _, fz = self._residual(trial, t1, active, False)
         self.system.commit()

@@ -1,7 +1,7 @@
 """End to end against forming runs the reference committed
-(benchmarks/physics_audit/calculix/punch/<case>/sparlab), all
-incompatible-mode Hex8 under logarithmic strain with J2 and Voce hardening
-and Coulomb friction 0.1:
+(benchmarks/physics_audit/calculix/punch/<case>/sparlab and
+benchmarks/physics_audit/challenge/cases/<case>), all incompatible-mode Hex8
+under logarithmic strain with Coulomb friction 0.1:
 
 - strip_h2_im_nz4: a 20 x 1 x 4 strip under a cylindrical punch pressed
   4 mm into it, the tool taken away over 20 increments and the clamps
@@ -10,7 +10,12 @@ and Coulomb friction 0.1:
   reference's Newton iterations cut four times;
 - plate_h2_im_mu0.1_drag3: a clamped 20 x 20 x 2 plate under a spherical
   punch pressed 3 mm in and dragged 3 mm sideways, released onto 3-2-1
-  supports (two cuts).
+  supports (two cuts);
+- kin_h0833 (benchmarks/physics_audit/challenge/cases): a 48 x 48 x 1
+  sheet with the 2 x 2 x 5 rule, Hill48 with two Chaboche backstresses and
+  Voce hardening, a spherical tool on a 113-knot spiral path over 395
+  increments (three cuts), released onto 3-2-1 supports - the element
+  microbenchmark's law class; about three minutes on a B200.
 
 The element loop and the contact are this package's, on the GPU; the
 Newton driver around them is the test harness in forming_harness.py, which
@@ -31,7 +36,7 @@ from forming_harness import FormingRun
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-CASES = ["strip_h2_im_nz4", "strip_h1_im_nz4", "plate_h2_im_mu0.1_drag3"]
+CASES = ["strip_h2_im_nz4", "strip_h1_im_nz4", "plate_h2_im_mu0.1_drag3", "kin_h0833"]
 HEIGHT_TOL = 1.0e-8  # [m]: 1e-5 mm
 
 
