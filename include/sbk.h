@@ -142,9 +142,9 @@ int sbk_system_destroy(sbk_system* sys);
 int sbk_system_set_stream(sbk_system* sys, void* stream);
 
 /* Launch shape of the element kernel: elements per thread block (0: the
- * default, 16 for rules of up to 8 points - four warps - and 4 for larger
- * rules; at most what 227 KB of shared memory holds; the batch autotuner
- * sets it). */
+ * default, 16 for rules of up to 8 points - four warps - and 8 for larger
+ * rules - eight warps; at most what 227 KB of shared memory and 256 threads
+ * hold; the batch autotuner sets it). */
 int sbk_system_set_elements_per_block(sbk_system* sys, int elements_per_block);
 
 /* The element schedule (no counterpart in the reference, whose OpenMP loop

@@ -1453,8 +1453,11 @@ int launch_elements(const Params& p, int64_t ne, const double* coords, const int
                        alpha_out, yield, iterations, code, first_failure, batch, epb, order, stream);
   }
   // Rules of 9 to 32 points (the sheet rules 2 x 2 x 3..7, the 3 x 3 x 3
-  // cube): a warp per element, lane = point.
-  const int epb = elements_per_block > 0 ? (elements_per_block < 8 ? elements_per_block : 8) : 4;
+  // cube): a warp per element, lane = point. The default, 8 warps per block
+  // (the most 256 threads allow), for the same shared instruction fetches:
+  // 42 ms per 80,000 elements of the 2 x 2 x 5 rule, against 55 ms at 4
+  // warps and 80 ms at 1.
+  const int epb = elements_per_block > 0 ? (elements_per_block < 8 ? elements_per_block : 8) : 8;
   return launch_g<32>(p, ne, coords, conn, u, state, alpha_n, want_tangent, force, tangent, energy, trial,
                       alpha_out, yield, iterations, code, first_failure, batch, epb, order, stream);
 }
