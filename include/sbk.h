@@ -355,6 +355,71 @@ int sbk_evaluate_noalloc(const sbk_material* material, const sbk_rule* rule, int
                          int64_t nnz, double* internal_dev, double* values_dev, double* trial_dev,
                          double* alpha_out_dev, uint8_t* yield_dev, double* summary_dev, void* stream);
 
+/* ---- the free-free tangent: PartitionedFactor --------------------------- */
+typedef struct sbk_partition sbk_partition;
+
+/* A Dirichlet partition of an n-DOF model and its free-free block:
+ * PartitionedFactor::reset (src/fem/Forming.cpp:73-84) and ::build
+ * (Forming.cpp:213-241) on the full tangent's CSC pattern (outer_dev,
+ * inner_dev: device, as sbk_system_pattern gives it; structurally
+ * symmetric). free_host lists the num_free free DOFs, strictly ascending.
+ * The block keeps the entries whose row and column are free, in the full
+ * pattern's order. A fill-reducing order of the block for the sparse
+ * factorisation is computed here too, once (METIS nested dissection). A new
+ * pattern or a new free set is a new partition. */
+int sbk_partition_create(int64_t num_dofs, const int32_t* outer_dev, const int32_t* inner_dev, int64_t nnz,
+                         int32_t num_free, const int32_t* free_host, sbk_partition** out);
+int sbk_partition_destroy(sbk_partition* part);
+/* All later work goes to this stream (a cudaStream_t; NULL: default). */
+int sbk_partition_set_stream(sbk_partition* part, void* stream);
+/* The block's size and pattern: num_free + 1 column offsets and nnz_ff row
+ * indices (CSC, free numbering), copied to caller device buffers (either may
+ * be NULL). */
+int sbk_partition_info(const sbk_partition* part, int32_t* num_free, int64_t* nnz_ff);
+int sbk_partition_pattern(const sbk_partition* part, int32_t* outer_dev, int32_t* inner_dev);
+
+/* PartitionedFactor::assemble (Forming.cpp:89-98): the free-free values of
+ * the full tangent values_dev (nnz, device) into kff_dev (nnz_ff, device),
+ * in the block's CSC order; every value is copied, none summed. */
+int sbk_partition_assemble(sbk_partition* part, const double* values_dev, double* kff_dev);
+/* restrict(v, free) (Forming.cpp:748,838): out_dev[i] = full_dev[free[i]];
+ * add_to(full, free, v, alpha) (Forming.cpp:1036): full_dev[free[i]] +=
+ * alpha v_dev[i]. Device arrays. */
+int sbk_partition_restrict(sbk_partition* part, const double* full_dev, double* out_dev);
+int sbk_partition_add_to(sbk_partition* part, double* full_dev, const double* v_dev, double alpha);
+
+/* PartitionedFactor::factorize (Forming.cpp:100-160) of the free-free block
+ * of values_dev (the full tangent, device), where the reference takes
+ * CHOLMOD's supernodal Cholesky, then LDL^T, then LU (UMFPACK):
+ *   symmetric: a sparse Cholesky on the device (cuSOLVER), its pattern
+ *     analysed on the first call;
+ *   not symmetric, or a Cholesky that meets a non-positive pivot or whose
+ *     correction's backward error exceeds 1e-10: a dense LU with partial
+ *     pivoting on the device while the block has at most the dense limit of
+ *     rows (sbk_partition_set_dense_limit; default 20000, n^2 doubles);
+ *   larger: restarted GMRES preconditioned by the Cholesky of the block's
+ *     symmetric part, and a sparse QR on the device where that part is not
+ *     positive definite or GMRES stalls.
+ * SBK_ERR_SOLVER when the LU finds the block singular (a pivot below 1e-13
+ * of the largest entry), as the reference's factorize returns false. kind
+ * (may be NULL) receives the method of the next solve. */
+#define SBK_FACTOR_CHOLESKY 1
+#define SBK_FACTOR_QR 2
+#define SBK_FACTOR_GMRES 3
+#define SBK_FACTOR_LU 4
+int sbk_partition_factorize(sbk_partition* part, const double* values_dev, int symmetric, int* kind);
+/* Blocks of at most max_rows rows take the dense LU (0: never). */
+int sbk_partition_set_dense_limit(sbk_partition* part, int32_t max_rows);
+/* PartitionedFactor::solve (Forming.cpp:162-172): x_dev = K_ff^-1 b_dev
+ * (num_free each, device, free numbering). SBK_ERR_SOLVER when the block is
+ * singular (the QR's or LU's pivot below 1e-13 of the largest entry). */
+int sbk_partition_solve(sbk_partition* part, const double* b_dev, double* x_dev);
+/* names() and failures() (Forming.cpp:174-181) as counts, since the
+ * partition was made: factorisations solved by Cholesky, by preconditioned
+ * GMRES, by dense LU, by QR; Choleskys and GMRES runs that fell back;
+ * singular blocks; GMRES Krylov steps; solves. */
+int sbk_partition_counts(const sbk_partition* part, int64_t counts[9]);
+
 /* Last error message of this thread (never NULL). */
 const char* sbk_last_error(void);
 

@@ -305,6 +305,52 @@ def stiffness_gross(pat: dict, values, u, free) -> float:
     return float(np.sqrt(s))
 
 
+def free_free_block(pat: dict, values, free):
+    """The free-free block of a full CSC tangent as PartitionedFactor::reset
+    and ::build (src/fem/Forming.cpp:73-84, 213-241) and
+    Assembler::reduce_free_free (src/fem/Assembler.cpp:294-320) form it:
+    for every free column in ascending order, the entries of its free rows in
+    the full column's order. Returns the block's outer, inner, the full index
+    of each entry (the inverse of the reference's positions_ map) and its
+    values (assemble, Forming.cpp:89-98, copies them)."""
+    outer, inner = pat["outer"], pat["inner"]
+    n = len(outer) - 1
+    free = [int(d) for d in free]
+    mapping = [-1] * n  # reset: DOF -> free index
+    for i, d in enumerate(free):
+        mapping[d] = i
+    ff_outer = [0] * (len(free) + 1)
+    ff_inner, source = [], []
+    for col in range(n):
+        c = mapping[col]
+        if c < 0:
+            continue
+        for k in range(int(outer[col]), int(outer[col + 1])):
+            r = mapping[int(inner[k])]
+            if r < 0:
+                continue
+            ff_inner.append(r)
+            source.append(k)
+        ff_outer[c + 1] = len(ff_inner)
+    source = np.array(source, dtype=np.int64)
+    return (np.array(ff_outer, dtype=np.int32), np.array(ff_inner, dtype=np.int32), source,
+            np.asarray(values, dtype=np.float64)[source])
+
+
+def restrict(full, free) -> np.ndarray:
+    """restrict(full, dofs) (src/fem/NonlinearSystem.hpp:336-340)."""
+    return np.asarray(full, dtype=np.float64)[np.asarray(free, dtype=np.int64)]
+
+
+def add_to(full, free, part, factor) -> np.ndarray:
+    """add_to(full, dofs, part, factor) (src/fem/NonlinearSystem.hpp:342-347):
+    full[dofs[i]] += factor * part[i], returned as a new array."""
+    out = np.array(full, dtype=np.float64, copy=True)
+    for i, d in enumerate(free):
+        out[int(d)] += factor * float(part[i])
+    return out
+
+
 class Contact:
     """ToolContact restated: tools = list of dicts with shape ('sphere',
     'plane', 'cylinder'), radius, friction, tangential_ratio, normal, axis,

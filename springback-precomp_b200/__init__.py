@@ -2,7 +2,8 @@
 logarithmic-strain kinematics and the J2 / Hill48 return map under
 isotropic, Prager and Chaboche hardening, their local Newton iteration and
 static condensation, the assembly into the node-block pattern and penalty
-contact with rigid tools - hand-written CUDA for sm_100a in libsbk.so
+contact with rigid tools, and the free-free tangent of a Dirichlet
+partition fed to a device sparse factorisation - hand-written CUDA for sm_100a in libsbk.so
 (include/sbk.h), wrapped here behind the reference's own interfaces.
 """
 from . import _capi
@@ -10,10 +11,11 @@ from ._capi import SbkError, SolverError
 from .contact import ToolContact, Tool
 from .material import Material
 from .mesh import HexMesh, structured_hex_mesh
+from .partition import PartitionedFactor
 from .system import Evaluation, NonlinearSystem, element_batch
 
 __all__ = ["Material", "HexMesh", "structured_hex_mesh", "NonlinearSystem", "Evaluation", "element_batch",
-           "ToolContact", "Tool", "SbkError", "SolverError"]
+           "ToolContact", "Tool", "SbkError", "SolverError", "PartitionedFactor"]
 
 
 def library_path() -> str:

@@ -134,6 +134,18 @@ SIGNATURES = {
     "sbk_contact_history": (_I, [_P, _I32, _I32, ctypes.POINTER(_D), ctypes.POINTER(_I32)]),
     "sbk_evaluate_noalloc": (_I, [ctypes.POINTER(sbk_material), ctypes.POINTER(sbk_rule), _I, _I32, _I32]
                              + [_P] * 7 + [_I64] + [_P] * 7),
+    "sbk_partition_create": (_I, [_I64, _P, _P, _I64, _I32, _P, ctypes.POINTER(_P)]),
+    "sbk_partition_destroy": (_I, [_P]),
+    "sbk_partition_set_stream": (_I, [_P, _P]),
+    "sbk_partition_info": (_I, [_P, ctypes.POINTER(_I32), ctypes.POINTER(_I64)]),
+    "sbk_partition_pattern": (_I, [_P, _P, _P]),
+    "sbk_partition_assemble": (_I, [_P, _P, _P]),
+    "sbk_partition_restrict": (_I, [_P, _P, _P]),
+    "sbk_partition_add_to": (_I, [_P, _P, _P, _D]),
+    "sbk_partition_factorize": (_I, [_P, _P, _I, ctypes.POINTER(_I)]),
+    "sbk_partition_solve": (_I, [_P, _P, _P]),
+    "sbk_partition_counts": (_I, [_P, ctypes.POINTER(_I64 * 9)]),
+    "sbk_partition_set_dense_limit": (_I, [_P, _I32]),
     "sbk_last_error": (ctypes.c_char_p, []),
 }
 
@@ -147,6 +159,10 @@ def lib() -> ctypes.CDLL:
         if not os.path.exists(LIB_PATH):
             raise ImportError(f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
                               "(the element loop has no CPU fallback)")
+        # torch first: the library's cuSOLVER and cuSPARSE then resolve to
+        # the copies torch has loaded, one set of CUDA math libraries per
+        # process.
+        import torch  # noqa: F401
         L = ctypes.CDLL(LIB_PATH)
         for name, (res, args) in SIGNATURES.items():
             f = getattr(L, name)

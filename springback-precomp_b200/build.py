@@ -2,7 +2,8 @@
 
 nvcc cross-compiles for sm_100a (B200) without a GPU. The library exports
 the C ABI of include/sbk.h and nothing else; it links the CUDA runtime
-statically, so it loads on any box with the driver.
+statically, so it loads on any box with the driver, and cuSOLVER and
+cuSPARSE (the free-free block's factorisation) dynamically, by soname.
 """
 from __future__ import annotations
 
@@ -15,7 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsbk.so")
-SOURCES = ["sbk_element.cu", "sbk_assembly.cu", "sbk_contact.cu", "sbk_capi.cu", "sbk_schedule.cu", "sbk_noalloc.cu"]
+SOURCES = ["sbk_element.cu", "sbk_assembly.cu", "sbk_contact.cu", "sbk_capi.cu", "sbk_schedule.cu", "sbk_noalloc.cu",
+           "sbk_partition.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -65,7 +67,9 @@ def build(force: bool = False, verbose_ptxas: bool = False) -> str:
         if p.returncode != 0:
             raise RuntimeError("nvcc failed: " + " ".join(cmd))
     tmp = LIB + ".tmp"
-    subprocess.run([nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-cudart", "static"], check=True)
+    cuda_lib = os.path.join(os.path.dirname(os.path.dirname(nvcc())), "lib64")
+    subprocess.run([nvcc()] + ARCH + ["-shared", "-o", tmp] + objs + ["-cudart", "static", "-L" + cuda_lib,
+                                                                      "-lcusolver", "-lcusparse"], check=True)
     os.replace(tmp, LIB)
     return LIB
 

@@ -2,9 +2,9 @@
 of the product. It stands in for the reference's FormingAnalysis::run
 (src/fem/Forming.cpp:686-1262), which calls the element loop and the contact
 every Newton iteration: it runs a committed forming deck of the reference
-through this package's NonlinearSystem and ToolContact on the GPU, solving
-the linear systems with scipy on the host, or densely on the GPU for a
-larger sheet (the reference's own sparse solver is outside the graft).
+through this package's NonlinearSystem, ToolContact and PartitionedFactor on
+the GPU - the free-free block gathered and factorised on the device (or,
+with solver="host", scipy's sparse LU on the host).
 
 What it restates of the driver, because the converged states depend on it:
 the step partition (prescribed DOFs held at their values, Forming.cpp:804-821),
@@ -89,8 +89,11 @@ class StepResult:
 
 
 class FormingRun:
-    def __init__(self, pkg, fixture: dict, device):
+    def __init__(self, pkg, fixture: dict, device, solver: str = "device"):
         self.pkg = pkg
+        self.solver = solver
+        self.part = None
+        self.contact_symmetric = True
         self.fx = fixture
         self.dev = device
         self.nodes = np.array(fixture["nodes"], dtype=np.float64)
@@ -143,26 +146,33 @@ class FormingRun:
         ev = self.system.evaluate(torch.tensor(u, device=self.dev), 0.0, tangent)
         r = ev.residual.double().cpu().numpy().copy()
         fz = 0.0
+        if tangent:
+            self.contact_symmetric = True
         if self.contact is not None and any(active):
             cev = self.contact.evaluate(torch.tensor(u, device=self.dev), t, tangent)
             r += cev.residual.cpu().numpy()
             fz = float(sum(cev.tools[k][5] for k in range(len(active)) if active[k]))
+            if tangent:
+                self.contact_symmetric = cev.symmetric
             if tangent and len(cev.nodes):
                 self.system.add_node_blocks(cev.nodes, cev.blocks)
         return ev, r, fz
 
     def _solve(self, ev, free, rhs):
-        """K_ff x = rhs: scipy's sparse LU on the host, or for a larger sheet
-        a dense LU on the GPU (torch)."""
-        n = self.mesh.num_dofs
-        if len(free) <= 3000:
+        """K_ff x = rhs as Forming.cpp:1000-1016 and :1043-1050 solve it:
+        the free-free block of the current tangent (node blocks included)
+        assembled and factorised - on the device by the package's
+        PartitionedFactor, symmetric when the system and the contact are -
+        or with scipy's sparse LU on the host."""
+        if self.solver == "host":
+            n = self.mesh.num_dofs
             k = scipy.sparse.csc_matrix((ev.tangent.cpu().numpy(), self.system.inner.cpu().numpy(),
                                          self.system.outer.cpu().numpy()), shape=(n, n))
             return scipy.sparse.linalg.spsolve(k[free][:, free].tocsc(), rhs)
-        k = torch.sparse_csc_tensor(self.system.outer.long(), self.system.inner.long(), ev.tangent, (n, n))
-        f = torch.as_tensor(free, device=self.dev)
-        kff = k.to_dense()[f][:, f]
-        return torch.linalg.solve(kff, torch.as_tensor(rhs, device=self.dev)).cpu().numpy()
+        if self.part is None or not self.part.same_partition(free):
+            self.part = self.pkg.PartitionedFactor.for_system(self.system, free)
+        self.part.factorize(ev.tangent, self.system.symmetric() and self.contact_symmetric)
+        return self.part.solve(torch.as_tensor(np.ascontiguousarray(rhs), device=self.dev)).cpu().numpy()
 
     def _speed(self, t, active):
         v = 0.0
