@@ -16,6 +16,10 @@ and f_int plus the tangent values copied back, every step. Under torchrun
 every rank evaluates its own part (independent meshes, no collective on the
 data path; weak scaling); the time is the max over ranks.
 
+--workload partition measures the free-free block of a Dirichlet partition
+(PartitionedFactor): its gather from the full tangent, and the device
+factorisation and solve it feeds.
+
 --impl reference times the reference's CPU algorithm - the oracle's
 restatement of it (the reference needs Eigen, which this image lacks) - on
 all host cores, on a bounded sample of the same workload per step.
@@ -44,6 +48,10 @@ METRIC = "Hex8 tangent+residual+assembly elem/s (FP64)"
 # grows with the elements, so a launch of ne elements moves about ne times
 # this.
 K1_DRAM_BYTES_PER_ELEMENT = 16.11e9 / 80000
+# DRAM bytes per block entry of one free-free gather (assemble), from the ncu
+# capture of the 200 x 200 x 2 sheet's block (profiles/free_free_partition.md:
+# 271.0 MB read + 139.0 MB written for 22,528,485 entries).
+GATHER_DRAM_BYTES_PER_ENTRY = (271.010304e6 + 139.048192e6) / 22528485
 UNIT = "elem/s"
 
 
@@ -290,6 +298,142 @@ def run_batched(args, rank, world):
     return 0
 
 
+def sheet_partition(pkg, torch, nx, ny, dev):
+    """A nx x ny x 2 sheet of 1 mm x 1 mm x 0.5 mm cells (aluminium, Swift
+    law, 2 x 2 x 2 points) under a small bending field, held on its two x
+    edges: the system, the tangent values and the free DOFs."""
+    mat = pkg.material.aluminium_swift()
+    m = pkg.structured_hex_mesh(nx, ny, 2, nx * 1e-3, ny * 1e-3, 1e-3)
+    x = m.coords
+    sysm = pkg.NonlinearSystem(m, mat)
+    u = np.zeros_like(x)
+    u[:, 2] = -1e-4 * (x[:, 0] / x[:, 0].max()) ** 2
+    ev = sysm.evaluate(torch.tensor(u.reshape(-1), device=dev), 0.0, True)
+    edge = np.flatnonzero((x[:, 0] == x[:, 0].min()) | (x[:, 0] == x[:, 0].max()))
+    held = np.zeros(m.num_dofs, dtype=bool)
+    for c in range(3):
+        held[3 * edge + c] = True
+    return sysm, ev.tangent.clone(), np.flatnonzero(~held).astype(np.int32)
+
+
+def run_partition(args, rank, world):
+    """The free-free block of a Dirichlet partition (PartitionedFactor,
+    Forming.cpp:59-241): one step = the gather of the block's values from
+    the full tangent (assemble), the kernel the roofline covers; beside it
+    the factorisation (sparse Cholesky) and solve the block feeds, and the
+    CPU: the oracle's restatement of the gather and scipy's SuperLU (the
+    reference's CHOLMOD / UMFPACK are not in this image) on a bounded
+    sample."""
+    import torch
+
+    if world > 1 and rank != 0:
+        return 0
+    pkg = importlib.import_module(PKG)
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    peaks = measured_peaks()
+    nx, ny = args.part_nx, args.part_ny
+    sysm, values, free = sheet_partition(pkg, torch, nx, ny, dev)
+    t0 = time.perf_counter()
+    part = pkg.PartitionedFactor.for_system(sysm, free)
+    torch.cuda.synchronize()
+    create_ms = (time.perf_counter() - t0) * 1e3
+    kff = torch.empty(part.nnz, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        part.assemble(values, kff)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(0) as clocks:
+        e0.record(stream)
+        for _ in range(args.steps):
+            part.assemble(values, kff)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    entries = part.nnz
+    alg_bytes = entries * (8 + 4 + 8)  # value read, source index read, block value written
+    achieved = alg_bytes / (ms / 1e3) / 1e9
+    # Through the public call with host buffers: the full tangent copied in
+    # from pinned memory, the block's values copied back, every step.
+    host_vals = values.cpu().pin_memory()
+    host_kff = torch.empty(entries, dtype=torch.float64).pin_memory()
+    dev_vals = torch.empty_like(values)
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        dev_vals.copy_(host_vals, non_blocking=True)
+        part.assemble(dev_vals, kff)
+        host_kff.copy_(kff, non_blocking=True)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e2.elapsed_time(e3) / args.steps
+    # The factorisation the block feeds.
+    part.factorize(values, True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        part.factorize(values, True)
+    torch.cuda.synchronize()
+    factor_ms = (time.perf_counter() - t0) / 3 * 1e3
+    b = torch.ones(part.num_free, dtype=torch.float64, device=dev)
+    part.solve(b)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        part.solve(b)
+    torch.cuda.synchronize()
+    solve_ms = (time.perf_counter() - t0) / 3 * 1e3
+    line = {"metric": "free-free block entries gathered/s (FP64)", "value": entries / (ms / 1e3),
+            "unit": "entries/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"free-free block of a {nx}x{ny}x2 IM Hex8 sheet held on its x edges "
+                                   f"({part.num_free} free DOFs, {entries} block entries of "
+                                   f"{sysm.nnz}); one step = PartitionedFactor.assemble",
+                       "l2": "inputs larger than L2 (full values, source map and block values "
+                             f"{alg_bytes / 1e6:.0f} MB per step)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                         "frac": achieved / peaks.get("hbm_gbs", 6650.0),
+                         "traffic": GATHER_DRAM_BYTES_PER_ENTRY * entries,
+                         "peak_source": peaks.get("source", "MEASURED_PEAKS.json")},
+            "e2e": {"value": entries / (e2e_ms / 1e3), "unit": "entries/s", "h2d_bytes_per_step": values.numel() * 8,
+                    "d2h_bytes_per_step": entries * 8},
+            "gpu_launches": args.steps, "clocks": clocks.summary(),
+            "create_ms": create_ms, "cholesky_factor_ms": factor_ms, "cholesky_solve_ms": solve_ms,
+            "counts": part.counts()}
+    if not args.no_cpu_baseline:
+        orc = oracle_module()
+        snx, sny = args.sample_nx, args.sample_ny
+        ssys, svals, sfree = sheet_partition(pkg, torch, snx, sny, dev)
+        pat = {"outer": ssys.outer.cpu().numpy(), "inner": ssys.inner.cpu().numpy()}
+        v = svals.cpu().numpy()
+        t0 = time.perf_counter()
+        _, _, src, sk = orc.free_free_block(pat, v, sfree)
+        cpu_s = time.perf_counter() - t0
+        import scipy.sparse as sp
+        import scipy.sparse.linalg as spl
+        n = ssys.num_dofs
+        K = sp.csc_matrix((v, pat["inner"], pat["outer"]), shape=(n, n))[sfree][:, sfree].tocsc()
+        t0 = time.perf_counter()
+        spl.splu(K).solve(np.ones(len(sfree)))
+        lu_s = time.perf_counter() - t0
+        spart = pkg.PartitionedFactor.for_system(ssys, sfree)
+        spart.factorize(svals, True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        spart.factorize(svals, True)
+        spart.solve(torch.ones(len(sfree), dtype=torch.float64, device=dev))
+        torch.cuda.synchronize()
+        gpu_fs = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": len(sk) / cpu_s, "unit": "entries/s", "cores": 1, "kind": "port",
+                                "sample": f"the oracle's gather of the {snx}x{sny}x2 sheet's block ({len(sk)} "
+                                          f"entries)",
+                                "superlu_factor_solve_ms": lu_s * 1e3, "gpu_cholesky_factor_solve_ms": gpu_fs * 1e3,
+                                "superlu_sample": f"{snx}x{sny}x2 sheet, {len(sfree)} free DOFs"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def config(args, world):
     return {"workload": f"element-kernel microbenchmark: {args.nx}x{args.ny}x{args.nz} IM Hex8 sheet "
                         f"(0.04x0.04x0.5 mm cells), 2x2x2 points, Hill48 r=(0.73,0.80,0.70) + Chaboche "
@@ -314,9 +458,12 @@ def main():
     p.add_argument("--epb", type=int, default=0, help="elements per block of the element kernel (0: default)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="microbench", choices=["microbench", "batched"],
+    p.add_argument("--workload", default="microbench", choices=["microbench", "batched", "partition"],
                    help="batched: the design-sweep batch (64 parts of 20k-150k elements) in one launch against the "
-                        "same parts evaluated one at a time")
+                        "same parts evaluated one at a time; partition: the free-free block of a Dirichlet "
+                        "partition gathered from the full tangent, and the factorisation it feeds")
+    p.add_argument("--part-nx", type=int, default=200)
+    p.add_argument("--part-ny", type=int, default=200)
     p.add_argument("--parts", type=int, default=64)
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -327,6 +474,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "batched":
         return run_batched(args, rank, world)
+    if args.workload == "partition":
+        return run_partition(args, rank, world)
 
     import torch
 
