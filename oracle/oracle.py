@@ -43,6 +43,7 @@ _ll = ctypes.c_longlong
 
 
 def _declare(L):
+    L.orc_set_element.argtypes = [ctypes.c_int, ctypes.c_int]
     L.orc_rule_size.argtypes = [ctypes.c_int] * 3
     L.orc_rule.argtypes = [ctypes.c_int] * 3 + [_d]
     L.orc_yield_matrix.argtypes = [_d, _d]
@@ -69,6 +70,22 @@ def _declare(L):
     L.orc_contact_anticipate.argtypes = [ctypes.c_void_p, _d, _d, ctypes.c_double, _d, ctypes.c_int, _i, _d]
     L.orc_contact_commit.argtypes = [ctypes.c_void_p]
     L.orc_contact_history.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _d]
+
+
+class element:
+    """Context: the calls inside evaluate the standard Hex8
+    (Elastoplastic.cpp:226-340; `averaged`: with mean dilatation) instead of
+    the incompatible-mode Hex8."""
+
+    def __init__(self, standard: bool, averaged: bool = False):
+        self.standard, self.averaged = bool(standard), bool(averaged)
+
+    def __enter__(self):
+        lib().orc_set_element(int(self.standard), int(self.averaged))
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_element(0, 0)
 
 
 def _p(a, kind=_d):

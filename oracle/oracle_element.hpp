@@ -724,4 +724,246 @@ class IMElement {
   std::vector<PointWork<T>> points_;
 };
 
+/// elastoplastic_element for the standard Hex8 (src/fem/Elastoplastic.cpp:226-340)
+/// with its kinematics (kinematics_of, :104-168): B, B_NL or P B_NL per point,
+/// the mean dilatation (B-bar) when `averaged` (the NonlinearSystem's choice,
+/// NonlinearSystem.hpp:302-309), the returns, f = sum w b^T sigma and the
+/// tangent; logarithmic kinematics assembles its tangent after every return,
+/// with the element's mean Kirchhoff pressure and the cross terms of the
+/// averaged ln J. Throws Failure.
+template <class T>
+class StdElement {
+ public:
+  StdElement(const Material& mat, const std::vector<QPoint>& rule, int kinematics, bool averaged)
+      : mat_(mat), rule_(rule), kin_(kinematics), averaged_(averaged && rule.size() > 1) {}
+
+  ElementOut<T> evaluate(const double* x, const T* ue, const std::vector<State<T>>& committed,
+                         bool want_tangent) {
+    kinematics_of(x, ue);
+    const bool finite = kin_ == kFinite, logarithmic = kin_ == kLogarithmic;
+    ElementOut<T> out;
+    for (std::size_t q = 0; q < pts_.size(); ++q) {
+      Pt& p = pts_[q];
+      const Response<T> r = plastic_return(mat_, p.strain, committed[q], want_tangent);
+      const T w = p.weight;
+      for (int j = 0; j < 24; ++j) {
+        T s = T(0.0);
+        for (int c = 0; c < 6; ++c) s += p.b(c, j) * r.stress[c];
+        out.force[j] += w * s;
+      }
+      out.energy += w * r.energy;
+      if (logarithmic && want_tangent) {
+        p.stress = r.stress;
+        p.tangent = r.tangent;
+      }
+      if (want_tangent && !logarithmic) {
+        const Mat<T, 6, 24> cb = mul(r.tangent, p.b);
+        for (int i = 0; i < 24; ++i)
+          for (int j = 0; j < 24; ++j) {
+            T s = T(0.0);
+            for (int c = 0; c < 6; ++c) s += p.b(c, i) * cb(c, j);
+            out.tangent(i, j) += w * s;
+          }
+        if (finite) {
+          // S : Delta delta E, with the averaged dilatation
+          // (tr S / 3) (Delta delta tr-bar E - Delta delta tr E).
+          const Mat<T, 3, 3> st = tensor3(r.stress);
+          Mat<T, 8, 8> geo = mul(mul(tr(p.g), st), p.g);
+          if (averaged_) {
+            const T third = (r.stress[0] + r.stress[1] + r.stress[2]) / T(3.0);
+            const Mat<T, 8, 8> gg = mul(tr(p.g), p.g);
+            for (int i = 0; i < 64; ++i) geo[i] += third * (gbar_[i] - gg[i]);
+          }
+          for (int a = 0; a < 8; ++a)
+            for (int b = 0; b < 8; ++b)
+              for (int k = 0; k < 3; ++k) out.tangent(3 * a + k, 3 * b + k) += w * geo(a, b);
+        }
+      }
+      if (r.yielding) ++out.yielding;
+      out.point_yield.push_back(r.yielding ? 1 : 0);
+      out.states.push_back(r.state);
+    }
+    if (logarithmic && want_tangent) {
+      T mean_pressure = T(0.0);
+      if (averaged_) {
+        T volume = T(0.0);
+        for (const Pt& p : pts_) {
+          mean_pressure += p.weight * (p.stress[0] + p.stress[1] + p.stress[2]) / T(3.0);
+          volume += p.weight;
+        }
+        mean_pressure /= volume;
+      }
+      Vec<T, 6> m;
+      m[0] = m[1] = m[2] = T(1.0);
+      for (const Pt& p : pts_) {
+        const T w = p.weight;
+        const Mat<T, 6, 6>& proj = p.log.projection;
+        Vec<T, 6> t = p.stress;
+        if (averaged_) {
+          const T shift = mean_pressure - (t[0] + t[1] + t[2]) / T(3.0);
+          for (int i = 0; i < 3; ++i) t[i] += shift;
+        }
+        const Mat<T, 6, 6> pcp = mul(mul(tr(proj), p.tangent), proj);
+        const Mat<T, 6, 6> curv = logarithmic_curvature(p.log, t);
+        Mat<T, 6, 6> inner;
+        for (int i = 0; i < 36; ++i) inner[i] = pcp[i] + curv[i];
+        const Mat<T, 6, 24> ib = mul(inner, p.bnl);
+        for (int i = 0; i < 24; ++i)
+          for (int j = 0; j < 24; ++j) {
+            T s = T(0.0);
+            for (int c = 0; c < 6; ++c) s += p.bnl(c, i) * ib(c, j);
+            out.tangent(i, j) += w * s;
+          }
+        if (averaged_) {
+          // (A + m s^T/3)^T C (A + m s^T/3) - A^T C A with A = P B_NL.
+          const Vec<T, 6> cm = mul(p.tangent, m);
+          const Vec<T, 6> mc = mul(tr(p.tangent), m);
+          const Vec<T, 24> a_cm = mul(tr(p.bnl), mul(tr(proj), cm));
+          const Vec<T, 24> a_mc = mul(tr(p.bnl), mul(tr(proj), mc));
+          const T mcm = dot(m, cm) / T(3.0);
+          for (int i = 0; i < 24; ++i) {
+            const T left = a_cm[i] + mcm * p.shift[i];
+            for (int j = 0; j < 24; ++j) out.tangent(i, j) += (w / T(3.0)) * (left * p.shift[j]);
+          }
+          for (int i = 0; i < 24; ++i)
+            for (int j = 0; j < 24; ++j) out.tangent(i, j) += (w / T(3.0)) * (p.shift[i] * a_mc[j]);
+        }
+        // add_geometric (:60-76) with S' = P^T T'.
+        const Mat<T, 3, 3> sd = tensor3(logarithmic_stress(p.log, t));
+        const Mat<T, 8, 8> geo = mul(mul(tr(p.g), sd), p.g);
+        for (int a = 0; a < 8; ++a)
+          for (int b = 0; b < 8; ++b)
+            for (int k = 0; k < 3; ++k) out.tangent(3 * a + k, 3 * b + k) += w * geo(a, b);
+      }
+    }
+    out.symmetric = mat_.symmetric();
+    if (want_tangent && out.symmetric) {
+      for (int i = 0; i < 24; ++i)
+        for (int j = i + 1; j < 24; ++j) {
+          const T v = T(0.5) * (out.tangent(i, j) + out.tangent(j, i));
+          out.tangent(i, j) = v;
+          out.tangent(j, i) = v;
+        }
+    }
+    return out;
+  }
+
+ private:
+  struct Pt {
+    Mat<T, 6, 24> b, bnl;
+    Vec<T, 6> strain, stress;
+    Mat<T, 3, 8> g;
+    Mat<T, 3, 3> h;
+    T weight = T(0.0);
+    LogStrain<T> log;
+    Vec<T, 24> shift;
+    Mat<T, 6, 6> tangent;
+  };
+
+  static Vec<T, 24> dilatation_row(const Mat<T, 6, 24>& b) {
+    Vec<T, 24> r;
+    for (int j = 0; j < 24; ++j) r[j] = b(0, j) + b(1, j) + b(2, j);
+    return r;
+  }
+
+  static Mat<T, 6, 24> gl_operator(const Mat<T, 3, 3>& f, const Mat<T, 3, 8>& g) {
+    static constexpr int kPair[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {1, 2}, {2, 0}};
+    Mat<T, 6, 24> b;
+    for (int c = 0; c < 6; ++c) {
+      const int i = kPair[c][0], j = kPair[c][1];
+      for (int a = 0; a < 8; ++a)
+        for (int k = 0; k < 3; ++k)
+          b(c, 3 * a + k) = i == j ? f(k, i) * g(i, a) : f(k, i) * g(j, a) + f(k, j) * g(i, a);
+    }
+    return b;
+  }
+
+  // kinematics_of (Elastoplastic.cpp:104-168).
+  void kinematics_of(const double* x, const T* ue) {
+    Mat<T, 3, 8> u;
+    for (int a = 0; a < 8; ++a)
+      for (int k = 0; k < 3; ++k) u(k, a) = ue[3 * a + k];
+    pts_.assign(rule_.size(), Pt());
+    for (std::size_t q = 0; q < rule_.size(); ++q) {
+      const QPoint& xi = rule_[q];
+      Pt& p = pts_[q];
+      const Mat<double, 8, 3> dn = shape_gradients(xi.xi, xi.eta, xi.zeta);
+      Mat<T, 3, 3> jac;
+      for (int i = 0; i < 3; ++i)
+        for (int c = 0; c < 3; ++c) {
+          T s = T(0.0);
+          for (int a = 0; a < 8; ++a) s += T(x[3 * a + i]) * T(dn(a, c));
+          jac(i, c) = s;
+        }
+      const T det = det3(jac);
+      if (!(det > T(0.0))) throw Failure{kMeshInverted};
+      const Mat<T, 3, 3> jinv = inv3(jac);
+      for (int a = 0; a < 8; ++a)
+        for (int i = 0; i < 3; ++i) {
+          T s = T(0.0);
+          for (int c = 0; c < 3; ++c) s += T(dn(a, c)) * jinv(c, i);
+          p.g(i, a) = s;
+        }
+      p.h = mul(u, tr(p.g));
+      Mat<T, 3, 3> f = p.h;
+      for (int i = 0; i < 3; ++i) f(i, i) += T(1.0);
+      if (kin_ == kFinite) {
+        p.b = gl_operator(f, p.g);
+        p.strain = green_lagrange_6(p.h);
+      } else if (kin_ == kLogarithmic) {
+        if (!(det3(f) > T(0.0))) throw Failure{kInverted};
+        p.bnl = gl_operator(f, p.g);
+        p.log = logarithmic_strain(green_lagrange_6(p.h));
+        p.strain = p.log.strain;
+        p.b = mul(p.log.projection, p.bnl);
+      } else {
+        Mat<T, 3, 3> id;
+        for (int i = 0; i < 3; ++i) id(i, i) = T(1.0);
+        p.b = gl_operator(id, p.g);
+        for (int c = 0; c < 6; ++c) {
+          T s = T(0.0);
+          for (int j = 0; j < 24; ++j) s += p.b(c, j) * ue[j];
+          p.strain[c] = s;
+        }
+      }
+      p.weight = T(xi.weight) * det;
+    }
+    if (!averaged_) return;
+    Vec<T, 24> mean_row;
+    T mean_trace = T(0.0), volume = T(0.0);
+    gbar_ = Mat<T, 8, 8>();
+    for (const Pt& p : pts_) {
+      const Vec<T, 24> d = dilatation_row(p.b);
+      for (int j = 0; j < 24; ++j) mean_row[j] += p.weight * d[j];
+      mean_trace += p.weight * (p.strain[0] + p.strain[1] + p.strain[2]);
+      volume += p.weight;
+      if (kin_ == kFinite) {
+        const Mat<T, 8, 8> gg = mul(tr(p.g), p.g);
+        for (int i = 0; i < 64; ++i) gbar_[i] += p.weight * gg[i];
+      }
+    }
+    for (int j = 0; j < 24; ++j) mean_row[j] /= volume;
+    mean_trace /= volume;
+    if (kin_ == kFinite)
+      for (int i = 0; i < 64; ++i) gbar_[i] /= volume;
+    for (Pt& p : pts_) {
+      const Vec<T, 24> d = dilatation_row(p.b);
+      if (kin_ == kLogarithmic)
+        for (int j = 0; j < 24; ++j) p.shift[j] = mean_row[j] - d[j];
+      const T shift = (mean_trace - (p.strain[0] + p.strain[1] + p.strain[2])) / T(3.0);
+      for (int r = 0; r < 3; ++r) {
+        for (int j = 0; j < 24; ++j) p.b(r, j) += (mean_row[j] - d[j]) / T(3.0);
+        p.strain[r] += shift;
+      }
+    }
+  }
+
+  const Material& mat_;
+  const std::vector<QPoint>& rule_;
+  int kin_;
+  bool averaged_;
+  std::vector<Pt> pts_;
+  Mat<T, 8, 8> gbar_;
+};
+
 }  // namespace orc

@@ -104,17 +104,25 @@ struct ElementBatch {
   signed char* yield_flags;  // nq per element, or null
 };
 
+// The element formulation of orc_elements / orc_system_evaluate: 0 the
+// incompatible-mode Hex8, 1 the standard Hex8 (with g_averaged: mean
+// dilatation), set by orc_set_element.
+int g_standard = 0;
+int g_averaged = 0;
+
 template <class T>
 void run_element(const ElementBatch& b, long long e) {
   const int nq = static_cast<int>(b.rule->size());
   IMElement<T> el(*b.mat, *b.rule, b.kin);
+  StdElement<T> std_el(*b.mat, *b.rule, b.kin, g_averaged != 0);
   std::vector<State<T>> committed(static_cast<std::size_t>(nq));
   for (int q = 0; q < nq; ++q) committed[q] = load_state<T>(b.committed + (e * nq + q) * kNF);
   T ue[24], an[9];
   for (int i = 0; i < 24; ++i) ue[i] = T(b.ue[e * 24 + i]);
   for (int i = 0; i < 9; ++i) an[i] = T(b.alpha_n ? b.alpha_n[e * 9 + i] : 0.0);
   try {
-    ElementOut<T> out = el.evaluate(b.X + e * 24, ue, committed, an, b.want_tangent != 0);
+    ElementOut<T> out = g_standard ? std_el.evaluate(b.X + e * 24, ue, committed, b.want_tangent != 0)
+                                   : el.evaluate(b.X + e * 24, ue, committed, an, b.want_tangent != 0);
     for (int i = 0; i < 24; ++i) b.f[e * 24 + i] = val(out.force[i]);
     if (b.want_tangent && b.K)
       for (int i = 0; i < 576; ++i) b.K[e * 576 + i] = val(out.tangent[i]);
@@ -209,6 +217,15 @@ void build_pattern(int nn, int ne, const int* conn, Pattern& p) {
 }  // namespace
 
 extern "C" {
+
+/// The element formulation of the calls that follow: standard 0 the
+/// incompatible-mode Hex8 (IncompatibleModes.cpp), 1 the standard Hex8
+/// (Elastoplastic.cpp:226-340), averaged 1 its mean dilatation.
+int orc_set_element(int standard, int averaged) {
+  g_standard = standard;
+  g_averaged = averaged;
+  return 0;
+}
 
 int orc_rule_size(int in_plane, int thickness, int axis) {
   return static_cast<int>(hex8_rule(in_plane, thickness, axis).size());
