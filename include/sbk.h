@@ -141,6 +141,23 @@ int sbk_system_destroy(sbk_system* sys);
 /* All later launches go to this stream (a cudaStream_t; NULL: default). */
 int sbk_system_set_stream(sbk_system* sys, void* stream);
 
+/* The element formulation (the model's "element_formulation" and the forming
+ * block's "mean_dilatation"; default: the incompatible-mode Hex8):
+ * SBK_ELEMENT_STANDARD is elastoplastic_element for the standard Hex8
+ * (src/fem/Elastoplastic.cpp:226-340) with B, B_NL or P B_NL per point,
+ * averaged (mean dilatation, B-bar) under "auto" or "all" when the rule has
+ * more than one point, as NonlinearSystem's constructor decides
+ * (NonlinearSystem.hpp:283-309); the incompatible-mode Hex8 refuses "all"
+ * (SBK_ERR_CONFIG). Stress recovery stays the incompatible-mode Hex8's. */
+#define SBK_ELEMENT_INCOMPATIBLE_MODES 0
+#define SBK_ELEMENT_STANDARD 1
+#define SBK_MEAN_DILATATION_AUTO 0
+#define SBK_MEAN_DILATATION_ALL 1
+#define SBK_MEAN_DILATATION_NONE 2
+int sbk_system_set_element(sbk_system* sys, int element, int mean_dilatation);
+/* The formulation in use and whether it averages the dilatation. */
+int sbk_system_element(const sbk_system* sys, int* element, int* averaged);
+
 /* Launch shape of the element kernel: elements per thread block (0: the
  * default, 16 for rules of up to 8 points - four warps - and 8 for larger
  * rules - eight warps; at most what 227 KB of shared memory and 256 threads

@@ -705,6 +705,34 @@ int sbk_system_set_schedule(sbk_system* sys, int by_cost) {
   return SBK_OK;
 }
 
+int sbk_system_set_element(sbk_system* sys, int element, int mean_dilatation) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  if (element != SBK_ELEMENT_INCOMPATIBLE_MODES && element != SBK_ELEMENT_STANDARD)
+    return fail(SBK_ERR_ARGUMENT, "unknown element formulation");
+  if (mean_dilatation < SBK_MEAN_DILATATION_AUTO || mean_dilatation > SBK_MEAN_DILATATION_NONE)
+    return fail(SBK_ERR_ARGUMENT, "unknown mean_dilatation");
+  // NonlinearSystem's constructor (NonlinearSystem.hpp:283-309): the
+  // incompatible-mode Hex8 refuses "all"; the standard Hex8 averages with
+  // "all" or "auto" when its rule has more than one point.
+  if (element == SBK_ELEMENT_INCOMPATIBLE_MODES && mean_dilatation == SBK_MEAN_DILATATION_ALL)
+    return fail(SBK_ERR_CONFIG,
+                "\"mean_dilatation\": \"all\" is not combined with the incompatible-mode Hex8: averaging the "
+                "dilatation of its modes leaves a zero-energy mode; use \"auto\" or \"none\"");
+  sys->p.element = element == SBK_ELEMENT_STANDARD ? 1 : 0;
+  sys->p.averaged = (element == SBK_ELEMENT_STANDARD && mean_dilatation != SBK_MEAN_DILATATION_NONE && sys->p.nq > 1)
+                        ? 1
+                        : 0;
+  sys->order_valid = false;
+  return SBK_OK;
+}
+
+int sbk_system_element(const sbk_system* sys, int* element, int* averaged) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  if (element) *element = sys->p.element ? SBK_ELEMENT_STANDARD : SBK_ELEMENT_INCOMPATIBLE_MODES;
+  if (averaged) *averaged = sys->p.averaged;
+  return SBK_OK;
+}
+
 int sbk_system_set_elements_per_block(sbk_system* sys, int epb) {
   if (!sys || epb < 0 || epb > 32) return fail(SBK_ERR_ARGUMENT, "bad elements per block");
   sys->elements_per_block = epb;
@@ -914,6 +942,8 @@ int sbk_system_add_node_blocks(sbk_system* sys, int32_t n, const int32_t* nodes_
 
 int sbk_system_stress(sbk_system* sys, const double* u_dev, double* out_dev) {
   if (!sys || !u_dev || !out_dev) return fail(SBK_ERR_ARGUMENT, "null argument");
+  if (sys->p.element != 0)
+    return fail(SBK_ERR_UNSUPPORTED, "stress recovery is built for the incompatible-mode Hex8 only");
   cudaStream_t st = sys->stream;
   SBK_CUDA(cudaMemsetAsync(sys->first_fail, 0x7f, sizeof(int32_t), st));
   // The returns reproduce the committed states into the trial buffer, which

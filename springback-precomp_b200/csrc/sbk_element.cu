@@ -1168,6 +1168,403 @@ __global__ void __launch_bounds__(256) element_kernel(const __grid_constant__ Pa
   for (int i = lane; i < 9; i += G) alpha_out[e * 9 + i] = s.alpha[i];
 }
 
+// ---- the standard Hex8 -------------------------------------------------------
+//
+// elastoplastic_element for an element without internal modes
+// (Elastoplastic.cpp:226-340, kinematics_of :104-168): per point the
+// kinematics (B, B_NL or P B_NL), with mean dilatation (B-bar) the
+// element's averaged dilatation in the strain and its variation, the return,
+// then f = sum w b^T sigma and the tangent. Lane = point as in K1; the
+// per-point material blocks go through the same slots, so the
+// B_NL^T M B_NL + geometric part is K1's V-tensor form; the mean-dilatation
+// terms are rank-two updates (w/3)(left s^T + s a_mc^T) of 24-vectors that
+// are all B_NL^T v for a per-point 6-vector v, built node by node.
+
+constexpr int kStdPt = 26;  // per point: pv 6 | u1 6 | u2 6 | m.C m | S(T) 6 | tr T
+constexpr int kStdPv = 0, kStdU1 = 6, kStdU2 = 12, kStdMcm = 18, kStdST = 19, kStdTr = 25;
+
+template <int G>
+struct __align__(16) StdExtra {
+  double pt[G][kStdPt];
+  double mean_row[24];  // the volume average of the points' dilatation rows
+  double red[32];       // group sums: w d (24), w, w tr(strain)
+};
+
+// [B_NL^T v] at DOF 3a + k for the node gradient g (B_NL from F; F = I: B).
+__device__ __forceinline__ double bnl_t(const double F[9], const double g[3], int k, const double v[6]) {
+  double b[6];
+  bcol(F, g, k, b);
+  return b[0] * v[0] + b[1] * v[1] + b[2] * v[2] + b[3] * v[3] + b[4] * v[4] + b[5] * v[5];
+}
+
+// The points of a standard element: kinematics, mean dilatation, returns,
+// slots. Returns 0 or the failure code of the first failing point in the
+// reference's order.
+template <int G>
+__device__ __noinline__ int std_points(const Ctx<G>& c, StdExtra<G>* x) {
+  ElemShared<G>& s = *c.s;
+  const Params& p = *c.p;
+  const int q = c.lane;
+  const bool active = q < p.nq;
+  const int kin = p.kinematics;
+  const bool averaged = p.averaged != 0;
+  int fail = 0, code = 0;
+  double F[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, strain[6] = {0, 0, 0, 0, 0, 0}, w = 0.0;
+  LogKin L;
+  if (active) {
+    w = s.geo[q][9];
+    const double* h = c.hu;
+    if (kin == SBK_SMALL_STRAIN) {
+      strain[0] = h[0];
+      strain[1] = h[4];
+      strain[2] = h[8];
+      strain[3] = h[1] + h[3];
+      strain[4] = h[5] + h[7];
+      strain[5] = h[6] + h[2];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 9; ++i) F[i] = h[i] + ((i % 4) == 0 ? 1.0 : 0.0);
+      double E[9];
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          E[i * 3 + j] = 0.5 * (h[i * 3 + j] + h[j * 3 + i] + h[0 * 3 + i] * h[0 * 3 + j] +
+                                h[1 * 3 + i] * h[1 * 3 + j] + h[2 * 3 + i] * h[2 * 3 + j]);
+      const double green[6] = {E[0], E[4], E[8], 2.0 * E[1], 2.0 * E[5], 2.0 * E[6]};
+      if (kin == SBK_FINITE) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) strain[i] = green[i];
+      } else {
+        code = det3(F) > 0.0 ? log_strain(green, L, strain) : SBK_EL_INVERTED_POINT;
+        if (code) fail = (1 << 8) | q;
+      }
+    }
+  }
+  int key = fail ? fail : 0x7fffffff;
+#pragma unroll
+  for (int o = G / 2; o >= 1; o >>= 1) key = min(key, __shfl_xor_sync(c.mask, key, o, G));
+  if (key != 0x7fffffff) {
+    const int out = __shfl_sync(c.mask, code, key & 0xff, G);
+    c.sync();
+    return out;
+  }
+  const double m6[6] = {1.0, 1.0, 1.0, 0.0, 0.0, 0.0};
+  double pv[6] = {1.0, 1.0, 1.0, 0.0, 0.0, 0.0};  // P^T m: the variation of the trace
+  if (averaged) {
+    if (active && kin == SBK_FINITE_LOGARITHMIC) log_stress(L, m6, pv);
+    // Group sums of w d(3a + k) (d = B_NL^T pv, the point's dilatation row),
+    // of w and of w tr(strain), in chunks of G through the reduce-scatter.
+    const double tr = strain[0] + strain[1] + strain[2];
+#pragma unroll 1
+    for (int chunk = 0; chunk * G < 26; ++chunk) {
+      double buf[G];
+#pragma unroll
+      for (int i = 0; i < G; ++i) {
+        const int idx = chunk * G + i;
+        double v = 0.0;
+        if (active && idx < 26) {
+          if (idx < 24) {
+            double g[3];
+            node_grad(c, q, idx / 3, g);
+            v = w * bnl_t(F, g, idx % 3, pv);
+          } else {
+            v = idx == 24 ? w : w * tr;
+          }
+        }
+        buf[i] = v;
+      }
+      const double y = reduce_scatter<G>(buf, c.lane, c.mask);
+      if (chunk * G + c.lane < 32) x->red[chunk * G + c.lane] = y;
+    }
+    c.sync();
+    const double volume = x->red[24];
+    if (c.lane < 24) x->mean_row[c.lane] = x->red[c.lane] / volume;
+    if (G < 24)
+      for (int j = c.lane + G; j < 24; j += G) x->mean_row[j] = x->red[j] / volume;
+    const double mean_trace = x->red[25] / volume;
+    if (active) {
+      const double shift = (mean_trace - tr) / 3.0;
+      strain[0] += shift;
+      strain[1] += shift;
+      strain[2] += shift;
+    }
+    c.sync();
+  }
+  Response r;
+  if (active) {
+    PointState st{c.state + c.e * p.nq + q, c.trial + c.e * p.nq + q, c.npts};
+    code = p.general ? general_return(p, strain, st, r, c.warm) : radial_return(p, strain, st, r);
+    if (code) fail = (2 << 8) | q;
+  }
+  key = fail ? fail : 0x7fffffff;
+#pragma unroll
+  for (int o = G / 2; o >= 1; o >>= 1) key = min(key, __shfl_xor_sync(c.mask, key, o, G));
+  if (key != 0x7fffffff) {
+    const int out = __shfl_sync(c.mask, code, key & 0xff, G);
+    c.sync();
+    return out;
+  }
+  const double trT = active ? r.stress[0] + r.stress[1] + r.stress[2] : 0.0;
+  // The element's mean Kirchhoff pressure (logarithmic + averaged): a
+  // butterfly sum, the same bits in every lane.
+  double mean_pressure = 0.0;
+  if (averaged && kin == SBK_FINITE_LOGARITHMIC) {
+    double v = active ? w * trT / 3.0 : 0.0;
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1) v += __shfl_xor_sync(c.mask, v, o, G);
+    mean_pressure = v / x->red[24];
+  }
+  if (active) {
+    c.yield[c.e * p.nq + q] = r.yielding ? 1 : 0;
+    double* e = x->pt[q];
+    double cm[6], mc[6];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      cm[i] = r.C[i * 6 + 0] + r.C[i * 6 + 1] + r.C[i * 6 + 2];
+      mc[i] = r.C[0 * 6 + i] + r.C[1 * 6 + i] + r.C[2 * 6 + i];
+    }
+    e[kStdMcm] = cm[0] + cm[1] + cm[2];
+    e[kStdTr] = trT;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) e[kStdPv + i] = pv[i];
+    double S[6], M[36];
+#pragma unroll
+    for (int i = 0; i < 36; ++i) M[i] = r.C[i];
+    if (kin == SBK_FINITE_LOGARITHMIC) {
+      double t[6], u[6];
+      log_stress(L, r.stress, u);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) e[kStdST + i] = u[i];
+      log_stress(L, cm, u);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) e[kStdU1 + i] = u[i];
+      log_stress(L, mc, u);
+#pragma unroll
+      for (int i = 0; i < 6; ++i) e[kStdU2 + i] = u[i];
+#pragma unroll
+      for (int i = 0; i < 6; ++i) t[i] = r.stress[i];
+      if (averaged) {
+        const double shift = mean_pressure - trT / 3.0;
+        t[0] += shift;
+        t[1] += shift;
+        t[2] += shift;
+      }
+      log_transform(L, t, S, M);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 6; ++i) {
+        S[i] = r.stress[i];
+        e[kStdST + i] = r.stress[i];
+        e[kStdU1 + i] = cm[i];
+        e[kStdU2 + i] = mc[i];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < 36; ++i) s.slot[q][i] = M[i];
+#pragma unroll
+    for (int i = 0; i < 6; ++i) s.slot[q][kSlotS + i] = S[i];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) s.slot[q][kSlotF + i] = F[i];
+    s.slot[q][kSlotW] = w;
+    s.slot[q][kSlotE] = r.energy;
+  }
+  c.sync();
+  return 0;
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) standard_kernel(const __grid_constant__ Params p, int64_t ne, bool batch,
+                                                       const double* __restrict__ coords,
+                                                       const int32_t* __restrict__ conn, const double* __restrict__ u,
+                                                       const double* __restrict__ state, int want_tangent,
+                                                       double* __restrict__ force, double* __restrict__ tangent,
+                                                       double* __restrict__ energy, double* __restrict__ trial,
+                                                       double* __restrict__ alpha_out, uint8_t* __restrict__ yield,
+                                                       int32_t* __restrict__ iterations, int32_t* __restrict__ code,
+                                                       int32_t* __restrict__ first_failure,
+                                                       const int32_t* __restrict__ order) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int epb = blockDim.x / G;
+  const int slot_in_block = threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  const int64_t slot = (int64_t)blockIdx.x * epb + slot_in_block;
+  ElemShared<G>* sh = reinterpret_cast<ElemShared<G>*>(smem_raw) + slot_in_block;
+  StdExtra<G>* xs = reinterpret_cast<StdExtra<G>*>(smem_raw + sizeof(ElemShared<G>) * epb) + slot_in_block;
+  const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+  const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
+  if (slot >= ne) return;
+  const int64_t e = order ? (int64_t)order[slot] : slot;
+  double hu_lane[9];
+  double warm_lane[8];
+  warm_lane[7] = 0.0;
+  Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, trial, yield, hu_lane, warm_lane};
+  ElemShared<G>& s = *sh;
+  if (lane < 8) {
+    if (batch) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        s.X[3 * lane + k] = coords[e * 24 + 3 * lane + k];
+        s.U[3 * lane + k] = u[e * 24 + 3 * lane + k];
+      }
+    } else {
+      const int64_t node = conn[e * 8 + lane];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        s.X[3 * lane + k] = coords[node * 3 + k];
+        s.U[3 * lane + k] = u[node * 3 + k];
+      }
+    }
+  }
+  c.sync();
+  int status = set_up<G>(c);
+  if (!status) status = std_points<G>(c, xs);
+  if (status) {
+    if (lane == 0) {
+      code[e] = status;
+      if (first_failure) atomicMin(first_failure, (int32_t)e);
+    }
+    return;
+  }
+  const bool sym = p.symmetric != 0;
+  const bool geometric = p.kinematics != SBK_SMALL_STRAIN;
+  const bool averaged = p.averaged != 0;
+  const bool finite = p.kinematics == SBK_FINITE;
+  const int nq = p.nq;
+  if (lane < 8) {
+    const int a = lane;
+    // f = sum w [B_NL^T S(T) + s (tr T) / 3], s = mean_row - d, in point order.
+    double ra[3] = {0, 0, 0}, en = 0.0;
+    for (int q = 0; q < nq; ++q) {
+      const double* sl = s.slot[q];
+      const double* ex = xs->pt[q];
+      const double* Fq = sl + kSlotF;
+      const double* Sq = ex + kStdST;
+      const double wq = sl[kSlotW];
+      double g[3];
+      node_grad(c, q, a, g);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        double v = bnl_t(Fq, g, k, Sq);
+        if (averaged) v += (xs->mean_row[3 * a + k] - bnl_t(Fq, g, k, ex + kStdPv)) * ex[kStdTr] / 3.0;
+        ra[k] += wq * v;
+      }
+      en += wq * sl[kSlotE];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) force[e * 24 + 3 * a + k] = ra[k];
+    if (a == 0) energy[e] = en;
+    if (want_tangent) {
+      // The volume average of g_a . g_b (finite + averaged).
+      double gbar[8];
+      if (averaged && finite) {
+#pragma unroll
+        for (int b = 0; b < 8; ++b) gbar[b] = 0.0;
+        double volume = 0.0;
+        for (int q = 0; q < nq; ++q) {
+          const double wq = s.slot[q][kSlotW];
+          double ga[3];
+          node_grad(c, q, a, ga);
+#pragma unroll
+          for (int b = 0; b < 8; ++b) {
+            double gb[3];
+            node_grad(c, q, b, gb);
+            gbar[b] += wq * (ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2]);
+          }
+          volume += wq;
+        }
+#pragma unroll
+        for (int b = 0; b < 8; ++b) gbar[b] /= volume;
+      }
+#pragma unroll 1
+      for (int chunk = 0; chunk < 2; ++chunk) {
+        double acc[4][9];
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+          for (int i = 0; i < 9; ++i) acc[b][i] = 0.0;
+        for (int q = 0; q < nq; ++q) {
+          const double* sl = s.slot[q];
+          const double* ex = xs->pt[q];
+          const double* Fq = sl + kSlotF;
+          const double wq = sl[kSlotW];
+          double g[3], V[27];
+          node_grad(c, q, a, g);
+          vtensor(sl, g, false, geometric, V);
+          double sa[3], la[3];
+          if (averaged) {
+            const double third = ex[kStdMcm] / 3.0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+              sa[k] = xs->mean_row[3 * a + k] - bnl_t(Fq, g, k, ex + kStdPv);
+              la[k] = bnl_t(Fq, g, k, ex + kStdU1) + third * sa[k];
+            }
+          }
+#pragma unroll
+          for (int b = 0; b < 4; ++b) {
+            const int bb = chunk * 4 + b;
+            double gb[3];
+            node_grad(c, q, bb, gb);
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+#pragma unroll
+              for (int l = 0; l < 3; ++l)
+                acc[b][k * 3 + l] += V[(k * 3 + l) * 3 + 0] * gb[0] + V[(k * 3 + l) * 3 + 1] * gb[1] +
+                                     V[(k * 3 + l) * 3 + 2] * gb[2];
+            if (averaged) {
+              double sb[3], mb[3];
+#pragma unroll
+              for (int l = 0; l < 3; ++l) {
+                sb[l] = xs->mean_row[3 * bb + l] - bnl_t(Fq, gb, l, ex + kStdPv);
+                mb[l] = bnl_t(Fq, gb, l, ex + kStdU2);
+              }
+              const double w3 = wq / 3.0;
+#pragma unroll
+              for (int k = 0; k < 3; ++k)
+#pragma unroll
+                for (int l = 0; l < 3; ++l) acc[b][k * 3 + l] += w3 * (la[k] * sb[l] + sa[k] * mb[l]);
+              if (finite) {
+                const double v = wq * (ex[kStdTr] / 3.0) * (gbar[bb] - (g[0] * gb[0] + g[1] * gb[1] + g[2] * gb[2]));
+#pragma unroll
+                for (int k = 0; k < 3; ++k) acc[b][k * 3 + k] += v;
+              }
+            }
+          }
+        }
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          double* out = tangent + e * 576 + (8 * a + chunk * 4 + b) * 9;
+#pragma unroll
+          for (int i = 0; i < 9; ++i) out[i] = acc[b][i];
+        }
+      }
+    }
+  }
+  if (want_tangent && sym) {
+    __threadfence_block();
+    c.sync();
+    if (lane < 8) {
+      double* Ke = tangent + e * 576;
+      auto at = [&](int i, int j) -> double* { return Ke + (8 * (i / 3) + j / 3) * 9 + 3 * (i % 3) + (j % 3); };
+      for (int k = 0; k < 3; ++k) {
+        const int i = 3 * lane + k;
+        for (int j = i + 1; j < 24; ++j) {
+          double* x1 = at(i, j);
+          double* y1 = at(j, i);
+          const double v = 0.5 * (*x1 + *y1);
+          *x1 = v;
+          *y1 = v;
+        }
+      }
+    }
+  }
+  if (lane == 0) {
+    iterations[e] = 0;
+    code[e] = 0;
+  }
+  for (int i = lane; i < 9; i += G) alpha_out[e * 9 + i] = 0.0;
+}
+
 // Stress recovery at the end of a step (incompatible_elastoplastic_stress,
 // IncompatibleModes.cpp:602-664, called for every element by the forming
 // driver, Forming.cpp:1266-1281): the kinematics at the committed modes
@@ -1430,6 +1827,29 @@ int launch_stress(const Params& p, int64_t ne, const double* coords, const int32
   return launch_stress_g<32>(p, ne, coords, conn, u, state, alpha_n, scratch, out, code, first_failure, 1, stream);
 }
 
+template <int G>
+int launch_standard_g(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
+                      const double* state, int want_tangent, double* force, double* tangent, double* energy,
+                      double* trial, double* alpha_out, uint8_t* yield, int32_t* iterations, int32_t* code,
+                      int32_t* first_failure, bool batch, int epb, const int32_t* order, cudaStream_t stream) {
+  const size_t per = sizeof(ElemShared<G>) + sizeof(StdExtra<G>);
+  const int most = (int)((227 * 1024) / per);
+  if (epb > most) epb = most;
+  if (epb * G > 256) epb = 256 / G;
+  const size_t smem = per * epb;
+  const int64_t blocks = (ne + epb - 1) / epb;
+  if (blocks == 0) return 0;
+  auto kern = standard_kernel<G>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return set_error(SBK_ERR_CUDA, std::string("standard kernel attribute: ") + cudaGetErrorString(err));
+  kern<<<(unsigned)blocks, epb * G, smem, stream>>>(p, ne, batch, coords, conn, u, state, want_tangent, force, tangent,
+                                                    energy, trial, alpha_out, yield, iterations, code, first_failure,
+                                                    order);
+  err = cudaGetLastError();
+  if (err != cudaSuccess) return set_error(SBK_ERR_CUDA, std::string("standard kernel launch: ") + cudaGetErrorString(err));
+  return 0;
+}
+
 size_t element_smem_bytes(int group) {
   return group == 8 ? sizeof(ElemShared<8>) : sizeof(ElemShared<32>);
 }
@@ -1439,6 +1859,16 @@ int launch_elements(const Params& p, int64_t ne, const double* coords, const int
                     double* energy, double* trial, double* alpha_out, uint8_t* yield, int32_t* iterations,
                     int32_t* code, int32_t* first_failure, bool batch, int elements_per_block,
                     const int32_t* order, cudaStream_t stream) {
+  if (p.element == 1) {
+    // The standard Hex8: the same launch shapes as K1.
+    if (p.nq <= 8)
+      return launch_standard_g<8>(p, ne, coords, conn, u, state, want_tangent, force, tangent, energy, trial,
+                                  alpha_out, yield, iterations, code, first_failure, batch,
+                                  elements_per_block > 0 ? elements_per_block : 16, order, stream);
+    return launch_standard_g<32>(p, ne, coords, conn, u, state, want_tangent, force, tangent, energy, trial,
+                                 alpha_out, yield, iterations, code, first_failure, batch,
+                                 elements_per_block > 0 ? elements_per_block : 8, order, stream);
+  }
   if (p.nq <= 8) {
     // At most what 227 KB of shared memory and 256 threads hold.
     const int most = (int)((227 * 1024) / sizeof(ElemShared<8>)) < 32 ? (int)((227 * 1024) / sizeof(ElemShared<8>)) : 32;

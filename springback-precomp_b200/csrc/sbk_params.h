@@ -45,6 +45,8 @@ struct Params {
   int kinematics;   // sbk_kinematics
   int nq;           // integration points
   int nfields;      // doubles per point of state
+  int element;      // 0 the incompatible-mode Hex8, 1 the standard Hex8
+  int averaged;     // standard Hex8: mean dilatation (B-bar)
   // The rule: xi, eta, zeta, weight per point.
   double qp[SBK_MAX_POINTS][4];
 };

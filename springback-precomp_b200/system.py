@@ -180,9 +180,19 @@ class Evaluation:
         return self.system.trial_modes()
 
 
+ELEMENTS = {"incompatible_modes": 0, "standard": 1}
+MEAN_DILATATION = {"auto": 0, "all": 1, "none": 2}
+
+
 class NonlinearSystem:
+    """element: "incompatible_modes" (the default) or "standard" (the
+    standard Hex8, Elastoplastic.cpp:226-340); mean_dilatation: "auto",
+    "all" or "none" (B-bar for the standard Hex8 under "auto" / "all"; the
+    incompatible-mode Hex8 refuses "all", NonlinearSystem.hpp:283-309)."""
+
     def __init__(self, mesh: HexMesh, material: Material, kinematics: str = "logarithmic", stiffness_points: int = 2,
-                 thickness_points: int = 0, thickness_axis: int = 2, stream=None):
+                 thickness_points: int = 0, thickness_axis: int = 2, stream=None, element: str = "incompatible_modes",
+                 mean_dilatation: str = "auto"):
         self.mesh = mesh
         self.material = material
         self.kinematics = kinematics
@@ -202,6 +212,13 @@ class NonlinearSystem:
                                                   _capi.KINEMATICS[kinematics], ctypes.byref(h)))
         self._h = h
         self.set_stream(stream)
+        if element not in ELEMENTS or mean_dilatation not in MEAN_DILATATION:
+            raise ValueError(f"unknown element {element!r} or mean_dilatation {mean_dilatation!r}")
+        _capi.check(_capi.lib().sbk_system_set_element(self._h, ELEMENTS[element], MEAN_DILATATION[mean_dilatation]))
+        self.element = element
+        av = ctypes.c_int(0)
+        _capi.check(_capi.lib().sbk_system_element(self._h, None, ctypes.byref(av)))
+        self.averaged = bool(av.value)
         pat = _capi.sbk_pattern()
         _capi.check(_capi.lib().sbk_system_pattern(self._h, ctypes.byref(pat)))
         self.num_dofs = int(pat.num_dofs)
