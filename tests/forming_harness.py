@@ -118,8 +118,13 @@ class FormingRun:
         integ = fixture.get("model", {}).get("integration", {})
         tp = int(integ.get("thickness_points", 0))
         axis = "xyz".index(integ.get("thickness_direction", "z"))
+        # The model's element formulation (the standard Hex8 unless it names
+        # incompatible modes) and the forming block's mean dilatation.
+        element = ("incompatible_modes" if fixture.get("model", {}).get("element_formulation") == "incompatible_modes"
+                   else "standard")
         self.system = pkg.NonlinearSystem(self.mesh, self.material, kinematics=kin, thickness_points=tp,
-                                          thickness_axis=axis)
+                                          thickness_axis=axis, element=element,
+                                          mean_dilatation=fixture.get("mean_dilatation", "auto"))
         extent = self.nodes.max(0) - self.nodes.min(0)
         self.tol = 1e-9 * float(np.linalg.norm(extent))
         self.tools = []

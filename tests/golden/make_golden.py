@@ -5,11 +5,14 @@ Run in a checkout that has the reference's sources (its Python package
 <reference root>``. The fixtures it writes are committed; the tests read
 only them, never the reference.
 
-strip_h2_im_nz4.json, strip_h1_im_nz4.json, plate_h2_im_mu0.1_drag3.json:
-committed forming runs of the reference
-(benchmarks/physics_audit/calculix/punch/<case>/sparlab): the mesh,
-the parts of its deck the element loop and the contact read (material,
-kinematics, tool, steps and their boundary regions), the nodal
+strip_h2_im_nz4.json, strip_h1_im_nz4.json, plate_h2_im_mu0.1_drag3.json
+(incompatible-mode Hex8) and strip_h2_std_mu0.1.json,
+plate_h2_std_mu0.1_drag3.json (standard Hex8 with mean dilatation),
+strip_h2_nobbar_mu0.1.json (standard Hex8 without): committed forming runs
+of the reference (benchmarks/physics_audit/calculix/punch/<case>/sparlab):
+the mesh, the parts of its deck the element loop and the contact read
+(material, model and element formulation, mean dilatation, kinematics,
+tool, steps and their boundary regions), the nodal
 displacements at the end of each step (17 significant digits in the
 reference's CSV output) and the tool force of every forming increment.
 
@@ -76,7 +79,9 @@ def strip(ref_root: str, case: str = "strip_h2_im_nz4") -> None:
     forces = [{k: r[k] for k in ("step", "increment", "t", "cx", "cz", "fx", "fz", "active_nodes")}
               for r in csv.DictReader(open(os.path.join(base, "out", "tool_forces.csv")))]
     out = {"source": os.path.relpath(base, ref_root), "nodes": mesh["nodes_m"], "elements": mesh["elements"],
-           "material": deck["material"], "kinematics": deck["forming"]["kinematics"],
+           "material": deck["material"], "model": deck.get("model", {}),
+           "mean_dilatation": deck["forming"].get("mean_dilatation", "auto"),
+           "kinematics": deck["forming"]["kinematics"],
            "tools": deck["forming"]["tools"], "steps": steps, "tool_forces": forces,
            "analysis": summary["analysis"]}
     with open(os.path.join(HERE, f"{case}.json"), "w") as f:
@@ -123,6 +128,7 @@ def challenge(ref_root: str, case: str = "kin_h0833") -> None:
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     main(root)
-    for case in ("strip_h2_im_nz4", "strip_h1_im_nz4", "plate_h2_im_mu0.1_drag3"):
+    for case in ("strip_h2_im_nz4", "strip_h1_im_nz4", "plate_h2_im_mu0.1_drag3", "strip_h2_std_mu0.1",
+                 "plate_h2_std_mu0.1_drag3", "strip_h2_nobbar_mu0.1"):
         strip(root, case)
     challenge(root)

@@ -13,7 +13,8 @@ import pytest
 from forming_harness import in_region, top_face_slaves
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-CASES = ["strip_h2_im_nz4", "strip_h1_im_nz4", "plate_h2_im_mu0.1_drag3"]
+CASES = ["strip_h2_im_nz4", "strip_h1_im_nz4", "plate_h2_im_mu0.1_drag3", "strip_h2_std_mu0.1",
+         "plate_h2_std_mu0.1_drag3", "strip_h2_nobbar_mu0.1"]
 
 
 def load(case):
