@@ -435,7 +435,8 @@ def run_partition(args, rank, world):
 
 
 def config(args, world):
-    return {"workload": f"element-kernel microbenchmark: {args.nx}x{args.ny}x{args.nz} IM Hex8 sheet "
+    element = "IM Hex8" if args.element == "incompatible_modes" else "standard Hex8 (B-bar)"
+    return {"workload": f"element-kernel microbenchmark: {args.nx}x{args.ny}x{args.nz} {element} sheet "
                         f"(0.04x0.04x0.5 mm cells), 2x2x2 points, Hill48 r=(0.73,0.80,0.70) + Chaboche "
                         f"(8000 MPa/200, 1200 MPa/20) + Voce, logarithmic strain, ~40% of points yielding; "
                         f"one step = NonlinearSystem.evaluate with tangent",
@@ -462,6 +463,8 @@ def main():
                    help="batched: the design-sweep batch (64 parts of 20k-150k elements) in one launch against the "
                         "same parts evaluated one at a time; partition: the free-free block of a Dirichlet "
                         "partition gathered from the full tangent, and the factorisation it feeds")
+    p.add_argument("--element", default="incompatible_modes", choices=["incompatible_modes", "standard"],
+                   help="standard: the standard Hex8 with mean dilatation on the same sheet and history")
     p.add_argument("--part-nx", type=int, default=200)
     p.add_argument("--part-ny", type=int, default=200)
     p.add_argument("--parts", type=int, default=64)
@@ -491,6 +494,9 @@ def main():
     sysm, u, s, mesh = wl.make_system_problem(args.nx, args.ny, args.nz, seed=replicas.replica_seed(7, rank),
                                               device=dev)
     ne = mesh.num_elements
+    if args.element == "standard":
+        # The standard Hex8 from the same committed history.
+        sysm.set_element("standard", "auto")
     if args.epb:
         sysm.set_elements_per_block(args.epb)
     sysm.set_timing(True)
@@ -554,26 +560,31 @@ def main():
             orc = oracle_module()
             prob, committed = oracle_problem(orc, args.sample_nx, args.sample_ny, args.nz, seed=7)
             cores = cpu_count()
-            all_rate, n_all = time_oracle(orc, prob, committed, cores, 10.0)
-            one_rate, n_one = time_oracle(orc, prob, committed, 1, 5.0)
+            std = orc.element(args.element == "standard", True)
+            with std:
+                all_rate, n_all = time_oracle(orc, prob, committed, cores, 10.0)
+                one_rate, n_one = time_oracle(orc, prob, committed, 1, 5.0)
             cpu = {"value": all_rate, "unit": UNIT, "cores": cores, "kind": "port",
                    "sample": f"{prob.mesh.num_elements} elements ({args.sample_nx}x{args.sample_ny}x{args.nz} of the "
                              f"same sheet, law and history construction), median of {n_all} runs on {cores} "
                              f"threads", "single_thread": one_rate}
             # Algorithmic flops per element (counting scalar) on the same sample.
-            cnt = orc.count_flops(prob.material.as_dict(), prob.mesh.element_coordinates(),
-                                  prob.mesh.gather(prob.u), committed, prob.alpha)
+            with std:
+                cnt = orc.count_flops(prob.material.as_dict(), prob.mesh.element_coordinates(),
+                                      prob.mesh.gather(prob.u), committed, prob.alpha)
             flops_per_element = cnt / prob.mesh.num_elements
         el_ms = statistics.mean(elem_ms)
         roofline = None
         if flops_per_element:
             achieved = flops_per_element * ne / (el_ms / 1e3) / 1e12
             roofline = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                        "frac": achieved / fp64_peak, "traffic": K1_DRAM_BYTES_PER_ELEMENT * ne,
+                        "frac": achieved / fp64_peak,
+                        "traffic": K1_DRAM_BYTES_PER_ELEMENT * ne if args.element == "incompatible_modes" else None,
                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one element_kernel "
                                           "launch on the 200x200x2 case, scaled by elements "
                                           "(profiles/element_kernel_microbench.md)",
-                        "kernel": "element_kernel (K1)", "kernel_ms": el_ms,
+                        "kernel": ("element_kernel (K1)" if args.element == "incompatible_modes"
+                                   else "standard_kernel (K1s)"), "kernel_ms": el_ms,
                         "flops_per_element": flops_per_element,
                         "peak_source": "measured in this run: cuBLAS FP64 GEMM 8192^3 burst (FP64 has no entry in "
                                        "MEASURED_PEAKS.json)"}

@@ -212,13 +212,7 @@ class NonlinearSystem:
                                                   _capi.KINEMATICS[kinematics], ctypes.byref(h)))
         self._h = h
         self.set_stream(stream)
-        if element not in ELEMENTS or mean_dilatation not in MEAN_DILATATION:
-            raise ValueError(f"unknown element {element!r} or mean_dilatation {mean_dilatation!r}")
-        _capi.check(_capi.lib().sbk_system_set_element(self._h, ELEMENTS[element], MEAN_DILATATION[mean_dilatation]))
-        self.element = element
-        av = ctypes.c_int(0)
-        _capi.check(_capi.lib().sbk_system_element(self._h, None, ctypes.byref(av)))
-        self.averaged = bool(av.value)
+        self.set_element(element, mean_dilatation)
         pat = _capi.sbk_pattern()
         _capi.check(_capi.lib().sbk_system_pattern(self._h, ctypes.byref(pat)))
         self.num_dofs = int(pat.num_dofs)
@@ -239,6 +233,17 @@ class NonlinearSystem:
 
     def set_stream(self, stream=None):
         _capi.check(_capi.lib().sbk_system_set_stream(self._h, _stream_ptr(stream)))
+
+    def set_element(self, element: str = "incompatible_modes", mean_dilatation: str = "auto"):
+        """The element formulation of the evaluations that follow (the
+        committed point states carry over; the standard Hex8 has no modes)."""
+        if element not in ELEMENTS or mean_dilatation not in MEAN_DILATATION:
+            raise ValueError(f"unknown element {element!r} or mean_dilatation {mean_dilatation!r}")
+        _capi.check(_capi.lib().sbk_system_set_element(self._h, ELEMENTS[element], MEAN_DILATATION[mean_dilatation]))
+        self.element = element
+        av = ctypes.c_int(0)
+        _capi.check(_capi.lib().sbk_system_element(self._h, None, ctypes.byref(av)))
+        self.averaged = bool(av.value)
 
     def set_stable_buffers(self, stable: bool = True):
         """Commit by copying on the device instead of exchanging buffers, so
