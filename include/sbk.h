@@ -148,7 +148,7 @@ int sbk_system_set_stream(sbk_system* sys, void* stream);
  * averaged (mean dilatation, B-bar) under "auto" or "all" when the rule has
  * more than one point, as NonlinearSystem's constructor decides
  * (NonlinearSystem.hpp:283-309); the incompatible-mode Hex8 refuses "all"
- * (SBK_ERR_CONFIG). Stress recovery stays the incompatible-mode Hex8's. */
+ * (SBK_ERR_CONFIG). */
 #define SBK_ELEMENT_INCOMPATIBLE_MODES 0
 #define SBK_ELEMENT_STANDARD 1
 #define SBK_MEAN_DILATATION_AUTO 0
@@ -257,7 +257,9 @@ int sbk_system_add_node_blocks(sbk_system* sys, int32_t n, const int32_t* nodes_
                                const double* blocks_dev);
 
 /* Stress recovery at the end of a step: elastoplastic_stress for every
- * element (IncompatibleModes.cpp:602-664, as the forming driver calls it at
+ * element (IncompatibleModes.cpp:602-664; for the standard Hex8
+ * Elastoplastic.cpp:342-430, the returns and the averaged measures at the
+ * mean-dilatation strain; as the forming driver calls it at
  * Forming.cpp:1266-1281) at the displacement u_dev (num_dofs, device), from
  * the committed points and modes - call it after sbk_system_commit. out_dev
  * (device) receives 28 doubles per element: the point averages of the Cauchy

@@ -737,6 +737,76 @@ class StdElement {
   StdElement(const Material& mat, const std::vector<QPoint>& rule, int kinematics, bool averaged)
       : mat_(mat), rule_(rule), kin_(kinematics), averaged_(averaged && rule.size() > 1) {}
 
+  /// elastoplastic_stress for the standard Hex8 (Elastoplastic.cpp:342-430):
+  /// the returns (elastic checks from the committed states) at the strain
+  /// the element takes - with mean dilatation the averaged one, which the
+  /// Cauchy stress (J-bar) and the averaged log strain follow - and the
+  /// point's own deformation for the largest strain and the smallest det F.
+  ElementStress stress(const double* x, const T* ue, const std::vector<State<T>>& committed) {
+    kinematics_of(x, ue);
+    ElementStress out;
+    out.min_jacobian = std::numeric_limits<double>::infinity();
+    const bool finite = kin_ == kFinite, logarithmic = kin_ == kLogarithmic;
+    auto absmax = [](const Mat<T, 3, 3>& m) {
+      double v = 0.0;
+      for (int i = 0; i < 9; ++i) v = std::max(v, std::fabs(val(m[i])));
+      return v;
+    };
+    for (std::size_t q = 0; q < pts_.size(); ++q) {
+      const Pt& p = pts_[q];
+      const Response<T> r = plastic_return(mat_, p.strain, committed[q], false);
+      Vec<T, 6> cauchy = r.stress, pk = r.stress;
+      Mat<T, 3, 3> f = p.h, sym;
+      for (int i = 0; i < 3; ++i) f(i, i) += T(1.0);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) sym(i, j) = T(0.5) * (p.h(i, j) + p.h(j, i));
+      if (logarithmic) {
+        pk = logarithmic_stress(p.log, r.stress);
+        const Vec<T, 6> tau = voigt_of(mul(mul(f, tensor3(pk)), tr(f)), 1.0);
+        Vec<T, 6> strain = p.strain;
+        for (int i = 3; i < 6; ++i) strain[i] = T(0.5) * strain[i];
+        const T j = exp(strain[0] + strain[1] + strain[2]);
+        for (int i = 0; i < 6; ++i) {
+          cauchy[i] = tau[i] / j;
+          out.kirchhoff[i] += val(tau[i]);
+          out.log_strain[i] += val(strain[i]);
+          const T own = i < 3 ? p.log.strain[i] : T(0.5) * p.log.strain[i];
+          out.max_strain = std::max(out.max_strain, std::fabs(val(own)));
+        }
+        out.min_jacobian = std::min(out.min_jacobian, val(det3(f)));
+      } else if (finite) {
+        const T j = det3(f);
+        const Vec<T, 6> c = voigt_of(mul(mul(f, tensor3(r.stress)), tr(f)), 1.0);
+        for (int i = 0; i < 6; ++i) cauchy[i] = c[i] / j;
+        Mat<T, 3, 3> green = sym;
+        const Mat<T, 3, 3> hth = mul(tr(p.h), p.h);
+        for (int i = 0; i < 9; ++i) green[i] += T(0.5) * hth[i];
+        out.max_strain = std::max(out.max_strain, absmax(green));
+        out.min_jacobian = std::min(out.min_jacobian, val(j));
+      } else {
+        out.max_strain = std::max(out.max_strain, absmax(sym));
+      }
+      for (int i = 0; i < 6; ++i) {
+        out.cauchy[i] += val(cauchy[i]);
+        out.piola_kirchhoff[i] += val(pk[i]);
+      }
+      out.max_eqps = std::max(out.max_eqps, val(r.state.eqps));
+    }
+    const double count = static_cast<double>(pts_.size());
+    for (int i = 0; i < 6; ++i) {
+      out.cauchy[i] /= count;
+      out.piola_kirchhoff[i] /= count;
+      out.kirchhoff[i] /= count;
+      out.log_strain[i] /= count;
+    }
+    const double* c = out.cauchy;
+    out.von_mises = std::sqrt(0.5 * ((c[0] - c[1]) * (c[0] - c[1]) + (c[1] - c[2]) * (c[1] - c[2]) +
+                                     (c[2] - c[0]) * (c[2] - c[0])) +
+                              3.0 * (c[3] * c[3] + c[4] * c[4] + c[5] * c[5]));
+    if (!finite && !logarithmic) out.min_jacobian = 1.0;
+    return out;
+  }
+
   ElementOut<T> evaluate(const double* x, const T* ue, const std::vector<State<T>>& committed,
                          bool want_tangent) {
     kinematics_of(x, ue);

@@ -331,10 +331,12 @@ int orc_element_stress(const double* material, int in_plane, int thickness, int 
 #pragma omp parallel for schedule(static) num_threads(nt) reduction(+ : failed)
   for (long long e = 0; e < ne; ++e) {
     IMElement<double> el(mat, rule, kinematics);
+    StdElement<double> std_el(mat, rule, kinematics, g_averaged != 0);
     std::vector<State<double>> c(static_cast<std::size_t>(nq));
     for (int q = 0; q < nq; ++q) c[q] = load_state<double>(committed + (e * nq + q) * kNF);
     try {
-      const ElementStress st = el.stress(X + e * 24, ue + e * 24, c, alpha ? alpha + e * 9 : nullptr);
+      const ElementStress st = g_standard ? std_el.stress(X + e * 24, ue + e * 24, c)
+                                          : el.stress(X + e * 24, ue + e * 24, c, alpha ? alpha + e * 9 : nullptr);
       double* o = out + e * 28;
       for (int i = 0; i < 6; ++i) {
         o[i] = st.cauchy[i];

@@ -942,8 +942,6 @@ int sbk_system_add_node_blocks(sbk_system* sys, int32_t n, const int32_t* nodes_
 
 int sbk_system_stress(sbk_system* sys, const double* u_dev, double* out_dev) {
   if (!sys || !u_dev || !out_dev) return fail(SBK_ERR_ARGUMENT, "null argument");
-  if (sys->p.element != 0)
-    return fail(SBK_ERR_UNSUPPORTED, "stress recovery is built for the incompatible-mode Hex8 only");
   cudaStream_t st = sys->stream;
   SBK_CUDA(cudaMemsetAsync(sys->first_fail, 0x7f, sizeof(int32_t), st));
   // The returns reproduce the committed states into the trial buffer, which

@@ -1604,7 +1604,8 @@ __global__ void __launch_bounds__(128) stress_kernel(const __grid_constant__ Par
       s.U[3 * lane + k] = u[node * 3 + k];
     }
   }
-  for (int i = lane; i < 9; i += G) s.alpha[i] = alpha_n ? alpha_n[e * 9 + i] : 0.0;
+  // The standard Hex8 has no modes: its kinematics are K1's at zero modes.
+  for (int i = lane; i < 9; i += G) s.alpha[i] = (alpha_n && !p.element) ? alpha_n[e * 9 + i] : 0.0;
   c.sync();
   int status = set_up<G>(c);
   if (status) {
@@ -1616,8 +1617,10 @@ __global__ void __launch_bounds__(128) stress_kernel(const __grid_constant__ Par
   }
   const int q = lane;
   int fail = 0, fcode = 0;
+  double h[9], F[9], sym[9], strain[6] = {0, 0, 0, 0, 0, 0};
+  LogKin L;
   if (q < p.nq) {
-    double gt[9], h[9], F[9];
+    double gt[9];
     mode_grads(c, q, gt);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
@@ -1630,13 +1633,10 @@ __global__ void __launch_bounds__(128) stress_kernel(const __grid_constant__ Par
       }
 #pragma unroll
     for (int i = 0; i < 9; ++i) F[i] = h[i] + ((i % 4) == 0 ? 1.0 : 0.0);
-    double sym[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
       for (int j = 0; j < 3; ++j) sym[i * 3 + j] = 0.5 * (h[i * 3 + j] + h[j * 3 + i]);
-    double strain[6];
-    LogKin L;
     if (p.kinematics == SBK_SMALL_STRAIN) {
       strain[0] = h[0];
       strain[1] = h[4];
@@ -1663,7 +1663,29 @@ __global__ void __launch_bounds__(128) stress_kernel(const __grid_constant__ Par
       }
       if (fcode) fail = (1 << 8) | q;
     }
-    if (!fail) {
+  }
+  // The standard Hex8 with mean dilatation (kinematics_of,
+  // Elastoplastic.cpp:140-167): every point's trace replaced by the volume
+  // average, once no point failed; the returns and the averaged measures
+  // take it, the largest strain component stays the point's own.
+  double own[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) own[i] = strain[i];
+  if (p.averaged && !__any_sync(c.mask, fail != 0)) {
+    const double w = q < p.nq ? s.geo[q][9] : 0.0;
+    double wt = w * (strain[0] + strain[1] + strain[2]), vol = w;
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1) {
+      wt += __shfl_xor_sync(c.mask, wt, o, G);
+      vol += __shfl_xor_sync(c.mask, vol, o, G);
+    }
+    const double shift = (wt / vol - (strain[0] + strain[1] + strain[2])) / 3.0;
+    strain[0] += shift;
+    strain[1] += shift;
+    strain[2] += shift;
+  }
+  if (q < p.nq && !fail) {
+    {
       PointState st{c.state + c.e * p.nq + q, c.trial + c.e * p.nq + q, c.npts};
       Response r;
       fcode = p.general ? general_return(p, strain, st, r) : radial_return(p, strain, st, r);
@@ -1700,7 +1722,7 @@ __global__ void __launch_bounds__(128) stress_kernel(const __grid_constant__ Par
 #pragma unroll
           for (int i = 0; i < 6; ++i) {
             cauchy[i] = tau[i] / vol;
-            max_strain = fmax(max_strain, fabs(lstr[i]));
+            max_strain = fmax(max_strain, fabs(i < 3 ? own[i] : 0.5 * own[i]));
           }
           jac = det3(F);
         } else if (p.kinematics == SBK_FINITE) {

@@ -60,3 +60,32 @@ def test_incompatible_modes_refuse_mean_dilatation_all(pkg, problem):
         pkg.NonlinearSystem(problem.mesh, problem.material, element="incompatible_modes", mean_dilatation="all")
     s = pkg.NonlinearSystem(problem.mesh, problem.material)
     assert s.element == "incompatible_modes" and not s.averaged
+
+
+@pytest.mark.parametrize("kin", ["small", "finite", "logarithmic"])
+@pytest.mark.parametrize("mean_dilatation", ["auto", "none"])
+def test_standard_stress_recovery_matches_oracle(pkg, orc, problem, cuda, kin, mean_dilatation):
+    """Step-end stress recovery of the standard Hex8 (elastoplastic_stress,
+    Elastoplastic.cpp:342-430) after a commit: the averages at the
+    committed points, with mean dilatation at the averaged strain, against
+    the oracle's restatement within 1e-11 of each field's scale."""
+    mesh, mat = problem.mesh, problem.material
+    s = pkg.NonlinearSystem(mesh, mat, kinematics=kin, element="standard", mean_dilatation=mean_dilatation)
+    s.set_committed(problem.state)
+    u = torch.tensor(problem.u if kin != "small" else 0.2 * problem.u, device=cuda)
+    s.evaluate(u, 0.0, False)
+    s.commit()
+    st, _ = s.committed_views()
+    committed = device_to_oracle(st.cpu().numpy(), mat.kinematic_terms)
+    got = s.stress(u)
+    with orc.element(True, mean_dilatation == "auto"):
+        ref, status = orc.element_stress(mat.as_dict(), mesh.element_coordinates(), mesh.gather(u.cpu().numpy()),
+                                         committed, None, kinematics=kin)
+    assert (status == 0).all()
+    packed = torch.cat([got.cauchy, got.piola_kirchhoff, got.von_mises[:, None], got.max_plastic_strain[:, None],
+                        got.max_strain[:, None], got.min_jacobian[:, None], got.kirchhoff, got.log_strain],
+                       dim=1).cpu().numpy()
+    for lo, hi in [(0, 6), (6, 12), (12, 13), (13, 14), (14, 15), (15, 16), (16, 22), (22, 28)]:
+        scale = max(np.abs(ref[:, lo:hi]).max(), 1e-300)
+        assert np.abs(packed[:, lo:hi] - ref[:, lo:hi]).max() <= 1e-11 * scale, (lo, hi)
+    assert ref[:, 13].max() > 0.0
