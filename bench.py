@@ -48,6 +48,9 @@ METRIC = "Hex8 tangent+residual+assembly elem/s (FP64)"
 # grows with the elements, so a launch of ne elements moves about ne times
 # this.
 K1_DRAM_BYTES_PER_ELEMENT = 16.11e9 / 80000
+# The same for the standard Hex8 kernel (profiles/standard_kernel_microbench.md:
+# 0.192 GB read + 1.610 GB written at 80,000 elements).
+K1S_DRAM_BYTES_PER_ELEMENT = (0.191949568e9 + 1.610487e9) / 80000
 # DRAM bytes per block entry of one free-free gather (assemble), from the ncu
 # capture of the 200 x 200 x 2 sheet's block (profiles/free_free_partition.md:
 # 271.0 MB read + 139.0 MB written for 22,528,485 entries).
@@ -579,10 +582,12 @@ def main():
             achieved = flops_per_element * ne / (el_ms / 1e3) / 1e12
             roofline = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                         "frac": achieved / fp64_peak,
-                        "traffic": K1_DRAM_BYTES_PER_ELEMENT * ne if args.element == "incompatible_modes" else None,
-                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one element_kernel "
-                                          "launch on the 200x200x2 case, scaled by elements "
-                                          "(profiles/element_kernel_microbench.md)",
+                        "traffic": (K1_DRAM_BYTES_PER_ELEMENT if args.element == "incompatible_modes"
+                                    else K1S_DRAM_BYTES_PER_ELEMENT) * ne,
+                        "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on "
+                                           "the 200x200x2 case, scaled by elements (profiles/"
+                                           + ("element_kernel_microbench.md)" if args.element == "incompatible_modes"
+                                              else "standard_kernel_microbench.md)")),
                         "kernel": ("element_kernel (K1)" if args.element == "incompatible_modes"
                                    else "standard_kernel (K1s)"), "kernel_ms": el_ms,
                         "flops_per_element": flops_per_element,
