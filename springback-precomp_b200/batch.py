@@ -42,7 +42,8 @@ class PartBatch:
     totals."""
 
     def __init__(self, meshes: Sequence[HexMesh], material: Material, kinematics: str = "logarithmic",
-                 stiffness_points: int = 2, thickness_points: int = 0, thickness_axis: int = 2, stream=None):
+                 stiffness_points: int = 2, thickness_points: int = 0, thickness_axis: int = 2, stream=None,
+                 element: str = "incompatible_modes", mean_dilatation: str = "auto"):
         nodes = np.cumsum([0] + [m.num_nodes for m in meshes])
         elems = np.cumsum([0] + [m.num_elements for m in meshes])
         coords = np.concatenate([m.coords for m in meshes])
@@ -50,7 +51,7 @@ class PartBatch:
         self.meshes = list(meshes)
         self.mesh = HexMesh(coords, conn)
         self.system = NonlinearSystem(self.mesh, material, kinematics, stiffness_points, thickness_points,
-                                      thickness_axis, stream)
+                                      thickness_axis, stream, element=element, mean_dilatation=mean_dilatation)
         outer = self.system.outer.cpu().numpy()
         dofs = 3 * nodes
         self.offsets = np.stack([nodes, elems, dofs, outer[dofs].astype(np.int64)], axis=1)

@@ -57,6 +57,25 @@ def test_batch_gives_every_part_its_own_result(pkg, cuda, batch_setup):
         assert torch.equal(view.values, oe.tangent)
 
 
+def test_standard_element_batch_gives_every_part_its_own_result(pkg, cuda, batch_setup):
+    """The same for the standard Hex8 with mean dilatation (the element of
+    the reference's springback_2mm preset): each element's averaged
+    dilatation is its own, so the batch changes no bit."""
+    batch_mod, meshes, mat, us = batch_setup
+    batch = batch_mod.PartBatch(meshes, mat, element="standard", mean_dilatation="auto")
+    assert batch.system.averaged
+    u = torch.tensor(np.concatenate(us), device=cuda)
+    ev = batch.evaluate(u)
+    assert ev.yielding_points > 0
+    internal, values = ev.internal.clone(), ev.tangent.clone()
+    for p, (m, up) in enumerate(zip(meshes, us)):
+        own = pkg.NonlinearSystem(m, mat, element="standard", mean_dilatation="auto")
+        oe = own.evaluate(torch.tensor(up, device=cuda), 0.0, True)
+        view = batch.part(p, internal, values)
+        assert torch.equal(view.internal, oe.internal)
+        assert torch.equal(view.values, oe.tangent)
+
+
 def test_graph_replay_across_commits(pkg, cuda, batch_setup):
     """A captured evaluation replayed at two displacements with a commit
     between equals the same sequence through plain evaluate calls."""
