@@ -62,6 +62,10 @@ struct __align__(16) ElemShared {
   double dir2[9];
   double r0[9];
   double lu[81];
+  // Lane 0's scratch of the local iteration (K_aa at alpha, its symmetric
+  // part, the Cholesky test, the shifted and Levenberg-Marquardt systems):
+  // in shared memory, where its serial loads stay close.
+  double work[243];
   double maxpivot;
   double dval[4];
   int rowp[9], colp[9], perm[9];
@@ -854,7 +858,7 @@ struct Local {
   // the factors of its K_aa.
   __device__ __noinline__ int run() {
     // K_aa at alpha (k0), its symmetric part and scratch: lane 0's alone.
-    double work[243];
+    double* work = s.work;
     {
       double at[9];
 #pragma unroll
