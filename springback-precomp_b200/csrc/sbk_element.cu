@@ -524,56 +524,88 @@ __device__ __noinline__ int pass(const Ctx<G>& c, const double at[9]) {
 
 // ---- element-level helpers (lane 0, shared memory) ---------------------------
 
-// FullPivLU of a (9x9 row-major) into lu; true if invertible (Eigen's rank test).
-__device__ __noinline__ bool fullpiv_lu9(const double* a, double* lu, int* rowp, int* colp, double* maxpivot_out) {
-  _Pragma("unroll 1") for (int i = 0; i < 81; ++i) lu[i] = a[i];
+// FullPivLU of a (9x9 row-major) into lu by the lanes of a group together
+// (every lane calls it); true if invertible (Eigen's rank test: every |U_ii|
+// above 9 eps of the largest pivot). Step k: lane l scans and eliminates
+// rows k + l, k + l + G, ...; the pivot is the group's largest |entry| of
+// the remaining block, ties to the first in column-major order as Eigen's
+// scan takes it; rows, then columns exchanged; the column below the pivot
+// multiplied by its reciprocal, then the rank-one update. rowp / colp hold
+// the transpositions.
+template <int G>
+__device__ __noinline__ bool fullpiv_lu9_rows(const Ctx<G>& c, const double* a, double* lu, int* rowp, int* colp,
+                                              double* maxpivot_out) {
+  const int lane = c.lane;
+  _Pragma("unroll 1") for (int i = lane; i < 81; i += G) lu[i] = a[i];
+  c.sync();
   double maxpivot = 0.0;
   int nonzero = 9;
   _Pragma("unroll 1") for (int k = 0; k < 9; ++k) {
-    int pr = k, pc = k;
     double big = -1.0;
+    int bi = k, bj = k;
     _Pragma("unroll 1") for (int j = k; j < 9; ++j)
-      _Pragma("unroll 1") for (int i = k; i < 9; ++i) {
+      _Pragma("unroll 1") for (int i = k + lane; i < 9; i += G) {
         const double v = fabs(lu[i * 9 + j]);
         if (v > big) {
           big = v;
-          pr = i;
-          pc = j;
+          bi = i;
+          bj = j;
         }
       }
+#pragma unroll
+    for (int o = G / 2; o >= 1; o >>= 1) {
+      const double ob = __shfl_xor_sync(c.mask, big, o, G);
+      const int oi = __shfl_xor_sync(c.mask, bi, o, G);
+      const int oj = __shfl_xor_sync(c.mask, bj, o, G);
+      if (ob > big || (ob == big && (oj < bj || (oj == bj && oi < bi)))) {
+        big = ob;
+        bi = oi;
+        bj = oj;
+      }
+    }
     if (big == 0.0) {
       nonzero = k;
-      _Pragma("unroll 1") for (int i = k; i < 9; ++i) rowp[i] = colp[i] = i;
       break;
     }
     if (big > maxpivot) maxpivot = big;
-    rowp[k] = pr;
-    colp[k] = pc;
-    if (pr != k)
-      _Pragma("unroll 1") for (int j = 0; j < 9; ++j) {
+    if (lane == 0) {
+      rowp[k] = bi;
+      colp[k] = bj;
+    }
+    if (bi != k)
+      _Pragma("unroll 1") for (int j = lane; j < 9; j += G) {
         const double t = lu[k * 9 + j];
-        lu[k * 9 + j] = lu[pr * 9 + j];
-        lu[pr * 9 + j] = t;
+        lu[k * 9 + j] = lu[bi * 9 + j];
+        lu[bi * 9 + j] = t;
       }
-    if (pc != k)
-      _Pragma("unroll 1") for (int i = 0; i < 9; ++i) {
+    c.sync();
+    if (bj != k)
+      _Pragma("unroll 1") for (int i = lane; i < 9; i += G) {
         const double t = lu[i * 9 + k];
-        lu[i * 9 + k] = lu[i * 9 + pc];
-        lu[i * 9 + pc] = t;
+        lu[i * 9 + k] = lu[i * 9 + bj];
+        lu[i * 9 + bj] = t;
       }
+    c.sync();
     const double inv = 1.0 / lu[k * 9 + k];
-    _Pragma("unroll 1") for (int i = k + 1; i < 9; ++i) lu[i * 9 + k] *= inv;
-    _Pragma("unroll 1") for (int i = k + 1; i < 9; ++i) {
-      const double l = lu[i * 9 + k];
+    _Pragma("unroll 1") for (int i = k + 1 + lane; i < 9; i += G) {
+      const double l = lu[i * 9 + k] * inv;
+      lu[i * 9 + k] = l;
       _Pragma("unroll 1") for (int j = k + 1; j < 9; ++j) lu[i * 9 + j] -= l * lu[k * 9 + j];
     }
+    c.sync();
   }
-  *maxpivot_out = maxpivot;
-  if (nonzero < 9) return false;
-  const double threshold = kEps * 9.0 * maxpivot;
-  _Pragma("unroll 1") for (int i = 0; i < 9; ++i)
-    if (!(fabs(lu[i * 9 + i]) > threshold)) return false;
-  return true;
+  if (lane == 0) {
+    _Pragma("unroll 1") for (int i = nonzero; i < 9; ++i) rowp[i] = colp[i] = i;
+    *maxpivot_out = maxpivot;
+  }
+  bool mine = true;
+  if (nonzero == 9) {
+    const double threshold = kEps * 9.0 * maxpivot;
+    _Pragma("unroll 1") for (int i = lane; i < 9; i += G) mine = mine && fabs(lu[i * 9 + i]) > threshold;
+  }
+  const bool ok = __all_sync(c.mask, mine) && nonzero == 9;
+  c.sync();
+  return ok;
 }
 
 // x = A^-1 b with the FullPivLU factors (any lane; b and x may alias).
@@ -635,6 +667,37 @@ __device__ __noinline__ bool llt9(double* a) {
   }
   return true;
 }
+// llt9 by the lanes of a group together (every lane calls it): step k's
+// diagonal by the lane of row k, then the rows below in parallel, each entry
+// the same dot product in the same order - the same factor and the same
+// answer.
+template <int G>
+__device__ __noinline__ bool llt9_rows(const Ctx<G>& c, double* a) {
+  const int lane = c.lane;
+  _Pragma("unroll 1") for (int k = 0; k < 9; ++k) {
+    int bad = 0;
+    if (lane == k % G) {
+      double x = a[k * 9 + k];
+      _Pragma("unroll 1") for (int j = 0; j < k; ++j) x -= a[k * 9 + j] * a[k * 9 + j];
+      if (x <= 0.0) {
+        bad = 1;
+      } else {
+        a[k * 9 + k] = sqrt(x);
+      }
+    }
+    bad = __shfl_sync(c.mask, bad, k % G, G);
+    c.sync();
+    if (bad) return false;
+    _Pragma("unroll 1") for (int i = k + 1 + ((lane - (k + 1)) % G + G) % G; i < 9; i += G) {
+      double v = a[i * 9 + k];
+      _Pragma("unroll 1") for (int j = 0; j < k; ++j) v -= a[i * 9 + j] * a[k * 9 + j];
+      a[i * 9 + k] = v / a[k * 9 + k];
+    }
+    c.sync();
+  }
+  return true;
+}
+
 __device__ __noinline__ void llt9_solve(const double* l, const double* b, double* x) {
   double y[9];
   _Pragma("unroll 1") for (int i = 0; i < 9; ++i) {
@@ -871,31 +934,31 @@ struct Local {
       const double largest = rinf();
       const double scale = vmax(s.scale);
       const double floor_ = kLocalRoundOff * vmax(s.flo);
-      if (c.lane == 0) {
-        s.ival[0] = fullpiv_lu9(s.kc, s.lu, s.rowp, s.colp, &s.maxpivot) ? 1 : 0;
-        // k0 and r0 copies (the trial passes overwrite the sums).
-        for (int i = 0; i < 81; ++i) work[i] = s.kc[i];
-        for (int i = 0; i < 9; ++i) s.r0[i] = s.r[24 + i];
-      }
+      const bool invertible = fullpiv_lu9_rows<G>(c, s.kc, s.lu, s.rowp, s.colp, &s.maxpivot);
+      // k0 and r0 copies (the trial passes overwrite the sums).
+      for (int i = c.lane; i < 81; i += G) work[i] = s.kc[i];
+      for (int i = c.lane; i < 9; i += G) s.r0[i] = s.r[24 + i];
       c.sync();
-      if (!s.ival[0]) return SBK_EL_LOCAL_SINGULAR;
+      if (!invertible) return SBK_EL_LOCAL_SINGULAR;
       if (largest <= kLocalTolerance * scale + floor_ || largest == 0.0) return 0;
       if (iterations == kMaxLocal || !isfinite(largest)) return SBK_EL_LOCAL_NO_CONVERGE;
       ++iterations;
       // Newton's direction and the Cholesky test of the symmetric part.
+      for (int idx = c.lane; idx < 81; idx += G) {
+        const int i = idx / 9, j = idx % 9;
+        const double v = 0.5 * (work[i * 9 + j] + work[j * 9 + i]);
+        work[81 + idx] = v;   // sym
+        work[162 + idx] = v;  // chol
+      }
+      c.sync();
       if (c.lane == 0) {
         double nw[9];
         fullpiv_solve9(s.lu, s.rowp, s.colp, s.r0, nw);
         for (int i = 0; i < 9; ++i) s.dir[i] = -nw[i];
-        double* sym = work + 81;
-        for (int i = 0; i < 9; ++i)
-          for (int j = 0; j < 9; ++j) sym[i * 9 + j] = 0.5 * (work[i * 9 + j] + work[j * 9 + i]);
-        double* chol = work + 162;
-        for (int i = 0; i < 81; ++i) chol[i] = sym[i];
-        s.ival[1] = llt9(chol) ? 1 : 0;
       }
+      const bool positive = llt9_rows<G>(c, work + 162);
       c.sync();
-      if (s.ival[1]) {
+      if (positive) {
         if (line_search(s.dir)) continue;
       } else {
         if (try_at(s.dir, 1.0)) {
