@@ -44,10 +44,10 @@ PKG = "springback-precomp_b200"
 METRIC = "Hex8 tangent+residual+assembly elem/s (FP64)"
 # DRAM bytes (read + write) per element of one element-kernel launch, from
 # the ncu capture of the same construction at 80,000 elements
-# (profiles/element_kernel_microbench.md: 16.11 GB / 80,000); the traffic
-# grows with the elements, so a launch of ne elements moves about ne times
-# this.
-K1_DRAM_BYTES_PER_ELEMENT = 16.11e9 / 80000
+# (profiles/element_kernel_microbench.md: 0.69 + 5.28 GB / 80,000); the
+# traffic grows with the elements, so a launch of ne elements moves about ne
+# times this.
+K1_DRAM_BYTES_PER_ELEMENT = (0.692594688e9 + 5.275133e9) / 80000
 # The same for the standard Hex8 kernel (profiles/standard_kernel_microbench.md:
 # 0.192 GB read + 1.610 GB written at 80,000 elements).
 K1S_DRAM_BYTES_PER_ELEMENT = (0.191949568e9 + 1.610487e9) / 80000
