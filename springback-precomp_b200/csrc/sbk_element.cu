@@ -142,7 +142,7 @@ __device__ __forceinline__ void bcol(const double F[9], const double g[3], int k
 // V(k, l, n) = sum_{j,i,m} g(j) F(k,i) F(l,m) D[v(i,j)][v(m,n)] (D, or D^T
 // with `transpose`), times w, plus the geometric w S(j,n) g(j) delta_kl:
 // K_ab(k, l) = sum_n V(k, l, n) g_b(n) is the block of B_a^T D B_b + G_a^T S G_b.
-__device__ __noinline__ void vtensor(const double* slot, const double g[3], bool transpose, bool geometric,
+__device__ __forceinline__ void vtensor(const double* slot, const double g[3], bool transpose, bool geometric,
                                      double V[27]) {
   const double w = slot[kSlotW];
   const double* D = slot;
