@@ -47,7 +47,8 @@ enum sbk_element_code {
   SBK_EL_LOCAL_NO_DESCENT = 5,   /* IncompatibleModes.cpp:537-545                  */
   SBK_EL_MESH_INVERTED = 6,      /* det J <= 0 (IncompatibleModes.cpp:159,176)     */
   SBK_EL_NONFINITE = 7,          /* LogarithmicStrain.cpp:110-112                  */
-  SBK_EL_DEGENERATE = 8          /* LogarithmicStrain.cpp:120-125                  */
+  SBK_EL_DEGENERATE = 8,         /* LogarithmicStrain.cpp:120-125                  */
+  SBK_EL_BAD_NODE = 9            /* a device connectivity names a node out of range */
 };
 
 enum sbk_kinematics { SBK_SMALL_STRAIN = 0, SBK_FINITE = 1, SBK_FINITE_LOGARITHMIC = 2 };
@@ -360,7 +361,10 @@ int sbk_contact_history(const sbk_contact* c, int32_t k, int32_t max_entries, do
  *   summed element by element in element order; NULL: no tangent),
  *   trial_dev / alpha_out_dev / yield_dev (as sbk_element_batch), and
  *   summary_dev: 5 doubles - energy, gross, yielding points, the lowest
- *   failing element (-1 if none) and its sbk_element_code.
+ *   failing element (-1 if none) and its sbk_element_code; an element whose
+ *   connectivity names a node out of range fails with SBK_EL_BAD_NODE and is
+ *   left out of the sums, and a mesh block the pattern lacks gives -2 and
+ *   SBK_EL_BAD_NODE.
  * The call only enqueues work on `stream`; read summary_dev after it. The
  * first call on a device looks up the array's device address (with that
  * device current), so make it before any stream capture. All calls share

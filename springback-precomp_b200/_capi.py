@@ -17,7 +17,7 @@ STATUS = {0: "OK", 1: "ARGUMENT", 2: "CONFIG", 3: "MESH", 4: "SOLVER", 5: "CUDA"
           7: "NO_EXTENSION"}
 ELEMENT_CODES = {0: "OK", 1: "INVERTED_POINT", 2: "RETURN_NO_CONVERGE", 3: "LOCAL_NO_CONVERGE",
                  4: "LOCAL_SINGULAR", 5: "LOCAL_NO_DESCENT", 6: "MESH_INVERTED", 7: "NONFINITE",
-                 8: "DEGENERATE"}
+                 8: "DEGENERATE", 9: "BAD_NODE"}
 KINEMATICS = {"small": 0, "finite": 1, "logarithmic": 2}
 MAX_POINTS = 32
 

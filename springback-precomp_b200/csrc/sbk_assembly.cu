@@ -119,12 +119,16 @@ __global__ void __launch_bounds__(kReduceThreads) finish_kernel(int nblocks, con
   }
 }
 
-__global__ void add_node_blocks_kernel(const int32_t* __restrict__ outer, const int32_t* __restrict__ inner,
+__global__ void add_node_blocks_kernel(int64_t nn, const int32_t* __restrict__ outer, const int32_t* __restrict__ inner,
                                        double* __restrict__ values, int32_t n, const int32_t* __restrict__ nodes,
                                        const double* __restrict__ blocks, int32_t* missing) {
   const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int32_t node = nodes[i];
+  if (node < 0 || node >= nn) {  // out of range: nothing is read or written
+    atomicExch(missing, 1);
+    return;
+  }
   for (int b = 0; b < 3; ++b) {
     const int32_t col = 3 * node + b;
     int32_t lo = outer[col], hi = outer[col + 1];
@@ -185,12 +189,18 @@ __global__ void __launch_bounds__(256) stiffness_rows_kernel(int64_t nn, const i
 
 // Second half: the sum of squares over the listed free DOFs, per block.
 __global__ void __launch_bounds__(kReduceThreads) free_squares_kernel(int32_t n, const int32_t* __restrict__ free_dofs,
+                                                                      int64_t ndofs,
                                                                       const double* __restrict__ product,
-                                                                      double* __restrict__ partial) {
+                                                                      double* __restrict__ partial, int32_t* bad) {
   __shared__ double sh[kReduceThreads];
   double s = 0.0;
   for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    const double v = product[free_dofs[i]];
+    const int32_t d = free_dofs[i];
+    if (d < 0 || d >= ndofs) {  // out of range: skipped and reported
+      atomicExch(bad, 1);
+      continue;
+    }
+    const double v = product[d];
     s += v * v;
   }
   s = block_sum(s, sh);
@@ -226,12 +236,13 @@ int launch_summary(const double* scalars, const int32_t* first_failure, const in
 
 int launch_stiffness_gross(int64_t nn, const int32_t* outer, const int32_t* inner, const double* values,
                            const double* u, int32_t num_free, const int32_t* free_dofs, double* product,
-                           double* scratch, double* scalars, cudaStream_t stream) {
+                           double* scratch, double* scalars, int32_t* bad, cudaStream_t stream) {
   int64_t blocks = (nn + 255) / 256;
   if (blocks > 148 * 32) blocks = 148 * 32;
   if (blocks > 0)
     stiffness_rows_kernel<<<(unsigned)blocks, 256, 0, stream>>>(nn, outer, inner, values, u, product);
-  free_squares_kernel<<<kReduceBlocks, kReduceThreads, 0, stream>>>(num_free, free_dofs, product, scratch);
+  free_squares_kernel<<<kReduceBlocks, kReduceThreads, 0, stream>>>(num_free, free_dofs, 3 * nn, product, scratch,
+                                                                     bad);
   finish_kernel<<<1, kReduceThreads, 0, stream>>>(kReduceBlocks, scratch, scalars);
   return (int)cudaGetLastError();
 }
@@ -255,10 +266,10 @@ int launch_assemble_forces(const GatherMaps& m, const double* force, const doubl
   return (int)cudaGetLastError();
 }
 
-int launch_add_node_blocks(const int32_t* outer, const int32_t* inner, double* values, int32_t n,
+int launch_add_node_blocks(int64_t nn, const int32_t* outer, const int32_t* inner, double* values, int32_t n,
                            const int32_t* nodes, const double* blocks, int32_t* missing, cudaStream_t stream) {
   if (n <= 0) return 0;
-  add_node_blocks_kernel<<<(n + 127) / 128, 128, 0, stream>>>(outer, inner, values, n, nodes, blocks, missing);
+  add_node_blocks_kernel<<<(n + 127) / 128, 128, 0, stream>>>(nn, outer, inner, values, n, nodes, blocks, missing);
   return (int)cudaGetLastError();
 }
 

@@ -615,6 +615,7 @@ int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const 
   rc = make_params(material, rule, kinematics, p);
   if (rc) return rc;
   sbk_system* s = new sbk_system();
+  p.num_nodes = mesh->num_nodes;
   s->p = p;
   s->nn = mesh->num_nodes;
   s->ne = mesh->num_elements;
@@ -931,12 +932,13 @@ int sbk_system_add_node_blocks(sbk_system* sys, int32_t n, const int32_t* nodes_
   if (n <= 0) return SBK_OK;
   cudaStream_t st = sys->stream;
   SBK_CUDA(cudaMemsetAsync(sys->missing, 0, sizeof(int32_t), st));
-  int rc = sbk::launch_add_node_blocks(sys->outer, sys->inner, sys->values, n, nodes_dev, blocks_dev, sys->missing, st);
+  int rc = sbk::launch_add_node_blocks(sys->nn, sys->outer, sys->inner, sys->values, n, nodes_dev, blocks_dev,
+                                       sys->missing, st);
   if (rc) return fail(SBK_ERR_CUDA, "add_node_blocks launch");
   int32_t missing = 0;
   SBK_CUDA(cudaMemcpyAsync(&missing, sys->missing, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   SBK_CUDA(cudaStreamSynchronize(st));
-  if (missing) return fail(SBK_ERR_ARGUMENT, "a node block lies outside the pattern");
+  if (missing) return fail(SBK_ERR_ARGUMENT, "a node block names a node out of range or lies outside the pattern");
   return SBK_OK;
 }
 
@@ -969,12 +971,16 @@ int sbk_system_stiffness_gross(sbk_system* sys, const double* u_dev, int32_t num
     return fail(SBK_ERR_ARGUMENT, "null argument");
   if (!sys->has_values) return fail(SBK_ERR_ARGUMENT, "stiffness_gross needs an evaluate with the tangent first");
   cudaStream_t st = sys->stream;
+  SBK_CUDA(cudaMemsetAsync(sys->missing, 0, sizeof(int32_t), st));
   int rc = sbk::launch_stiffness_gross(sys->nn, sys->outer, sys->inner, sys->values, u_dev, num_free, free_dev,
-                                       sys->product, sys->scratch, sys->scalars, st);
+                                       sys->product, sys->scratch, sys->scalars, sys->missing, st);
   if (rc) return fail(SBK_ERR_CUDA, "stiffness_gross launch");
   double sum = 0.0;
+  int32_t bad = 0;
   SBK_CUDA(cudaMemcpyAsync(&sum, sys->scalars, sizeof(double), cudaMemcpyDeviceToHost, st));
+  SBK_CUDA(cudaMemcpyAsync(&bad, sys->missing, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   SBK_CUDA(cudaStreamSynchronize(st));
+  if (bad) return fail(SBK_ERR_ARGUMENT, "a free DOF lies outside the model");
   *out = std::sqrt(sum);
   return SBK_OK;
 }

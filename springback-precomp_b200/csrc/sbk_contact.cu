@@ -598,6 +598,16 @@ int sbk_contact_create(const sbk_mesh* mesh, int32_t num_tools, const sbk_tool* 
       free_contact(c);
       return cfail(SBK_ERR_ARGUMENT, "an invalid tool");
     }
+    for (int32_t i = 0; i < s.num_slaves; ++i) {
+      // Every slave node inside the mesh and in ascending order, its area and
+      // penalty finite and non-negative: the kernels index by them.
+      if (s.nodes[i] < 0 || s.nodes[i] >= mesh->num_nodes || (i > 0 && s.nodes[i] <= s.nodes[i - 1]) ||
+          !std::isfinite(s.area[i]) || !(s.area[i] >= 0.0) || !std::isfinite(s.kappa[i]) || !(s.kappa[i] >= 0.0)) {
+        free_contact(c);
+        return cfail(SBK_ERR_ARGUMENT, "a tool's slave nodes must lie in the mesh, ascending, with finite "
+                                       "non-negative areas and penalties");
+      }
+    }
     if (s.shape != 1 && !(s.radius > 0.0)) {
       free_contact(c);
       return cfail(SBK_ERR_CONFIG, "a sphere or cylinder needs a positive radius");

@@ -1073,7 +1073,9 @@ __global__ void __launch_bounds__(256) element_kernel(const __grid_constant__ Pa
   warm_lane[7] = 0.0;  // no closest point yet
   Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, trial, yield, hu_lane, warm_lane};
   ElemShared<G>& s = *sh;
-  // Stage the element's coordinates and displacements (lane a: node a).
+  // Stage the element's coordinates and displacements (lane a: node a); a
+  // node index out of range fails the element before anything is read.
+  int bad_node = 0;
   if (lane < 8) {
     if (batch) {
 #pragma unroll
@@ -1083,12 +1085,23 @@ __global__ void __launch_bounds__(256) element_kernel(const __grid_constant__ Pa
       }
     } else {
       const int64_t node = conn[e * 8 + lane];
+      if (p.num_nodes > 0 && (node < 0 || node >= p.num_nodes)) {
+        bad_node = 1;
+      } else {
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        s.X[3 * lane + k] = coords[node * 3 + k];
-        s.U[3 * lane + k] = u[node * 3 + k];
+        for (int k = 0; k < 3; ++k) {
+          s.X[3 * lane + k] = coords[node * 3 + k];
+          s.U[3 * lane + k] = u[node * 3 + k];
+        }
       }
     }
+  }
+  if (__any_sync(mask, bad_node)) {
+    if (lane == 0) {
+      code[e] = SBK_EL_BAD_NODE;
+      if (first_failure) atomicMin(first_failure, (int32_t)e);
+    }
+    return;
   }
   for (int i = lane; i < 9; i += G) s.alpha[i] = alpha_n ? alpha_n[e * 9 + i] : 0.0;
   c.sync();
@@ -1467,6 +1480,7 @@ __global__ void __launch_bounds__(256) standard_kernel(const __grid_constant__ P
   warm_lane[7] = 0.0;
   Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, trial, yield, hu_lane, warm_lane};
   ElemShared<G>& s = *sh;
+  int bad_node = 0;
   if (lane < 8) {
     if (batch) {
 #pragma unroll
@@ -1476,12 +1490,23 @@ __global__ void __launch_bounds__(256) standard_kernel(const __grid_constant__ P
       }
     } else {
       const int64_t node = conn[e * 8 + lane];
+      if (p.num_nodes > 0 && (node < 0 || node >= p.num_nodes)) {
+        bad_node = 1;
+      } else {
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        s.X[3 * lane + k] = coords[node * 3 + k];
-        s.U[3 * lane + k] = u[node * 3 + k];
+        for (int k = 0; k < 3; ++k) {
+          s.X[3 * lane + k] = coords[node * 3 + k];
+          s.U[3 * lane + k] = u[node * 3 + k];
+        }
       }
     }
+  }
+  if (__any_sync(mask, bad_node)) {
+    if (lane == 0) {
+      code[e] = SBK_EL_BAD_NODE;
+      if (first_failure) atomicMin(first_failure, (int32_t)e);
+    }
+    return;
   }
   c.sync();
   int status = set_up<G>(c);
@@ -1663,13 +1688,25 @@ __global__ void __launch_bounds__(128) stress_kernel(const __grid_constant__ Par
   double hu_lane[9];
   Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, scratch, nullptr, hu_lane, nullptr};
   ElemShared<G>& s = *sh;
+  int bad_node = 0;
   if (lane < 8) {
     const int64_t node = conn[e * 8 + lane];
+    if (p.num_nodes > 0 && (node < 0 || node >= p.num_nodes)) {
+      bad_node = 1;
+    } else {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      s.X[3 * lane + k] = coords[node * 3 + k];
-      s.U[3 * lane + k] = u[node * 3 + k];
+      for (int k = 0; k < 3; ++k) {
+        s.X[3 * lane + k] = coords[node * 3 + k];
+        s.U[3 * lane + k] = u[node * 3 + k];
+      }
     }
+  }
+  if (__any_sync(mask, bad_node)) {
+    if (lane == 0) {
+      code[e] = SBK_EL_BAD_NODE;
+      atomicMin(first_failure, (int32_t)e);
+    }
+    return;
   }
   // The standard Hex8 has no modes: its kinematics are K1's at zero modes.
   for (int i = lane; i < 9; i += G) s.alpha[i] = (alpha_n && !p.element) ? alpha_n[e * 9 + i] : 0.0;

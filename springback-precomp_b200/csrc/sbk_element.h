@@ -66,7 +66,7 @@ int launch_summary(const double* scalars, const int32_t* first_failure, const in
 // squares of its listed free DOFs into scalars[0] (scratch as for the forces).
 int launch_stiffness_gross(int64_t nn, const int32_t* outer, const int32_t* inner, const double* values,
                            const double* u, int32_t num_free, const int32_t* free_dofs, double* product,
-                           double* scratch, double* scalars, cudaStream_t stream);
+                           double* scratch, double* scalars, int32_t* bad, cudaStream_t stream);
 // The schedule of the next element launch: the elements bucketed by the
 // cost of their last evaluation (local iterations, yielding points), so
 // that elements of alike cost share a warp. scratch: schedule_scratch_ints().
@@ -74,7 +74,7 @@ int launch_schedule(int64_t ne, int nq, const int32_t* iterations, const uint8_t
                     int32_t* order, cudaStream_t stream);
 size_t schedule_scratch_ints(int64_t ne);
 // add_node_block for n blocks, in list order.
-int launch_add_node_blocks(const int32_t* outer, const int32_t* inner, double* values, int32_t n,
-                           const int32_t* nodes, const double* blocks, int32_t* missing, cudaStream_t stream);
+int launch_add_node_blocks(int64_t nn, const int32_t* outer, const int32_t* inner, double* values, int32_t n,
+                          const int32_t* nodes, const double* blocks, int32_t* missing, cudaStream_t stream);
 
 }  // namespace sbk

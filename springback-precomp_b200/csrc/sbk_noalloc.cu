@@ -82,16 +82,29 @@ __global__ void __launch_bounds__(576) scatter_small_kernel(
   __syncthreads();
   const int r = t / 24, c = t % 24;
   const int a = r / 3, ka = r % 3, b = c / 3, kb = c % 3;
+  __shared__ int mismatch;
+  if (t == 0) mismatch = 0;
+  __syncthreads();
   for (int e = 0; e < ne; ++e) {
     const int32_t* nodes = conn + 8 * (int64_t)e;
+    // An element naming a node out of range (failed by the element kernel)
+    // is left out; a block the caller's pattern lacks is reported.
+    bool inside = true;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) inside = inside && nodes[k] >= 0 && nodes[k] < nn;
+    if (!inside) continue;  // the same for every thread
     if (values) {
       const int32_t row = 3 * nodes[a] + ka, col = 3 * nodes[b] + kb;
       int32_t lo = outer[col], hi = outer[col + 1];
+      const int32_t end = hi;
       while (lo < hi) {
         const int32_t mid = lo + (hi - lo) / 2;
         if (inner[mid] < row) lo = mid + 1; else hi = mid;
       }
-      values[lo] += s->tangent[(int64_t)e * 576 + (8 * a + b) * 9 + 3 * ka + kb];
+      if (lo < end && inner[lo] == row)
+        values[lo] += s->tangent[(int64_t)e * 576 + (8 * a + b) * 9 + 3 * ka + kb];
+      else
+        mismatch = 1;
     }
     if (t < 24) {
       const int32_t dof = 3 * nodes[t / 3] + t % 3;
@@ -122,6 +135,10 @@ __global__ void __launch_bounds__(576) scatter_small_kernel(
     summary[2] = (double)y;
     summary[3] = first == 0x7f7f7f7f ? -1.0 : (double)first;
     summary[4] = first == 0x7f7f7f7f ? 0.0 : (double)s->code[first];
+    if (mismatch && first == 0x7f7f7f7f) {  // the pattern does not cover the mesh
+      summary[3] = -2.0;
+      summary[4] = (double)SBK_EL_BAD_NODE;
+    }
   }
 }
 
@@ -145,6 +162,7 @@ extern "C" int sbk_evaluate_noalloc(const sbk_material* material, const sbk_rule
   sbk::Params p;
   int rc = sbk::make_launch_params(material, rule, kinematics, p);
   if (rc) return rc;
+  p.num_nodes = num_nodes;  // the element kernel checks the caller's connectivity against it
   Scratch* s = nullptr;
   rc = scratch_address(&s);
   if (rc) return rc;

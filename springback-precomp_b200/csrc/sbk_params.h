@@ -47,6 +47,7 @@ struct Params {
   int nfields;      // doubles per point of state
   int element;      // 0 the incompatible-mode Hex8, 1 the standard Hex8
   int averaged;     // standard Hex8: mean dilatation (B-bar)
+  int num_nodes;    // mesh mode: node indices are checked against it (0: batch mode, unchecked)
   // The rule: xi, eta, zeta, weight per point.
   double qp[SBK_MAX_POINTS][4];
 };

@@ -166,6 +166,23 @@ def test_node_through_the_tool_is_refused(pkg, orc, cuda):
         gpu.evaluate(torch.tensor(u, device=cuda), 0.0, True)
 
 
+def test_slave_nodes_outside_the_mesh_are_refused(pkg, cuda):
+    """A tool whose slave list names a node outside the mesh, or repeats
+    one, is refused when the contact is made (the kernels index by it)."""
+    mesh = sheet(pkg)
+    for bad in ("out_of_range", "repeated"):
+        tool = tools_for(mesh, "sphere", 0.0)
+        nodes = np.array(tool["nodes"])
+        if bad == "out_of_range":
+            nodes[-1] = mesh.num_nodes
+        else:
+            nodes[1] = nodes[0]
+        tool["nodes"] = nodes
+        # (the Python wrapper already refuses a list that does not ascend)
+        with pytest.raises((ValueError, pkg.SbkError)):
+            pkg.ToolContact(mesh, [pkg.Tool(**tool)])
+
+
 def test_contact_blocks_into_the_system_tangent(pkg, orc, cuda):
     """add_node_block of the contact blocks into the assembled tangent
     (src/fem/Forming.cpp:280-297) equals the oracle's."""

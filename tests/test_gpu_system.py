@@ -214,3 +214,19 @@ def test_stress_recovery_matches_oracle(pkg, orc, problem, cuda, kin):
         assert np.abs(packed[:, lo:hi] - ref[:, lo:hi]).max() <= 1e-11 * scale, (lo, hi)
     if kin == "logarithmic":
         assert ref[:, 13].max() > 0.0
+
+
+def test_out_of_range_indices_are_refused(pkg, problem, cuda):
+    """Node blocks naming a node outside the mesh and free DOFs outside the
+    model are refused: the kernels check each index before using it."""
+    mesh = problem.mesh
+    sys_ = make_system(pkg, problem)
+    u = torch.tensor(problem.u, device=cuda)
+    sys_.evaluate(u, 0.0, True)
+    nodes = torch.tensor([0, mesh.num_nodes], dtype=torch.int32, device=cuda)
+    blocks = torch.zeros((2, 3, 3), dtype=torch.float64, device=cuda)
+    with pytest.raises(pkg.SbkError):
+        sys_.add_node_blocks(nodes, blocks)
+    free = torch.tensor([0, 1, mesh.num_dofs], dtype=torch.int32, device=cuda)
+    with pytest.raises(pkg.SbkError):
+        sys_.stiffness_gross(u, free)

@@ -82,3 +82,31 @@ def test_noalloc_refuses_a_mesh_beyond_its_maximum(pkg, cuda):
                                 buf, torch.zeros(8 * n, dtype=torch.uint8, device=cuda),
                                 torch.zeros(5, dtype=torch.float64, device=cuda))
     assert err.value.status == 6 and "2048" in str(err.value)
+
+
+def test_noalloc_fails_an_element_naming_a_node_out_of_range(pkg, cuda):
+    """The caller's device connectivity is not checked on the host: an
+    element naming a node out of range fails (SBK_EL_BAD_NODE) before
+    anything of it is read, and the sums leave it out."""
+    wl = importlib.import_module("springback-precomp_b200.workload")
+    system = importlib.import_module("springback-precomp_b200.system")
+    prob = wl.make_problem(6, 4, 1, seed=3, sample=24)
+    mesh, mat = prob.mesh, prob.material
+    sysm = pkg.NonlinearSystem(mesh, mat, kinematics="logarithmic")
+    u = torch.tensor(prob.u, device=cuda)
+    coords = torch.tensor(mesh.coords, device=cuda)
+    conn = torch.tensor(mesh.connectivity, device=cuda)
+    conn[5, 3] = mesh.num_nodes  # one past the last node
+    state = torch.tensor(prob.state, device=cuda)
+    alpha = torch.tensor(prob.alpha, device=cuda)
+    internal = torch.empty(mesh.num_dofs, dtype=torch.float64, device=cuda)
+    values = torch.empty(sysm.nnz, dtype=torch.float64, device=cuda)
+    trial = torch.empty_like(state)
+    alpha_out = torch.empty_like(alpha)
+    yielding = torch.zeros((mesh.num_elements, 8), dtype=torch.uint8, device=cuda)
+    summary = torch.empty(5, dtype=torch.float64, device=cuda)
+    system.evaluate_noalloc(mat, coords, conn, u, state, alpha, sysm.outer.clone(), sysm.inner.clone(), internal,
+                            values, trial, alpha_out, yielding, summary)
+    torch.cuda.synchronize()
+    s = summary.cpu().numpy()
+    assert s[3] == 5.0 and int(s[4]) == 9, s
