@@ -593,6 +593,13 @@ int sbk_partition_create(int64_t num_dofs, const int32_t* outer_dev, const int32
   PCUDA(cudaMemcpy(inner.data(), inner_dev, sizeof(int32_t) * inner.size(), cudaMemcpyDeviceToHost));
   if (outer[0] != 0 || outer[(size_t)num_dofs] != nnz)
     return pfail(SBK_ERR_ARGUMENT, "sbk_partition_create: the pattern's offsets do not span nnz");
+  for (int64_t c = 0; c < num_dofs; ++c) {
+    if (outer[(size_t)c + 1] < outer[(size_t)c])
+      return pfail(SBK_ERR_ARGUMENT, "sbk_partition_create: the pattern's offsets decrease");
+    for (int32_t k = outer[(size_t)c]; k < outer[(size_t)c + 1]; ++k)
+      if (inner[(size_t)k] < 0 || inner[(size_t)k] >= num_dofs || (k > outer[(size_t)c] && inner[(size_t)k] <= inner[(size_t)k - 1]))
+        return pfail(SBK_ERR_ARGUMENT, "sbk_partition_create: a column's rows are out of range or not ascending");
+  }
   sbk_partition* P = new sbk_partition;
   P->n = num_dofs;
   P->nnz = nnz;
