@@ -44,6 +44,7 @@ _ll = ctypes.c_longlong
 
 def _declare(L):
     L.orc_set_element.argtypes = [ctypes.c_int, ctypes.c_int]
+    L.orc_vjp_x.argtypes = [_d] + [ctypes.c_int] * 4 + [_ll, _d, _d, _d, _d, _d, _d, _i]
     L.orc_rule_size.argtypes = [ctypes.c_int] * 3
     L.orc_rule.argtypes = [ctypes.c_int] * 3 + [_d]
     L.orc_yield_matrix.argtypes = [_d, _d]
@@ -231,6 +232,28 @@ def count_flops(m: dict, X, ue, committed=None, alpha_n=None, kinematics="logari
                else np.ascontiguousarray(alpha_n, dtype=np.float64).reshape(ne, 9))
     return int(lib().orc_count_flops(_p(rec), in_plane, thickness, axis, KIN[kinematics], ne, _p(X), _p(ue),
                                      _p(committed), _p(alpha_n), int(want_tangent)))
+
+
+def vjp_x(m: dict, X, ue, lam, committed=None, alpha_n=None, kinematics="logarithmic", in_plane=2, thickness=0,
+          axis=2):
+    """lambda . d f*/d X per IM Hex8 (ne, 24) at fixed ue and committed
+    history, the modes through their local equilibrium; and a status per
+    element."""
+    rec = material_record(m)
+    X = np.ascontiguousarray(X, dtype=np.float64).reshape(-1, 24)
+    ne = X.shape[0]
+    ue = np.ascontiguousarray(ue, dtype=np.float64).reshape(ne, 24)
+    lam = np.ascontiguousarray(lam, dtype=np.float64).reshape(ne, 24)
+    nq = lib().orc_rule_size(in_plane, thickness, axis)
+    committed = (np.zeros((ne, nq, NF)) if committed is None
+                 else np.ascontiguousarray(committed, dtype=np.float64).reshape(ne, nq, NF))
+    alpha_n = (np.zeros((ne, 9)) if alpha_n is None
+               else np.ascontiguousarray(alpha_n, dtype=np.float64).reshape(ne, 9))
+    out = np.zeros((ne, 24))
+    st = np.zeros(ne, dtype=np.int32)
+    lib().orc_vjp_x(_p(rec), in_plane, thickness, axis, KIN[kinematics], ne, _p(X), _p(ue), _p(committed),
+                    _p(alpha_n), _p(lam), _p(out), _p(st, _i))
+    return out, st
 
 
 def pattern(nn: int, conn) -> dict:

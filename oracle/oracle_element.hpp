@@ -278,6 +278,222 @@ class IMElement {
   IMElement(const Material& mat, const std::vector<QPoint>& rule, int kinematics)
       : mat_(mat), rule_(rule), kin_(kinematics) {}
 
+  /// The vector-Jacobian product of the condensed residual with respect to
+  /// the element's reference coordinates, out[3a+i] = lambda . d f* / d X_ia,
+  /// at fixed displacements and committed history (finite or logarithmic
+  /// kinematics), the modes following through their local equilibrium:
+  ///   d f*/dX = d r_u/dX + K_ua d alpha/dX,  K_aa d alpha/dX = -d r_a/dX,
+  /// so lambda^T d f*/dX = [lambda; mu]^T d r/dX|_alpha with
+  /// mu = -K_aa^-T K_ua^T lambda and r = (r_u, r_a) = sum_q w F S [G | G~].
+  /// Per point the chain runs r -> (F, S, [G | G~], w); S -> E (the point's
+  /// material tangent dS/dE) -> F; F = I + U [G | G~]^T -> [G | G~];
+  /// G = dN J^-1, G~ = (det0/det)(-2 xi) J0^-1, w = w_q det J -> (J, J0) -> X.
+  /// Throws Failure where evaluate does.
+  void vjp_x(const double* x, const T* ue, const std::vector<State<T>>& committed, const T* alpha_n,
+             const double* lambda, double* out) {
+    ElementOut<T> eo = evaluate(x, ue, committed, alpha_n, true);
+    Vec<T, 9> a;
+    for (int i = 0; i < 9; ++i) a[i] = eo.alpha[i];
+    kinematics_at(a);
+    respond(committed);
+    Sums<T> sums;
+    accumulate_local(sums);
+    accumulate_coupling(false, sums);
+    // mu = -K_aa^-T K_ua^T lambda.
+    Vec<T, 9> b;
+    for (int j = 0; j < 9; ++j) {
+      T acc = T(0.0);
+      for (int i = 0; i < 24; ++i) acc += sums.kua(i, j) * T(lambda[i]);
+      b[j] = acc;
+    }
+    FullPivLU<T, 9> lut;
+    lut.compute(tr(sums.kaa));
+    const Vec<T, 9> y = lut.solve(b);
+    // Lambda (3 x 11): nodes, then modes (residual index 3 m + k).
+    double L[3][11], Uu[3][11];
+    for (int k = 0; k < 3; ++k) {
+      for (int n = 0; n < 8; ++n) {
+        L[k][n] = lambda[3 * n + k];
+        Uu[k][n] = val(ue[3 * n + k]);
+      }
+      for (int m = 0; m < 3; ++m) {
+        L[k][8 + m] = -val(y[3 * m + k]);
+        Uu[k][8 + m] = val(a[3 * m + k]);
+      }
+    }
+    for (int i = 0; i < 24; ++i) out[i] = 0.0;
+    // Reference Jacobians (set_up's).
+    auto jac_at = [&](const Mat<double, 8, 3>& dn, double J[3][3]) {
+      for (int i = 0; i < 3; ++i)
+        for (int c = 0; c < 3; ++c) {
+          double acc = 0.0;
+          for (int n = 0; n < 8; ++n) acc += x[3 * n + i] * dn(n, c);
+          J[i][c] = acc;
+        }
+    };
+    auto inv_det = [](const double J[3][3], double Ji[3][3]) {
+      const double d = J[0][0] * (J[1][1] * J[2][2] - J[2][1] * J[1][2]) -
+                       J[1][0] * (J[0][1] * J[2][2] - J[2][1] * J[0][2]) +
+                       J[2][0] * (J[0][1] * J[1][2] - J[1][1] * J[0][2]);
+      Ji[0][0] = (J[1][1] * J[2][2] - J[1][2] * J[2][1]) / d;
+      Ji[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) / d;
+      Ji[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) / d;
+      Ji[1][0] = (J[1][2] * J[2][0] - J[1][0] * J[2][2]) / d;
+      Ji[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) / d;
+      Ji[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) / d;
+      Ji[2][0] = (J[1][0] * J[2][1] - J[1][1] * J[2][0]) / d;
+      Ji[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) / d;
+      Ji[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) / d;
+      return d;
+    };
+    const Mat<double, 8, 3> dn0 = shape_gradients(0.0, 0.0, 0.0);
+    double J0[3][3], J0i[3][3];
+    jac_at(dn0, J0);
+    inv_det(J0, J0i);
+    double J0bar[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (std::size_t q = 0; q < rule_.size(); ++q) {
+      const PointWork<T>& p = points_[q];
+      const QPoint& xi = rule_[q];
+      const Mat<double, 8, 3> dn = shape_gradients(xi.xi, xi.eta, xi.zeta);
+      double J[3][3], Ji[3][3];
+      jac_at(dn, J);
+      inv_det(J, Ji);
+      const double w = val(p.weight);
+      double F[3][3], S[3][3], G[3][11];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) F[i][j] = val(p.h(i, j)) + (i == j ? 1.0 : 0.0);
+      const double s6[6] = {val(p.s[0]), val(p.s[1]), val(p.s[2]), val(p.s[3]), val(p.s[4]), val(p.s[5])};
+      S[0][0] = s6[0]; S[1][1] = s6[1]; S[2][2] = s6[2];
+      S[0][1] = S[1][0] = s6[3]; S[1][2] = S[2][1] = s6[4]; S[2][0] = S[0][2] = s6[5];
+      for (int j = 0; j < 3; ++j)
+        for (int n = 0; n < 11; ++n) G[j][n] = val(p.g(j, n));
+      // phi_q = w sum_{k,n} L_kn (F S G)_kn; Q = L G^T.
+      double FS[3][3], Q[3][3];
+      for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j) {
+          double acc = 0.0, acq = 0.0;
+          for (int i = 0; i < 3; ++i) acc += F[k][i] * S[i][j];
+          for (int n = 0; n < 11; ++n) acq += L[k][n] * G[j][n];
+          FS[k][j] = acc;
+          Q[k][j] = acq;
+        }
+      double phi = 0.0;
+      for (int k = 0; k < 3; ++k)
+        for (int n = 0; n < 11; ++n) {
+          double acc = 0.0;
+          for (int j = 0; j < 3; ++j) acc += FS[k][j] * G[j][n];
+          phi += L[k][n] * acc;
+        }
+      phi *= w;
+      // Gbar = w S F^T L (direct), Fbar = w Q S + F Ebar.
+      double Gb[3][11];
+      for (int j = 0; j < 3; ++j)
+        for (int n = 0; n < 11; ++n) {
+          double acc = 0.0;
+          for (int k = 0; k < 3; ++k) acc += FS[k][j] * L[k][n];  // (S F^T L)_jn = sum_k (F S)_kj L_kn
+          Gb[j][n] = w * acc;
+        }
+      // Sbar = w sym(F^T Q); sbar (Voigt: normal, 2 x shear) -> ebar = M^T sbar.
+      double FtQ[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          double acc = 0.0;
+          for (int k = 0; k < 3; ++k) acc += F[k][i] * Q[k][j];
+          FtQ[i][j] = w * acc;
+        }
+      const int vi[6] = {0, 1, 2, 0, 1, 2}, vj[6] = {0, 1, 2, 1, 2, 0};
+      double sb[6];
+      for (int c = 0; c < 6; ++c) {
+        const double sym = 0.5 * (FtQ[vi[c]][vj[c]] + FtQ[vj[c]][vi[c]]);
+        sb[c] = c < 3 ? sym : 2.0 * sym;
+      }
+      double eb[6];
+      for (int d = 0; d < 6; ++d) {
+        double acc = 0.0;
+        for (int c = 0; c < 6; ++c) acc += val(p.material(c, d)) * sb[c];
+        eb[d] = acc;
+      }
+      double Eb[3][3];
+      for (int c = 0; c < 6; ++c) {
+        Eb[vi[c]][vj[c]] = eb[c];
+        Eb[vj[c]][vi[c]] = eb[c];
+      }
+      double Fb[3][3];
+      for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j) {
+          double acc = 0.0, acf = 0.0;
+          for (int i = 0; i < 3; ++i) {
+            acc += Q[k][i] * S[i][j];
+            acf += F[k][i] * Eb[i][j];
+          }
+          Fb[k][j] = w * acc + acf;
+        }
+      // F = I + U G^T: Gbar += Fbar^T U.
+      for (int j = 0; j < 3; ++j)
+        for (int n = 0; n < 11; ++n) {
+          double acc = 0.0;
+          for (int i = 0; i < 3; ++i) acc += Fb[i][j] * Uu[i][n];
+          Gb[j][n] += acc;
+        }
+      // w = w_q det J: Jbar = phi J^-T.
+      double Jb[3][3];
+      for (int i = 0; i < 3; ++i)
+        for (int c = 0; c < 3; ++c) Jb[i][c] = phi * Ji[c][i];
+      // G = (dN J^-1)^T: Jbar -= J^-T K1 J^-T with K1_cj = sum_n dN_nc Gbar_jn.
+      double K1[3][3];
+      for (int c = 0; c < 3; ++c)
+        for (int j = 0; j < 3; ++j) {
+          double acc = 0.0;
+          for (int n = 0; n < 8; ++n) acc += dn(n, c) * Gb[j][n];
+          K1[c][j] = acc;
+        }
+      for (int pp = 0; pp < 3; ++pp)
+        for (int r = 0; r < 3; ++r) {
+          double acc = 0.0;
+          for (int c = 0; c < 3; ++c)
+            for (int j = 0; j < 3; ++j) acc += Ji[c][pp] * K1[c][j] * Ji[r][j];
+          Jb[pp][r] -= acc;
+        }
+      // G~_im = ratio c_m J0^-1_mi, ratio = det0 / det, c_m = -2 xi_m.
+      const double det = J[0][0] * (J[1][1] * J[2][2] - J[2][1] * J[1][2]) -
+                         J[1][0] * (J[0][1] * J[2][2] - J[2][1] * J[0][2]) +
+                         J[2][0] * (J[0][1] * J[1][2] - J[1][1] * J[0][2]);
+      const double det0 = J0[0][0] * (J0[1][1] * J0[2][2] - J0[2][1] * J0[1][2]) -
+                          J0[1][0] * (J0[0][1] * J0[2][2] - J0[2][1] * J0[0][2]) +
+                          J0[2][0] * (J0[0][1] * J0[1][2] - J0[1][1] * J0[0][2]);
+      const double ratio = det0 / det;
+      const double cm[3] = {-2.0 * xi.xi, -2.0 * xi.eta, -2.0 * xi.zeta};
+      double R = 0.0, K2[3][3];
+      for (int m = 0; m < 3; ++m)
+        for (int i = 0; i < 3; ++i) {
+          R += Gb[i][8 + m] * cm[m] * J0i[m][i];
+          K2[m][i] = cm[m] * Gb[i][8 + m];
+        }
+      for (int pp = 0; pp < 3; ++pp)
+        for (int r = 0; r < 3; ++r) {
+          J0bar[pp][r] += ratio * R * J0i[r][pp];
+          Jb[pp][r] -= ratio * R * Ji[r][pp];
+          double acc = 0.0;
+          for (int m = 0; m < 3; ++m)
+            for (int i = 0; i < 3; ++i) acc += J0i[m][pp] * K2[m][i] * J0i[r][i];
+          J0bar[pp][r] -= ratio * acc;
+        }
+      // J = X dN: Xbar_in += sum_c Jbar_ic dN_nc.
+      for (int n = 0; n < 8; ++n)
+        for (int i = 0; i < 3; ++i) {
+          double acc = 0.0;
+          for (int c = 0; c < 3; ++c) acc += Jb[i][c] * dn(n, c);
+          out[3 * n + i] += acc;
+        }
+    }
+    for (int n = 0; n < 8; ++n)
+      for (int i = 0; i < 3; ++i) {
+        double acc = 0.0;
+        for (int c = 0; c < 3; ++c) acc += J0bar[i][c] * dn0(n, c);
+        out[3 * n + i] += acc;
+      }
+  }
+
   /// incompatible_elastoplastic_element (IncompatibleModes.cpp:577-600).
   /// Throws Failure.
   ElementOut<T> evaluate(const double* x /*3x8 node-major: x[3a+i]*/, const T* ue,

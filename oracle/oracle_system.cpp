@@ -357,6 +357,32 @@ int orc_element_stress(const double* material, int in_plane, int thickness, int 
   return static_cast<int>(failed);
 }
 
+/// The vector-Jacobian product lambda . d f*/d X of a batch of IM Hex8 (24
+/// per element), at fixed displacements and committed history
+/// (IMElement::vjp_x). Returns the number of failed elements.
+int orc_vjp_x(const double* material, int in_plane, int thickness, int axis, int kinematics, long long ne,
+              const double* X, const double* ue, const double* committed, const double* alpha_n,
+              const double* lambda, double* out, int* status) {
+  Material mat;
+  if (!make_material(material, mat)) return -1;
+  const std::vector<QPoint> rule = hex8_rule(in_plane, thickness, axis);
+  const int nq = static_cast<int>(rule.size());
+  long long failed = 0;
+  for (long long e = 0; e < ne; ++e) {
+    IMElement<double> el(mat, rule, kinematics);
+    std::vector<State<double>> c(static_cast<std::size_t>(nq));
+    for (int q = 0; q < nq; ++q) c[q] = load_state<double>(committed + (e * nq + q) * kNF);
+    try {
+      el.vjp_x(X + e * 24, ue + e * 24, c, alpha_n ? alpha_n + e * 9 : nullptr, lambda + e * 24, out + e * 24);
+      status[e] = 0;
+    } catch (const Failure& f) {
+      status[e] = f.code;
+      ++failed;
+    }
+  }
+  return static_cast<int>(failed);
+}
+
 /// The algorithmic flop count of the same batch (counting scalar, one
 /// thread): +, -, *, / and each sqrt/log1p/exp/expm1 count one.
 long long orc_count_flops(const double* material, int in_plane, int thickness, int axis,
