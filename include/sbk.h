@@ -282,6 +282,19 @@ int sbk_system_stress(sbk_system* sys, const double* u_dev, double* out_dev);
 int sbk_system_stiffness_gross(sbk_system* sys, const double* u_dev, int32_t num_free, const int32_t* free_dev,
                                double* out);
 
+/* The shape derivative of the internal force (the building block of an
+ * adjoint with respect to the reference geometry): gx_dev (num_dofs, device)
+ * = lambda^T d f_int / d X at the displacement u_dev, lambda_dev (num_dofs,
+ * device) a cotangent on the DOFs, X the nodal reference coordinates, the
+ * committed points and modes the history; every element's modes follow
+ * through their local equilibrium (mu = -K_aa^-T K_ua^T lambda). frozen = 1
+ * takes the committed plastic state as it is - the elastic response from the
+ * committed plastic strain and back stresses, no return - as a release step
+ * with the end-of-forming state frozen. The incompatible-mode Hex8 under
+ * finite or logarithmic kinematics; the trial buffers of the last evaluate
+ * are overwritten. SBK_ERR_SOLVER names the lowest failing element. */
+int sbk_system_vjp_x(sbk_system* sys, const double* u_dev, const double* lambda_dev, int frozen, double* gx_dev);
+
 /* ---- contact: ToolContact ---------------------------------------------- */
 typedef struct sbk_contact sbk_contact;
 

@@ -965,6 +965,34 @@ int sbk_system_stress(sbk_system* sys, const double* u_dev, double* out_dev) {
   return SBK_OK;
 }
 
+int sbk_system_vjp_x(sbk_system* sys, const double* u_dev, const double* lambda_dev, int frozen, double* gx_dev) {
+  if (!sys || !u_dev || !lambda_dev || !gx_dev) return fail(SBK_ERR_ARGUMENT, "null argument");
+  if (sys->p.element != 0 || sys->p.kinematics == SBK_SMALL_STRAIN)
+    return fail(SBK_ERR_UNSUPPORTED, "the shape derivative is built for the incompatible-mode Hex8 under finite or "
+                                     "logarithmic kinematics");
+  cudaStream_t st = sys->stream;
+  Params p = sys->p;
+  if (frozen) p.enabled = 0;  // the committed plastic state, no return
+  SBK_CUDA(cudaMemsetAsync(sys->first_fail, 0x7f, sizeof(int32_t), st));
+  sys->has_trial = false;  // the trial buffers are overwritten
+  int rc = sbk::launch_vjp(p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c, lambda_dev,
+                           sys->trial, sys->yield, sys->code, sys->first_fail, sys->force, st);
+  if (rc) return rc;
+  int32_t first = 0;
+  SBK_CUDA(cudaMemcpyAsync(&first, sys->first_fail, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+  SBK_CUDA(cudaStreamSynchronize(st));
+  if (first != 0x7f7f7f7f) {
+    int32_t code = 0;
+    SBK_CUDA(cudaMemcpy(&code, sys->code + first, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    return fail(SBK_ERR_SOLVER, "element " + std::to_string(first) + " failed in the shape derivative (code " +
+                                    std::to_string(code) + ")");
+  }
+  rc = sbk::launch_assemble_forces(sys->maps(), sys->force, sys->energy_e, sys->yield, sys->p.nq, gx_dev, sys->scratch,
+                                   sys->scalars, st);
+  if (rc) return fail(SBK_ERR_CUDA, "shape derivative gather");
+  return SBK_OK;
+}
+
 int sbk_system_stiffness_gross(sbk_system* sys, const double* u_dev, int32_t num_free, const int32_t* free_dev,
                                double* out) {
   if (!sys || !u_dev || !out || num_free < 0 || (num_free > 0 && !free_dev))

@@ -652,6 +652,52 @@ __device__ __noinline__ void fullpiv_solve9(const double* lu, const int* rowp, c
   for (int i = 0; i < 9; ++i) x[i] = y[i];
 }
 
+// x = A^-T b with the FullPivLU factors of A (P A Q = L U, so
+// A^-T = P^T L^-T U^-T Q^T): the column transpositions in order, U^T
+// forward, L^T backward (unit diagonal), the row transpositions in reverse.
+__device__ __noinline__ void fullpiv_solve9_t(const double* lu, const int* rowp, const int* colp, const double* b,
+                                                 double* x) {
+  double y[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) y[i] = b[i];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const int pk = colp[k];
+#pragma unroll
+    for (int i = k + 1; i < 9; ++i) {
+      if (i == pk) {
+        const double t = y[k];
+        y[k] = y[i];
+        y[i] = t;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+#pragma unroll
+    for (int j = 0; j < i; ++j) y[i] -= lu[j * 9 + i] * y[j];
+    y[i] /= lu[i * 9 + i];
+  }
+#pragma unroll
+  for (int i = 8; i >= 0; --i)
+#pragma unroll
+    for (int j = i + 1; j < 9; ++j) y[i] -= lu[j * 9 + i] * y[j];
+#pragma unroll
+  for (int k = 8; k >= 0; --k) {
+    const int pk = rowp[k];
+#pragma unroll
+    for (int i = k + 1; i < 9; ++i) {
+      if (i == pk) {
+        const double t = y[k];
+        y[k] = y[i];
+        y[i] = t;
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < 9; ++i) x[i] = y[i];
+}
+
 // Cholesky (lower, in place); false at the first non-positive pivot.
 __device__ __noinline__ bool llt9(double* a) {
   _Pragma("unroll 1") for (int k = 0; k < 9; ++k) {
@@ -1246,6 +1292,277 @@ __global__ void __launch_bounds__(256) element_kernel(const __grid_constant__ Pa
     code[e] = 0;
   }
   for (int i = lane; i < 9; i += G) alpha_out[e * 9 + i] = s.alpha[i];
+}
+
+// ---- the shape derivative: lambda . d f* / d X ---------------------------------
+//
+// For the condensed residual f*(u, X) of an IM Hex8 at fixed displacements
+// and committed history, with the modes at their local equilibrium
+// r_a(u, alpha, X) = 0: lambda^T d f*/dX = [lambda; mu]^T d r/dX |_alpha with
+// mu = -K_aa^-T K_ua^T lambda, and r = sum_q w F S [G | G~] (nodes and
+// modes). Per point the reverse chain runs r -> (w, F, S, [G | G~]);
+// S -> E through the point's material tangent dS/dE; E -> F; F = I + U
+// [G | G~]^T -> [G | G~]; G = dN J^-1, G~ = (det0/det)(-2 xi) J0^-1 and
+// w = w_q det J -> (J, J0) -> X.
+
+// One point's share: xb (24, node-major) and j0b (9, row-major) accumulate.
+template <int G>
+__device__ __noinline__ void vjp_point(const Ctx<G>& c, int q, const double* lam, const double* mu, double xb[24],
+                                       double j0b[9]) {
+  const ElemShared<G>& s = *c.s;
+  const double* sl = s.slot[q];
+  const double* Fp = sl + kSlotF;
+  const double* Sv = sl + kSlotS;
+  const double w = sl[kSlotW];
+  const double* Ji = s.geo[q];  // J^-1, row-major
+  const double ratio = s.geo[q][10];
+  double S[9] = {Sv[0], Sv[3], Sv[5], Sv[3], Sv[1], Sv[4], Sv[5], Sv[4], Sv[2]};
+  // Q = Lambda Ghat^T (3 x 3), FS = F S, phi = w sum Lambda . (F S Ghat).
+  double Q[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  double dn[8][3];
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    shape_grad(a, c.p->qp[q][0], c.p->qp[q][1], c.p->qp[q][2], dn[a]);
+    double g[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) g[i] = dn[a][0] * Ji[i] + dn[a][1] * Ji[3 + i] + dn[a][2] * Ji[6 + i];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Q[k * 3 + j] += lam[3 * a + k] * g[j];
+  }
+  double gt[9];  // G~(i, m) at gt[i * 3 + m]
+  mode_grads(c, q, gt);
+#pragma unroll
+  for (int m = 0; m < 3; ++m)
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) Q[k * 3 + j] += mu[3 * m + k] * gt[j * 3 + m];
+  double FS[9];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) FS[k * 3 + j] = Fp[k * 3 + 0] * S[j] + Fp[k * 3 + 1] * S[3 + j] + Fp[k * 3 + 2] * S[6 + j];
+  double phi = 0.0;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) phi += FS[i] * Q[i];
+  phi *= w;
+  // Sbar = w sym(F^T Q) -> sbar (normal, 2 x shear) -> ebar = M^T sbar -> Ebar.
+  double FtQ[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      FtQ[i * 3 + j] = w * (Fp[0 * 3 + i] * Q[0 * 3 + j] + Fp[1 * 3 + i] * Q[1 * 3 + j] + Fp[2 * 3 + i] * Q[2 * 3 + j]);
+  const int vi[6] = {0, 1, 2, 0, 1, 2}, vj[6] = {0, 1, 2, 1, 2, 0};
+  double sb[6];
+#pragma unroll
+  for (int cc = 0; cc < 6; ++cc) {
+    const double sym = 0.5 * (FtQ[vi[cc] * 3 + vj[cc]] + FtQ[vj[cc] * 3 + vi[cc]]);
+    sb[cc] = cc < 3 ? sym : 2.0 * sym;
+  }
+  double Eb[9];
+#pragma unroll
+  for (int d = 0; d < 6; ++d) {
+    double acc = 0.0;
+#pragma unroll
+    for (int cc = 0; cc < 6; ++cc) acc += sl[cc * 6 + d] * sb[cc];
+    Eb[vi[d] * 3 + vj[d]] = acc;
+    Eb[vj[d] * 3 + vi[d]] = acc;
+  }
+  // Fbar = w Q S + F Ebar.
+  double Fb[9];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      Fb[k * 3 + j] = w * (Q[k * 3 + 0] * S[j] + Q[k * 3 + 1] * S[3 + j] + Q[k * 3 + 2] * S[6 + j]) +
+                      Fp[k * 3 + 0] * Eb[j] + Fp[k * 3 + 1] * Eb[3 + j] + Fp[k * 3 + 2] * Eb[6 + j];
+  // Gbar = w (F S)^T Lambda + Fbar^T U, node by node; K1 = sum_a dN_a Gbar_a^T.
+  double K1[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int a = 0; a < 8; ++a) {
+    double gb[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+      gb[j] = w * (FS[0 * 3 + j] * lam[3 * a + 0] + FS[1 * 3 + j] * lam[3 * a + 1] + FS[2 * 3 + j] * lam[3 * a + 2]) +
+              Fb[0 * 3 + j] * s.U[3 * a + 0] + Fb[1 * 3 + j] * s.U[3 * a + 1] + Fb[2 * 3 + j] * s.U[3 * a + 2];
+#pragma unroll
+    for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+      for (int j = 0; j < 3; ++j) K1[cc * 3 + j] += dn[a][cc] * gb[j];
+  }
+  // Modes: Gbar~ (3 x 3), R and K2.
+  double R = 0.0, K2[9];
+  const double cm[3] = {-2.0 * c.p->qp[q][0], -2.0 * c.p->qp[q][1], -2.0 * c.p->qp[q][2]};
+#pragma unroll
+  for (int m = 0; m < 3; ++m)
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const double gbm = w * (FS[0 * 3 + i] * mu[3 * m + 0] + FS[1 * 3 + i] * mu[3 * m + 1] + FS[2 * 3 + i] * mu[3 * m + 2]) +
+                         Fb[0 * 3 + i] * s.alpha[3 * m + 0] + Fb[1 * 3 + i] * s.alpha[3 * m + 1] +
+                         Fb[2 * 3 + i] * s.alpha[3 * m + 2];
+      R += gbm * cm[m] * s.jinv0[m * 3 + i];
+      K2[m * 3 + i] = cm[m] * gbm;
+    }
+  // Jbar = (phi - ratio R) J^-T - J^-T K1 J^-T; J0bar += ratio R J0^-T - ratio J0^-T K2 J0^-T.
+  const double* J0i = s.jinv0;
+  double Jb[9];
+#pragma unroll
+  for (int pp = 0; pp < 3; ++pp)
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+      double a1 = 0.0, a2 = 0.0;
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          a1 += Ji[cc * 3 + pp] * K1[cc * 3 + j] * Ji[r * 3 + j];
+          a2 += J0i[cc * 3 + pp] * K2[cc * 3 + j] * J0i[r * 3 + j];
+        }
+      Jb[pp * 3 + r] = (phi - ratio * R) * Ji[r * 3 + pp] - a1;
+      j0b[pp * 3 + r] += ratio * R * J0i[r * 3 + pp] - ratio * a2;
+    }
+  // J = X dN: Xbar_ia += sum_c Jbar_ic dN_ac.
+#pragma unroll
+  for (int a = 0; a < 8; ++a)
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      xb[3 * a + i] += Jb[i * 3 + 0] * dn[a][0] + Jb[i * 3 + 1] * dn[a][1] + Jb[i * 3 + 2] * dn[a][2];
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) vjp_kernel(const __grid_constant__ Params p, int64_t ne,
+                                                  const double* __restrict__ coords, const int32_t* __restrict__ conn,
+                                                  const double* __restrict__ u, const double* __restrict__ state,
+                                                  const double* __restrict__ alpha_n,
+                                                  const double* __restrict__ lambda, double* __restrict__ trial,
+                                                  uint8_t* __restrict__ yield, int32_t* __restrict__ code,
+                                                  int32_t* __restrict__ first_failure, double* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int epb = blockDim.x / G;
+  const int slot_in_block = threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  const int64_t e = (int64_t)blockIdx.x * epb + slot_in_block;
+  ElemShared<G>* sh = reinterpret_cast<ElemShared<G>*>(smem_raw) + slot_in_block;
+  const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+  const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
+  if (e >= ne) return;
+  double hu_lane[9];
+  double warm_lane[8];
+  warm_lane[7] = 0.0;
+  Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, trial, yield, hu_lane, warm_lane};
+  ElemShared<G>& s = *sh;
+  int bad_node = 0;
+  double lam_a[3] = {0.0, 0.0, 0.0};
+  if (lane < 8) {
+    const int64_t node = conn[e * 8 + lane];
+    if (p.num_nodes > 0 && (node < 0 || node >= p.num_nodes)) {
+      bad_node = 1;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        s.X[3 * lane + k] = coords[node * 3 + k];
+        s.U[3 * lane + k] = u[node * 3 + k];
+        lam_a[k] = lambda[node * 3 + k];
+      }
+    }
+  }
+  if (__any_sync(mask, bad_node)) {
+    if (lane == 0) {
+      code[e] = SBK_EL_BAD_NODE;
+      atomicMin(first_failure, (int32_t)e);
+    }
+    return;
+  }
+  for (int i = lane; i < 9; i += G) s.alpha[i] = alpha_n ? alpha_n[e * 9 + i] : 0.0;
+  c.sync();
+  int status = set_up<G>(c);
+  Local<G> loc(c);
+  if (!status) status = loc.run();
+  if (status) {
+    if (lane == 0) {
+      code[e] = status;
+      atomicMin(first_failure, (int32_t)e);
+    }
+    return;
+  }
+  const bool geometric = p.kinematics != SBK_SMALL_STRAIN;
+  // K_ua^T lambda, node by node (lane a), summed in node order by lane 0.
+  double* part = s.work;  // 8 x 9 partial sums, then lambda (24) and mu (9)
+  if (lane < 8) {
+    const int a = lane;
+    double kua[3][9];
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int j = 0; j < 9; ++j) kua[k][j] = 0.0;
+    for (int q = 0; q < p.nq; ++q) {
+      double g[3], gt[9], V[27];
+      node_grad(c, q, a, g);
+      mode_grads(c, q, gt);
+      vtensor(s.slot[q], g, false, geometric, V);
+#pragma unroll
+      for (int m = 0; m < 3; ++m)
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int l = 0; l < 3; ++l)
+            kua[k][3 * m + l] += V[(k * 3 + l) * 3 + 0] * gt[0 * 3 + m] + V[(k * 3 + l) * 3 + 1] * gt[1 * 3 + m] +
+                                 V[(k * 3 + l) * 3 + 2] * gt[2 * 3 + m];
+    }
+#pragma unroll
+    for (int j = 0; j < 9; ++j)
+      part[a * 9 + j] = kua[0][j] * lam_a[0] + kua[1][j] * lam_a[1] + kua[2][j] * lam_a[2];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) part[72 + 3 * a + k] = lam_a[k];
+  }
+  c.sync();
+  if (lane == 0) {
+    double b[9], y[9];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      double acc = 0.0;
+      for (int a = 0; a < 8; ++a) acc += part[a * 9 + j];
+      b[j] = acc;
+    }
+    fullpiv_solve9_t(s.lu, s.rowp, s.colp, b, y);
+#pragma unroll
+    for (int j = 0; j < 9; ++j) part[96 + j] = -y[j];
+  }
+  c.sync();
+  // Every point's share, then the sums over the points (reduce-scatter of
+  // 33 values: 24 of Xbar, 9 of J0bar), and J0 = X dN(0) folded in.
+  double xb[24], j0b[9];
+#pragma unroll
+  for (int i = 0; i < 24; ++i) xb[i] = 0.0;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) j0b[i] = 0.0;
+  if (lane < p.nq) vjp_point<G>(c, lane, part + 72, part + 96, xb, j0b);
+  double* red = s.kc;  // 33 sums
+#pragma unroll
+  for (int chunk = 0; chunk * G < 33; ++chunk) {
+    double buf[G];
+#pragma unroll
+    for (int i = 0; i < G; ++i) {
+      const int idx = chunk * G + i;
+      buf[i] = idx < 24 ? xb[idx < 24 ? idx : 0] : (idx < 33 ? j0b[idx - 24 < 9 && idx >= 24 ? idx - 24 : 0] : 0.0);
+    }
+    const double v = reduce_scatter<G>(buf, lane, mask);
+    if (chunk * G + lane < 33) red[chunk * G + lane] = v;
+  }
+  c.sync();
+  if (lane < 8) {
+    const int a = lane;
+    double dn0[3];
+    shape_grad(a, 0.0, 0.0, 0.0, dn0);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      out[e * 24 + 3 * a + i] = red[3 * a + i] + red[24 + i * 3 + 0] * dn0[0] + red[24 + i * 3 + 1] * dn0[1] +
+                                red[24 + i * 3 + 2] * dn0[2];
+  }
+  if (lane == 0) code[e] = 0;
 }
 
 // ---- the standard Hex8 -------------------------------------------------------
@@ -1974,6 +2291,34 @@ int launch_standard_g(const Params& p, int64_t ne, const double* coords, const i
   err = cudaGetLastError();
   if (err != cudaSuccess) return set_error(SBK_ERR_CUDA, std::string("standard kernel launch: ") + cudaGetErrorString(err));
   return 0;
+}
+
+template <int G>
+int launch_vjp_g(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
+                 const double* state, const double* alpha_n, const double* lambda, double* trial, uint8_t* yield,
+                 int32_t* code, int32_t* first_failure, double* out, cudaStream_t stream) {
+  const int epb = G == 8 ? 16 : 4;
+  const size_t smem = sizeof(ElemShared<G>) * epb;
+  const int64_t blocks = (ne + epb - 1) / epb;
+  if (blocks == 0) return 0;
+  auto kern = vjp_kernel<G>;
+  cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (err != cudaSuccess) return set_error(SBK_ERR_CUDA, std::string("vjp kernel attribute: ") + cudaGetErrorString(err));
+  kern<<<(unsigned)blocks, epb * G, smem, stream>>>(p, ne, coords, conn, u, state, alpha_n, lambda, trial, yield, code,
+                                                    first_failure, out);
+  err = cudaGetLastError();
+  if (err != cudaSuccess) return set_error(SBK_ERR_CUDA, std::string("vjp kernel launch: ") + cudaGetErrorString(err));
+  return 0;
+}
+
+int launch_vjp(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
+               const double* state, const double* alpha_n, const double* lambda, double* trial, uint8_t* yield,
+               int32_t* code, int32_t* first_failure, double* out, cudaStream_t stream) {
+  if (p.nq <= 8)
+    return launch_vjp_g<8>(p, ne, coords, conn, u, state, alpha_n, lambda, trial, yield, code, first_failure, out,
+                           stream);
+  return launch_vjp_g<32>(p, ne, coords, conn, u, state, alpha_n, lambda, trial, yield, code, first_failure, out,
+                          stream);
 }
 
 size_t element_smem_bytes(int group) {

@@ -26,6 +26,14 @@ int launch_elements(const Params& p, int64_t ne, const double* coords, const int
                     int32_t* code, int32_t* first_failure, bool batch, int elements_per_block,
                     const int32_t* order, cudaStream_t stream);
 size_t element_smem_bytes(int group);
+// The shape derivative: per element lambda . d f*/d X (24, node-major) into
+// out, at u with the committed points (state) and modes (alpha_n) as the
+// history and lambda a global DOF vector; the local iteration runs again to
+// the modes' equilibrium (its trial state and yield flags into trial and
+// yield). Mesh mode only.
+int launch_vjp(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
+               const double* state, const double* alpha_n, const double* lambda, double* trial, uint8_t* yield,
+               int32_t* code, int32_t* first_failure, double* out, cudaStream_t stream);
 // Stress recovery of ne mesh elements at u from the committed points and
 // modes: 28 doubles per element into out (see stress_kernel); the returns
 // write their (reproduced) states into scratch (the state layout).

@@ -385,6 +385,20 @@ class NonlinearSystem:
         _capi.check(st)
         return ElementStresses.from_packed(out)
 
+    def vjp_x(self, u: torch.Tensor, lam: torch.Tensor, frozen: bool = True) -> torch.Tensor:
+        """lambda^T d f_int / d X (num_dofs) at u: the shape derivative of the
+        internal force with respect to the nodal reference coordinates, the
+        modes through their local equilibrium, the committed history as the
+        history (frozen: its plastic state taken as it is, no return). The
+        trial state of the last evaluate is overwritten."""
+        out = torch.empty(self.num_dofs, dtype=torch.float64, device="cuda")
+        st = _capi.lib().sbk_system_vjp_x(self._h, _ptr(u.contiguous()), _ptr(lam.contiguous()), int(bool(frozen)),
+                                          _ptr(out))
+        if st == 4:
+            raise _capi.SolverError(st, _capi.last_error())
+        _capi.check(st)
+        return out
+
     def stiffness_gross(self, u: torch.Tensor, free: torch.Tensor) -> float:
         """stiffness_gross (src/fem/NonlinearSystem.hpp:49-67): the norm over
         the DOFs in `free` of |K| |u|, K the tangent of the last evaluate (with
