@@ -450,6 +450,10 @@ int sbk_partition_set_dense_limit(sbk_partition* part, int32_t max_rows);
  * (num_free each, device, free numbering). SBK_ERR_SOLVER when the block is
  * singular (the QR's or LU's pivot below 1e-13 of the largest entry). */
 int sbk_partition_solve(sbk_partition* part, const double* b_dev, double* x_dev);
+/* x_dev = K_ff^-T b_dev with the same factorisation - the adjoint system of
+ * a partition. A Cholesky (symmetric) or a dense LU factorisation;
+ * SBK_ERR_UNSUPPORTED for the GMRES and QR solves. */
+int sbk_partition_solve_transpose(sbk_partition* part, const double* b_dev, double* x_dev);
 /* names() and failures() (Forming.cpp:174-181) as counts, since the
  * partition was made: factorisations solved by Cholesky, by preconditioned
  * GMRES, by dense LU, by QR; Choleskys and GMRES runs that fell back;

@@ -147,6 +147,7 @@ SIGNATURES = {
     "sbk_partition_add_to": (_I, [_P, _P, _P, _D]),
     "sbk_partition_factorize": (_I, [_P, _P, _I, ctypes.POINTER(_I)]),
     "sbk_partition_solve": (_I, [_P, _P, _P]),
+    "sbk_partition_solve_transpose": (_I, [_P, _P, _P]),
     "sbk_partition_counts": (_I, [_P, ctypes.POINTER(_I64 * 9)]),
     "sbk_partition_set_dense_limit": (_I, [_P, _I32]),
     "sbk_last_error": (ctypes.c_char_p, []),

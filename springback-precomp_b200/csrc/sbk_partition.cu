@@ -568,9 +568,10 @@ int dense_factor(sbk_partition* P, bool* singular) {
   return SBK_OK;
 }
 
-int dense_solve(sbk_partition* P) {
+int dense_solve(sbk_partition* P, bool transpose = false) {
   PCUDA(cudaMemcpyAsync(P->sol, P->rhs, sizeof(double) * (size_t)P->nf, cudaMemcpyDeviceToDevice, P->stream));
-  PSOLVER(cusolverDnDgetrs(P->dense, CUBLAS_OP_N, P->nf, 1, P->lu, P->nf, P->ipiv, P->sol, P->nf, P->lu_info));
+  PSOLVER(cusolverDnDgetrs(P->dense, transpose ? CUBLAS_OP_T : CUBLAS_OP_N, P->nf, 1, P->lu, P->nf, P->ipiv, P->sol,
+                           P->nf, P->lu_info));
   return SBK_OK;
 }
 
@@ -799,6 +800,23 @@ int sbk_partition_solve(sbk_partition* part, const double* b_dev, double* x_dev)
   } else if (P->kind == SBK_FACTOR_QR) {
     if (int rc = solve_qr(P)) return rc;
   }
+  scatter_kernel<<<grid_for(P->nf), kThreads, 0, P->stream>>>(P->sol, P->perm, P->nf, 0.0, false, x_dev);
+  PCUDA(cudaGetLastError());
+  return SBK_OK;
+}
+
+int sbk_partition_solve_transpose(sbk_partition* part, const double* b_dev, double* x_dev) {
+  if (!part || !b_dev || !x_dev) return pfail(SBK_ERR_ARGUMENT, "sbk_partition_solve_transpose: null argument");
+  sbk_partition* P = part;
+  if (P->kind == 0) return pfail(SBK_ERR_ARGUMENT, "the free-free block was solved before it was factorised");
+  if (P->kind == SBK_FACTOR_CHOLESKY) return sbk_partition_solve(part, b_dev, x_dev);  // symmetric
+  if (P->kind != SBK_FACTOR_LU)
+    return pfail(SBK_ERR_UNSUPPORTED, "the transposed solve takes a Cholesky or a dense LU factorisation");
+  // K^T x = b with B = K(p, p): B^T (x(p)) = b(p), the permutations as solve's.
+  ++P->counts[kSolves];
+  gather_kernel<<<grid_for(P->nf), kThreads, 0, P->stream>>>(b_dev, P->perm, P->nf, P->rhs);
+  PCUDA(cudaGetLastError());
+  if (int rc = dense_solve(P, true)) return rc;
   scatter_kernel<<<grid_for(P->nf), kThreads, 0, P->stream>>>(P->sol, P->perm, P->nf, 0.0, false, x_dev);
   PCUDA(cudaGetLastError());
   return SBK_OK;

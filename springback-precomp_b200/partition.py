@@ -121,12 +121,14 @@ class PartitionedFactor:
         self.kind = int(kind.value)
         return self.kind
 
-    def solve(self, b: torch.Tensor, out: Optional[torch.Tensor] = None) -> torch.Tensor:
-        """x = K_ff^-1 b on the free DOFs; SolverError when the block is
-        singular (a rigid-body motion or a mechanism left free)."""
+    def solve(self, b: torch.Tensor, out: Optional[torch.Tensor] = None, transpose: bool = False) -> torch.Tensor:
+        """x = K_ff^-1 b on the free DOFs (transpose: K_ff^-T b, the adjoint
+        system; Cholesky or dense LU); SolverError when the block is singular
+        (a rigid-body motion or a mechanism left free)."""
         if out is None:
             out = torch.empty(self.num_free, dtype=torch.float64, device="cuda")
-        st = _capi.lib().sbk_partition_solve(self._h, _ptr(b.contiguous()), _ptr(out))
+        fn = _capi.lib().sbk_partition_solve_transpose if transpose else _capi.lib().sbk_partition_solve
+        st = fn(self._h, _ptr(b.contiguous()), _ptr(out))
         if st == 4:
             raise SolverError(st, _capi.last_error())
         if st != 0:

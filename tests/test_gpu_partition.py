@@ -190,3 +190,38 @@ def test_bad_partitions_are_refused(pkg, elastic):
         pkg.PartitionedFactor.for_system(s, free[::-1].copy())
     with pytest.raises(pkg.SbkError):
         pkg.PartitionedFactor.for_system(s, np.array([0, s.num_dofs], dtype=np.int32))
+
+
+@pytest.mark.parametrize("skew", [0.0, 1e-3])
+def test_transposed_solve(pkg, plastic, cuda, skew):
+    """K_ff^-T b with the factorisation K_ff^-1 b uses (the adjoint system):
+    the Cholesky of a symmetric block solves it as it stands; the dense LU of
+    a non-symmetric block solves with its transpose, against a dense solve."""
+    s, values = plastic
+    rng = np.random.default_rng(12)
+    free = np.flatnonzero(rng.random(s.num_dofs) < 0.8).astype(np.int32)
+    v = values.cpu().numpy() * (1.0 + skew * rng.standard_normal(s.nnz))
+    part = pkg.PartitionedFactor.for_system(s, free)
+    kind = part.factorize(torch.tensor(v, device=cuda), symmetric=skew == 0.0 and s.symmetric())
+    b = rng.standard_normal(len(free))
+    x = part.solve(torch.tensor(b, device=cuda), transpose=True).cpu().numpy()
+    ref = np.linalg.solve(dense_block(s, v, free).T, b)
+    assert np.linalg.norm(x - ref) <= SOLVE_TOL * np.linalg.norm(ref)
+    if skew:
+        assert kind == 4
+        fwd = np.linalg.solve(dense_block(s, v, free), b)
+        assert np.linalg.norm(fwd - ref) > 1e3 * SOLVE_TOL * np.linalg.norm(ref)
+
+
+def test_transposed_solve_is_refused_by_gmres(pkg, plastic, cuda):
+    """GMRES keeps no factorisation of the block to transpose."""
+    s, values = plastic
+    rng = np.random.default_rng(13)
+    free = np.flatnonzero(rng.random(s.num_dofs) < 0.8).astype(np.int32)
+    v = values.cpu().numpy() * (1.0 + 1e-3 * rng.standard_normal(s.nnz))
+    part = pkg.PartitionedFactor.for_system(s, free)
+    part.set_dense_limit(0)
+    if part.factorize(torch.tensor(v, device=cuda), symmetric=False) != 3:
+        pytest.skip("the block left GMRES")
+    with pytest.raises(pkg.SbkError):
+        part.solve(torch.ones(len(free), dtype=torch.float64, device=cuda), transpose=True)
