@@ -20,6 +20,13 @@ data path; weak scaling); the time is the max over ranks.
 (PartitionedFactor): its gather from the full tangent, and the device
 factorisation and solve it feeds.
 
+--workload adjoint measures the adjoint springback sensitivity: a sheet part
+with a frozen end-of-forming history released onto 3-2-1 supports, the
+gradient of the RMS springback of its top face with respect to a 20 x 20
+bicubic grid of commanded heights (torch.autograd through the release
+solve), its cost against one release solve, and its agreement with central
+differences (h = 1e-6 mm) along seeded random directions.
+
 --impl reference times the reference's CPU algorithm - the oracle's
 restatement of it (the reference needs Eigen, which this image lacks) - on
 all host cores, on a bounded sample of the same workload per step.
@@ -319,6 +326,114 @@ def sheet_partition(pkg, torch, nx, ny, dev):
     return sysm, ev.tangent.clone(), np.flatnonzero(~held).astype(np.int32)
 
 
+def run_adjoint(args, rank, world):
+    """The adjoint springback sensitivity on one GPU: the frozen release of
+    an adj_nx x adj_ny x 2 IM Hex8 sheet part carrying the committed history
+    of the microbenchmark's loading (Hill48 + Chaboche), J = the RMS vertical
+    deviation of its top face from the formed heights, p = the 20 x 20
+    bicubic grid of height offsets over the footprint. One step = one
+    gradient dJ/dp: the release solve (forward) and the adjoint (backward:
+    points re-evaluated at u*, one factorisation, one transposed solve, the
+    shape-derivative kernel). Reported: the gradient's cost over one release
+    solve, and central differences of J along `directions` seeded random
+    directions of p."""
+    import torch
+
+    if world > 1 and rank != 0:
+        return 0
+    pkg = importlib.import_module(PKG)
+    wl = importlib.import_module(PKG + ".workload")
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    nx, ny = args.adj_nx, args.adj_ny
+    prob = wl.make_problem(nx, ny, 2, seed=5, sample=min(4096, nx * ny * 2))
+    mesh = prob.mesh
+    x0 = torch.tensor(mesh.coords, device=dev)
+    lo, hi = mesh.coords.min(axis=0), mesh.coords.max(axis=0)
+    grid = pkg.BicubicHeights(lo[0], hi[0], lo[1], hi[1], n=20)
+    stencil = grid.stencil(mesh.coords[:, :2], device=dev)
+    top = torch.tensor(np.flatnonzero(np.isclose(mesh.coords[:, 2], hi[2])), device=dev)
+    u_formed = torch.tensor(prob.u, device=dev)
+    target = x0[top, 2] + u_formed.reshape(-1, 3)[top, 2]
+    release = pkg.Release(mesh, prob.material, prob.state, prob.alpha, pkg.supports_321(mesh))
+
+    def coords_of(p):
+        lift = torch.zeros_like(x0)
+        lift[:, 2] = grid.heights(p, stencil)
+        return x0 + lift
+
+    def gradient():
+        p = torch.zeros((20, 20), dtype=torch.float64, device=dev, requires_grad=True)
+        c = coords_of(p)
+        u = pkg.released(c, release, u_formed)
+        j = pkg.springback_rms(c, u, top, target)
+        j.backward()
+        return float(j.detach()), p.grad.detach(), u.detach()
+
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), out
+
+    for _ in range(args.warmup):
+        j, grad, u_star = gradient()
+    # The backward alone: the adjoint at the released state, dJ/du of the RMS.
+    c0 = coords_of(torch.zeros((20, 20), dtype=torch.float64, device=dev))
+    dj = torch.zeros_like(u_star)
+    dj.reshape(-1, 3)[top, 2] = (u_star.reshape(-1, 3)[top, 2] + c0[top, 2] - target) / (len(top) * j)
+    lam = torch.tensor(np.random.default_rng(4).standard_normal(mesh.num_dofs), device=dev)
+    release_ms, grad_ms, adjoint_ms, vjp_ms = [], [], [], []
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            release_ms.append(timed(lambda: release.solve(x0, u_formed))[0])
+            iterations = release.iterations
+            grad_ms.append(timed(gradient)[0])
+            adjoint_ms.append(timed(lambda: release.adjoint(c0, u_star, dj))[0])
+            vjp_ms.append(timed(lambda: release.system.vjp_x(u_star, lam, frozen=True))[0])
+    rel_ms, g_ms, a_ms = statistics.median(release_ms), statistics.median(grad_ms), statistics.median(adjoint_ms)
+    g = grad.cpu().numpy()
+    h = 1e-9
+    rng = np.random.default_rng(32)
+    errors = []
+    t0 = time.perf_counter()
+    for _ in range(args.directions):
+        d = rng.uniform(-1.0, 1.0, size=(20, 20))
+        jd = []
+        for sign in (1.0, -1.0):
+            c = coords_of(torch.tensor(sign * h * d, device=dev))
+            jd.append(float(pkg.springback_rms(c, release.solve(c, u_star), top, target)))
+        fd = (jd[0] - jd[1]) / (2.0 * h)
+        errors.append(abs(float((g * d).sum()) - fd) / abs(fd))
+    fd_s = time.perf_counter() - t0
+    line = {"metric": "adjoint springback gradient (400 commanded heights): cost relative to one release solve",
+            "value": g_ms / rel_ms, "unit": "x", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": g_ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"frozen release of a {nx}x{ny}x2 IM Hex8 sheet part ({mesh.num_elements} "
+                                   f"elements, {len(release.free)} free DOFs) carrying the microbenchmark's "
+                                   "committed Hill48 + Chaboche history, 3-2-1 supports; J = RMS springback of "
+                                   "the top face; p = 20x20 bicubic height grid; one step = dJ/dp by "
+                                   "torch.autograd (release solve + adjoint)"},
+            "release_solve_ms": rel_ms, "newton_iterations": iterations, "gradient_ms": g_ms,
+            "adjoint_ms": a_ms, "adjoint_over_release": a_ms / rel_ms, "springback_rms_m": j,
+            "per_step_ms": {"release": release_ms, "gradient": grad_ms, "adjoint": adjoint_ms, "vjp_x": vjp_ms},
+            "vjp_x_elements_per_s": mesh.num_elements / (statistics.median(vjp_ms) / 1e3),
+            "central_differences": {"directions": args.directions, "h_mm": 1e-6,
+                                    "max_relative_difference": max(errors) if errors else None,
+                                    "median_relative_difference": statistics.median(errors) if errors else None,
+                                    "seconds": fd_s},
+            "factor_kind": release.part.kind, "clocks": clocks.summary()}
+    print(json.dumps(line))
+    release.close()
+    return 0
+
+
 def run_partition(args, rank, world):
     """The free-free block of a Dirichlet partition (PartitionedFactor,
     Forming.cpp:59-241): one step = the gather of the block's values from
@@ -462,15 +577,20 @@ def main():
     p.add_argument("--epb", type=int, default=0, help="elements per block of the element kernel (0: default)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="microbench", choices=["microbench", "batched", "partition"],
+    p.add_argument("--workload", default="microbench", choices=["microbench", "batched", "partition", "adjoint"],
                    help="batched: the design-sweep batch (64 parts of 20k-150k elements) in one launch against the "
                         "same parts evaluated one at a time; partition: the free-free block of a Dirichlet "
-                        "partition gathered from the full tangent, and the factorisation it feeds")
+                        "partition gathered from the full tangent, and the factorisation it feeds; adjoint: the "
+                        "springback gradient with respect to 400 commanded heights against one release solve and "
+                        "central differences")
     p.add_argument("--element", default="incompatible_modes", choices=["incompatible_modes", "standard"],
                    help="standard: the standard Hex8 with mean dilatation on the same sheet and history")
     p.add_argument("--part-nx", type=int, default=200)
     p.add_argument("--part-ny", type=int, default=200)
     p.add_argument("--parts", type=int, default=64)
+    p.add_argument("--adj-nx", type=int, default=100)
+    p.add_argument("--adj-ny", type=int, default=100)
+    p.add_argument("--directions", type=int, default=32)
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -482,6 +602,8 @@ def main():
         return run_batched(args, rank, world)
     if args.workload == "partition":
         return run_partition(args, rank, world)
+    if args.workload == "adjoint":
+        return run_adjoint(args, rank, world)
 
     import torch
 

@@ -295,6 +295,22 @@ int sbk_system_stiffness_gross(sbk_system* sys, const double* u_dev, int32_t num
  * are overwritten. SBK_ERR_SOLVER names the lowest failing element. */
 int sbk_system_vjp_x(sbk_system* sys, const double* u_dev, const double* lambda_dev, int frozen, double* gx_dev);
 
+/* Freeze the committed plastic state (frozen = 1): the evaluations, stress
+ * recoveries and shape derivatives that follow take the committed plastic
+ * strain and back stresses as they are and return no point - the release
+ * step of the adjoint with the end-of-forming state frozen. The tangent is
+ * then the elastic one and symmetric (sbk_system_symmetric says so); frozen =
+ * 0 restores the material's own response. No counterpart in the reference,
+ * whose release step always runs the returns. */
+int sbk_system_set_frozen(sbk_system* sys, int frozen);
+
+/* Replace the nodal reference coordinates (num_nodes x 3, device, row-major)
+ * by a device-to-device copy on the system's stream; the connectivity,
+ * pattern and history stay. The reference builds a new NonlinearSystem for a
+ * new mesh; a shape optimisation or a finite-difference check moves the
+ * nodes of one system instead. */
+int sbk_system_set_coordinates(sbk_system* sys, const double* coords_dev);
+
 /* ---- contact: ToolContact ---------------------------------------------- */
 typedef struct sbk_contact sbk_contact;
 

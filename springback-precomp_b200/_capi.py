@@ -126,6 +126,8 @@ SIGNATURES = {
     "sbk_system_stiffness_gross": (_I, [_P, _P, _I32, _P, ctypes.POINTER(_D)]),
     "sbk_system_stress": (_I, [_P, _P, _P]),
     "sbk_system_vjp_x": (_I, [_P, _P, _P, _I, _P]),
+    "sbk_system_set_frozen": (_I, [_P, _I]),
+    "sbk_system_set_coordinates": (_I, [_P, _P]),
     "sbk_contact_create": (_I, [ctypes.POINTER(sbk_mesh), _I32, ctypes.POINTER(sbk_tool), _I, ctypes.POINTER(_P)]),
     "sbk_contact_destroy": (_I, [_P]),
     "sbk_contact_set_stream": (_I, [_P, _P]),

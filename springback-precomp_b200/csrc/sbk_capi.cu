@@ -361,6 +361,8 @@ struct sbk_system {
   int64_t nn = 0, ne = 0, nnz = 0, num_blocks = 0;
   cudaStream_t stream = nullptr;
   bool plastic = false;
+  bool frozen = false;            // committed plastic state frozen: no return
+  int material_symmetric = 1;     // Params::symmetric of the material
   // mesh
   double* coords = nullptr;
   int32_t* conn = nullptr;
@@ -620,6 +622,7 @@ int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const 
   s->nn = mesh->num_nodes;
   s->ne = mesh->num_elements;
   s->plastic = p.enabled != 0;
+  s->material_symmetric = p.symmetric;
   if (s->ne * p.nq > 0x7fffffffLL) {
     free_system(s);
     return fail(SBK_ERR_UNSUPPORTED, "too many points");
@@ -724,6 +727,22 @@ int sbk_system_set_element(sbk_system* sys, int element, int mean_dilatation) {
                         ? 1
                         : 0;
   sys->order_valid = false;
+  return SBK_OK;
+}
+
+int sbk_system_set_frozen(sbk_system* sys, int frozen) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  sys->frozen = frozen != 0;
+  sys->p.enabled = (sys->plastic && !sys->frozen) ? 1 : 0;
+  sys->p.symmetric = sys->frozen ? 1 : sys->material_symmetric;
+  sys->order_valid = false;
+  return SBK_OK;
+}
+
+int sbk_system_set_coordinates(sbk_system* sys, const double* coords_dev) {
+  if (!sys || !coords_dev) return fail(SBK_ERR_ARGUMENT, "null argument");
+  SBK_CUDA(cudaMemcpyAsync(sys->coords, coords_dev, static_cast<size_t>(sys->nn) * 3 * sizeof(double),
+                           cudaMemcpyDeviceToDevice, sys->stream));
   return SBK_OK;
 }
 

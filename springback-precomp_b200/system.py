@@ -213,6 +213,7 @@ class NonlinearSystem:
         self._h = h
         self.set_stream(stream)
         self.set_element(element, mean_dilatation)
+        self.frozen = False
         pat = _capi.sbk_pattern()
         _capi.check(_capi.lib().sbk_system_pattern(self._h, ctypes.byref(pat)))
         self.num_dofs = int(pat.num_dofs)
@@ -398,6 +399,22 @@ class NonlinearSystem:
             raise _capi.SolverError(st, _capi.last_error())
         _capi.check(st)
         return out
+
+    def set_frozen(self, frozen: bool = True):
+        """Take the committed plastic state as it is in the evaluations that
+        follow (no return; the elastic, symmetric tangent): the release step
+        with the end-of-forming state frozen."""
+        _capi.check(_capi.lib().sbk_system_set_frozen(self._h, int(bool(frozen))))
+        self.frozen = bool(frozen)
+
+    def set_coordinates(self, coords: torch.Tensor):
+        """Move the nodes: the reference coordinates (num_nodes x 3, float64,
+        on the device) replace the mesh's; connectivity, pattern and history
+        stay."""
+        if coords.dtype != torch.float64 or coords.numel() != 3 * self.mesh.num_nodes or not coords.is_cuda:
+            raise ValueError("coords must hold num_nodes x 3 float64 values on the device")
+        self._coords_dev = coords.detach().contiguous()
+        _capi.check(_capi.lib().sbk_system_set_coordinates(self._h, _ptr(self._coords_dev)))
 
     def stiffness_gross(self, u: torch.Tensor, free: torch.Tensor) -> float:
         """stiffness_gross (src/fem/NonlinearSystem.hpp:49-67): the norm over

@@ -192,23 +192,28 @@ def test_bad_partitions_are_refused(pkg, elastic):
         pkg.PartitionedFactor.for_system(s, np.array([0, s.num_dofs], dtype=np.int32))
 
 
-@pytest.mark.parametrize("skew", [0.0, 1e-3])
-def test_transposed_solve(pkg, plastic, cuda, skew):
+@pytest.mark.parametrize("case", ["cholesky", "lu"])
+def test_transposed_solve(pkg, elastic, plastic, cuda, case):
     """K_ff^-T b with the factorisation K_ff^-1 b uses (the adjoint system):
-    the Cholesky of a symmetric block solves it as it stands; the dense LU of
-    a non-symmetric block solves with its transpose, against a dense solve."""
-    s, values = plastic
+    the Cholesky of the held elastic block solves it as it stands; the dense
+    LU of a non-symmetric block solves with its transpose - against a dense
+    solve of the transposed block."""
     rng = np.random.default_rng(12)
-    free = np.flatnonzero(rng.random(s.num_dofs) < 0.8).astype(np.int32)
-    v = values.cpu().numpy() * (1.0 + skew * rng.standard_normal(s.nnz))
+    if case == "cholesky":
+        s, values, free = elastic
+        v = values.cpu().numpy()
+    else:
+        s, values = plastic
+        free = np.flatnonzero(rng.random(s.num_dofs) < 0.8).astype(np.int32)
+        v = values.cpu().numpy() * (1.0 + 1e-3 * rng.standard_normal(s.nnz))
     part = pkg.PartitionedFactor.for_system(s, free)
-    kind = part.factorize(torch.tensor(v, device=cuda), symmetric=skew == 0.0 and s.symmetric())
+    kind = part.factorize(torch.tensor(v, device=cuda), symmetric=case == "cholesky")
+    assert kind == (1 if case == "cholesky" else 4)
     b = rng.standard_normal(len(free))
     x = part.solve(torch.tensor(b, device=cuda), transpose=True).cpu().numpy()
     ref = np.linalg.solve(dense_block(s, v, free).T, b)
     assert np.linalg.norm(x - ref) <= SOLVE_TOL * np.linalg.norm(ref)
-    if skew:
-        assert kind == 4
+    if case == "lu":
         fwd = np.linalg.solve(dense_block(s, v, free), b)
         assert np.linalg.norm(fwd - ref) > 1e3 * SOLVE_TOL * np.linalg.norm(ref)
 
