@@ -429,9 +429,39 @@ def run_adjoint(args, rank, world):
                                     "median_relative_difference": statistics.median(errors) if errors else None,
                                     "seconds": fd_s},
             "factor_kind": release.part.kind, "clocks": clocks.summary()}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_adjoint(pkg, args.adj_sample)
     print(json.dumps(line))
     release.close()
     return 0
+
+
+def cpu_adjoint(pkg, n):
+    """The same release and gradient with the oracle on the host cores (the
+    oracle's release Newton with scipy's sparse LU, its adjoint with the
+    transposed block and its per-element shape derivative) on an n x n x 2
+    sample part whose history the oracle loads."""
+    orc = oracle_module()
+    prob, committed = oracle_problem(orc, n, n, 2, 5)
+    mesh, mat = prob.mesh, prob.material
+    m = mat.as_dict()
+    m["yield_stress"] = 1e300  # frozen
+    free = pkg.supports_321(mesh)
+    top = np.flatnonzero(np.isclose(mesh.coords[:, 2], mesh.coords[:, 2].max()))
+    t0 = time.perf_counter()
+    u, iterations = orc.release_solve(m, mesh.coords, mesh.connectivity, committed, prob.alpha, free, prob.u)
+    release_s = time.perf_counter() - t0
+    d = u.reshape(-1, 3)[top, 2] - prob.u.reshape(-1, 3)[top, 2]
+    j = float(np.sqrt(np.mean(d * d)))
+    dj = np.zeros(mesh.num_dofs)
+    dj[3 * top + 2] = d / (len(top) * j)
+    t0 = time.perf_counter()
+    orc.release_adjoint(m, mesh.coords, mesh.connectivity, committed, prob.alpha, free, u, dj)
+    adjoint_s = time.perf_counter() - t0
+    return {"value": (release_s + adjoint_s) / release_s, "unit": "x", "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{n}x{n}x2 part ({mesh.num_elements} elements), the oracle's history, one release and one "
+                      "gradient",
+            "release_solve_ms": release_s * 1e3, "newton_iterations": iterations, "adjoint_ms": adjoint_s * 1e3}
 
 
 def run_partition(args, rank, world):
@@ -591,6 +621,7 @@ def main():
     p.add_argument("--adj-nx", type=int, default=100)
     p.add_argument("--adj-ny", type=int, default=100)
     p.add_argument("--directions", type=int, default=32)
+    p.add_argument("--adj-sample", type=int, default=40)
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
 

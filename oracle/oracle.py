@@ -391,6 +391,64 @@ def add_to(full, free, part, factor) -> np.ndarray:
     return out
 
 
+def release_solve(m: dict, coords, conn, committed, alpha_n, free, u0, kinematics="logarithmic", tol=1e-10,
+                  max_iterations=40, threads=0):
+    """The released equilibrium on the CPU: Newton on the free rows of
+    f_int(u) = 0 from u0 (its held DOFs kept), every tangent the oracle's
+    assembled CSC (NonlinearSystem::evaluate restated) and every correction
+    a scipy sparse solve of its free-free block, until a full step is below
+    `tol` of u, then one step more. The frozen release passes a material
+    whose yield stress no point reaches. Returns (u, iterations)."""
+    import scipy.sparse
+    import scipy.sparse.linalg
+
+    coords = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+    nn = coords.shape[0]
+    pat = pattern(nn, conn)
+    free = np.asarray(free, dtype=np.int64)
+    u = np.array(u0, dtype=np.float64, copy=True)
+    converged = False
+    for it in range(max_iterations):
+        r = system_evaluate(m, coords, conn, u, committed, alpha_n, kinematics=kinematics, threads=threads, pat=pat)
+        if r["code"] != 0:
+            raise RuntimeError(f"the oracle's element {r['failed_element']} failed in the release")
+        if converged:
+            return u, it
+        k = scipy.sparse.csc_matrix((r["values"], pat["inner"], pat["outer"]), shape=(3 * nn, 3 * nn))
+        du = scipy.sparse.linalg.spsolve(k[free][:, free].tocsc(), -r["internal"][free])
+        u[free] += du
+        converged = np.linalg.norm(du) <= tol * np.linalg.norm(u)
+    raise RuntimeError("the oracle's release did not converge")
+
+
+def release_adjoint(m: dict, coords, conn, committed, alpha_n, free, u, dj_du, kinematics="logarithmic",
+                    threads=0) -> np.ndarray:
+    """dJ/dX (nn, 3) of a functional J(u*) of the released equilibrium u* on
+    the CPU: K_ff^T lambda_f = (dJ/du)_f with the oracle's tangent at u*
+    (scipy sparse solve of the transposed block), lambda zero on the held
+    DOFs, and -lambda . d f_int / d X from the oracle's per-element shape
+    derivative (vjp_x), summed into the nodes in element order."""
+    import scipy.sparse
+    import scipy.sparse.linalg
+
+    coords = np.ascontiguousarray(coords, dtype=np.float64).reshape(-1, 3)
+    conn = np.ascontiguousarray(conn, dtype=np.int32).reshape(-1, 8)
+    nn = coords.shape[0]
+    pat = pattern(nn, conn)
+    free = np.asarray(free, dtype=np.int64)
+    r = system_evaluate(m, coords, conn, u, committed, alpha_n, kinematics=kinematics, threads=threads, pat=pat)
+    k = scipy.sparse.csc_matrix((r["values"], pat["inner"], pat["outer"]), shape=(3 * nn, 3 * nn))
+    lam = np.zeros(3 * nn)
+    lam[free] = scipy.sparse.linalg.spsolve(k[free][:, free].T.tocsc(), np.asarray(dj_du)[free])
+    dofs = (3 * conn[:, :, None] + np.arange(3)).reshape(-1, 24)
+    per, st = vjp_x(m, coords[conn].reshape(-1, 24), u[dofs], lam[dofs], committed, alpha_n, kinematics=kinematics)
+    if (st != 0).any():
+        raise RuntimeError("the oracle's shape derivative failed")
+    gx = np.zeros(3 * nn)
+    np.add.at(gx, dofs.reshape(-1), per.reshape(-1))
+    return -gx.reshape(nn, 3)
+
+
 class Contact:
     """ToolContact restated: tools = list of dicts with shape ('sphere',
     'plane', 'cylinder'), radius, friction, tangential_ratio, normal, axis,

@@ -232,3 +232,35 @@ def test_height_gradient_matches_central_differences(pkg, part, cuda):
         worst = max(worst, abs(adj - fd) / abs(fd))
         assert abs(adj - fd) <= GRADIENT_TOL * abs(fd), (adj, fd, abs(adj - fd) / abs(fd))
     print(f"heights: J {float(j.detach()):.6e} m, worst relative difference over 32 directions {worst:.2e}")
+
+
+def test_height_gradient_is_the_oracles(pkg, orc, part, cuda):
+    """The device's release and its 400-height gradient against the same
+    built from the oracle's CPU element routines (the oracle's release
+    Newton with scipy solves, the oracle's adjoint and per-element shape
+    derivative): u* within 1e-10 and dJ/dp within 1e-8 relative."""
+    import test_oracle_adjoint as toa
+
+    j_ref, grad_ref, u_ref, _ = toa.oracle_gradient(pkg, orc, part)
+    mesh = part.mesh
+    x0 = torch.tensor(mesh.coords, device=cuda)
+    lo, hi = mesh.coords.min(axis=0), mesh.coords.max(axis=0)
+    grid = pkg.BicubicHeights(lo[0], hi[0], lo[1], hi[1], n=20)
+    stencil = grid.stencil(mesh.coords[:, :2], device=cuda)
+    top = torch.tensor(np.flatnonzero(np.isclose(mesh.coords[:, 2], hi[2])), device=cuda)
+    u_formed = torch.tensor(part.u, device=cuda)
+    target = x0[top, 2] + u_formed.reshape(-1, 3)[top, 2]
+    release = pkg.Release(mesh, part.material, part.state, part.alpha, pkg.supports_321(mesh))
+    p = torch.zeros((20, 20), dtype=torch.float64, device=cuda, requires_grad=True)
+    lift = torch.zeros_like(x0)
+    lift[:, 2] = grid.heights(p, stencil)
+    coords = x0 + lift
+    u_star = pkg.released(coords, release, u_formed)
+    j = pkg.springback_rms(coords, u_star, top, target)
+    j.backward()
+    u_np, grad = u_star.detach().cpu().numpy(), p.grad.cpu().numpy()
+    assert np.linalg.norm(u_np - u_ref) <= 1e-10 * np.linalg.norm(u_ref)
+    assert abs(float(j.detach()) - j_ref) <= 1e-10 * j_ref
+    rel = np.linalg.norm(grad - grad_ref) / np.linalg.norm(grad_ref)
+    print(f"heights: device against oracle gradient {rel:.2e}")
+    assert rel <= 1e-8
