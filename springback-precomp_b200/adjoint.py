@@ -15,11 +15,12 @@ gradient:
   the formed part left them, the committed points and modes frozen
   (sbk_system_set_frozen) - the release step of the forming driver
   (Forming.cpp release handling) without its tool and clamp bookkeeping.
-- Release.adjoint: the points re-evaluated at u* (not stored from the
-  forward solve), the tangent factorised again, K_ff^T lambda_f = dJ/du_f
-  solved with that factorisation transposed, and
-  dJ/dX = -lambda^T d f_int / d X by the shape-derivative kernel
-  (sbk_system_vjp_x, the modes through their local equilibrium).
+- Release.adjoint: K_ff^T lambda_f = dJ/du_f solved with the factorisation
+  of the tangent at u* transposed (the one the release's last Newton
+  evaluate left, or a new one), and dJ/dX = -lambda^T d f_int / d X by the
+  shape-derivative kernel (sbk_system_vjp_x, the modes through their local
+  equilibrium), which recomputes the points from the committed state rather
+  than reading them from the forward solve.
 - ReleaseFunction: both as a torch.autograd.Function of X.
 - BicubicHeights: the commanded-shape parametrisation, a clamped uniform
   cubic B-spline surface over the footprint whose n x n control heights move
@@ -120,16 +121,29 @@ class Release:
         self.max_iterations = max_iterations
         self.iterations = 0
         self.factorizations = 0
+        self._factored = None
 
     def close(self):
         self.part.close()
         self.system.close()
 
-    def _tangent(self, u: torch.Tensor):
+    def _tangent(self, u: torch.Tensor, coords: torch.Tensor):
+        """Evaluate and factorise at (u, coords), remembering where: the last
+        Newton evaluate is at the root, and the adjoint reuses it."""
+        self._factored = None
         ev = self.system.evaluate(u, 0.0, True)
         self.part.factorize(ev.tangent, self.system.symmetric())
         self.factorizations += 1
+        self._factored = (u.detach().clone(), coords.detach().reshape(-1, 3).clone())
         return ev
+
+    def forget_factorization(self):
+        """Make the next adjoint re-evaluate and factorise at its u."""
+        self._factored = None
+
+    def _factored_at(self, u: torch.Tensor, coords: torch.Tensor) -> bool:
+        f = getattr(self, "_factored", None)
+        return f is not None and torch.equal(f[0], u) and torch.equal(f[1], coords.reshape(-1, 3))
 
     def solve(self, coords: torch.Tensor, u0: torch.Tensor) -> torch.Tensor:
         """The released displacement u* at the reference coordinates coords
@@ -139,7 +153,7 @@ class Release:
         converge."""
         self.system.set_coordinates(coords.reshape(-1, 3))
         u = u0.detach().clone()
-        ev = self._tangent(u)
+        ev = self._tangent(u, coords)
         r = self.part.restrict(ev.internal)
         converged = False
         for it in range(self.max_iterations):
@@ -148,7 +162,7 @@ class Release:
             while True:
                 trial = self.part.add_to(u.clone(), du, step)
                 try:
-                    ev = self._tangent(trial)
+                    ev = self._tangent(trial, coords)
                     break
                 except _capi.SolverError:
                     step *= 0.5
@@ -163,12 +177,16 @@ class Release:
         raise _capi.SolverError(4, f"the release did not converge in {self.max_iterations} Newton iterations")
 
     def adjoint(self, coords: torch.Tensor, u: torch.Tensor, grad_u: torch.Tensor) -> torch.Tensor:
-        """dJ/dX (num_nodes x 3) from dJ/du at the released u: the points
-        re-evaluated at u, K_ff^T lambda_f = (dJ/du)_f with that tangent's
-        factorisation, -lambda^T d f_int / d X. The held DOFs of u do not
-        depend on X; their share of dJ/du stays with the caller."""
+        """dJ/dX (num_nodes x 3) from dJ/du at the released u: K_ff^T
+        lambda_f = (dJ/du)_f with the factorisation of the tangent at u (the
+        one the release's last Newton evaluate left, when it was at this u
+        and these coordinates; else the points re-evaluated at u and the
+        tangent factorised again), then -lambda^T d f_int / d X, whose kernel
+        recomputes the points from the committed state. The held DOFs of u do
+        not depend on X; their share of dJ/du stays with the caller."""
         self.system.set_coordinates(coords.reshape(-1, 3))
-        self._tangent(u)
+        if not self._factored_at(u, coords):
+            self._tangent(u, coords)
         lam_f = self.part.solve(self.part.restrict(grad_u.detach().to(torch.float64)), transpose=True)
         lam = self.part.add_to(torch.zeros_like(u), lam_f, 1.0)
         return -self.system.vjp_x(u, lam, frozen=True).reshape(-1, 3)

@@ -264,3 +264,24 @@ def test_height_gradient_is_the_oracles(pkg, orc, part, cuda):
     rel = np.linalg.norm(grad - grad_ref) / np.linalg.norm(grad_ref)
     print(f"heights: device against oracle gradient {rel:.2e}")
     assert rel <= 1e-8
+
+
+def test_adjoint_reuses_the_factorisation_at_the_root(pkg, part, cuda):
+    """The adjoint after a release reuses the factorisation its last Newton
+    evaluate left at u*: the same gradient as one that re-evaluates and
+    factorises again, one factorisation fewer; a u it was not factorised at
+    is factorised anew."""
+    mesh = part.mesh
+    x0 = torch.tensor(mesh.coords, device=cuda)
+    release = pkg.Release(mesh, part.material, part.state, part.alpha, pkg.supports_321(mesh))
+    u_star = release.solve(x0, torch.tensor(part.u, device=cuda))
+    c = torch.tensor(np.random.default_rng(2).standard_normal(mesh.num_dofs), device=cuda)
+    n0 = release.factorizations
+    warm = release.adjoint(x0, u_star, c)
+    assert release.factorizations == n0
+    release.forget_factorization()
+    cold = release.adjoint(x0, u_star, c)
+    assert release.factorizations == n0 + 1
+    assert float(torch.linalg.norm(warm - cold)) <= 1e-12 * float(torch.linalg.norm(cold))
+    other = release.adjoint(x0, u_star * (1.0 + 1e-9), c)
+    assert release.factorizations == n0 + 2 and torch.isfinite(other).all()
