@@ -10,7 +10,7 @@ own interfaces.
 """
 from . import _capi
 from ._capi import SbkError, SolverError
-from .adjoint import BicubicHeights, Release, ReleaseFunction, released, springback_rms, supports_321
+from .adjoint import BicubicHeights, Release, ReleaseFunction, compensate, released, springback_rms, supports_321
 from .contact import ToolContact, Tool
 from .material import Material
 from .mesh import HexMesh, structured_hex_mesh
@@ -19,7 +19,8 @@ from .system import Evaluation, NonlinearSystem, element_batch
 
 __all__ = ["Material", "HexMesh", "structured_hex_mesh", "NonlinearSystem", "Evaluation", "element_batch",
            "ToolContact", "Tool", "SbkError", "SolverError", "PartitionedFactor",
-           "BicubicHeights", "Release", "ReleaseFunction", "released", "springback_rms", "supports_321"]
+           "BicubicHeights", "Release", "ReleaseFunction", "compensate", "released", "springback_rms",
+           "supports_321"]
 
 
 def library_path() -> str:

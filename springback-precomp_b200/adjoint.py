@@ -242,3 +242,50 @@ def supports_321(mesh: HexMesh, tol: Optional[float] = None) -> np.ndarray:
     held = np.zeros(mesh.num_dofs, dtype=bool)
     held[[3 * a, 3 * a + 1, 3 * a + 2, 3 * b + 1, 3 * b + 2, 3 * c + 2]] = True
     return np.flatnonzero(~held).astype(np.int32)
+
+
+def compensate(release: Release, grid: BicubicHeights, stencil, coords0: torch.Tensor, nodes: torch.Tensor,
+               target_z: torch.Tensor, u0: torch.Tensor, iterations: int = 10, history_size: int = 10):
+    """Adjoint-driven compensation: the control heights p that minimise the
+    RMS vertical deviation of the released part from the target, by L-BFGS
+    with a strong-Wolfe line search (torch.optim.LBFGS), every objective one
+    release solve (warm-started from the last) and every gradient one
+    adjoint. It takes the place of the reference's displacement adjustment,
+    c_{k+1} = c_k - alpha (f(c_k) - t) (compensation.py:273-366), which
+    needs one forming and release simulation per step and no gradient.
+
+    p is optimised in units of the initial deviation (q = p / J0, the
+    objective J / J0), so that the first step is of the springback's size.
+    Returns (p, the objective after each evaluation in metres, the number of
+    release solves)."""
+    device = coords0.device
+    warm = [u0.detach()]
+    history = []
+
+    def objective(q: torch.Tensor, scale: float) -> torch.Tensor:
+        lift = torch.zeros_like(coords0)
+        lift[:, 2] = grid.heights(q * scale, stencil)
+        coords = coords0 + lift
+        u = released(coords, release, warm[0])
+        warm[0] = u.detach()
+        return springback_rms(coords, u, nodes, target_z)
+
+    zero = torch.zeros((grid.n, grid.n), dtype=torch.float64, device=device)
+    with torch.no_grad():
+        j0 = float(objective(zero, 1.0))
+    history.append(j0)
+    if j0 == 0.0:
+        return zero, history, 1
+    q = zero.clone().requires_grad_(True)
+    opt = torch.optim.LBFGS([q], lr=1.0, max_iter=iterations, history_size=history_size,
+                            tolerance_grad=0.0, tolerance_change=0.0, line_search_fn="strong_wolfe")
+
+    def closure():
+        opt.zero_grad()
+        j = objective(q, j0)
+        history.append(float(j.detach()))
+        (j / j0).backward()
+        return j / j0
+
+    opt.step(closure)
+    return (q.detach() * j0), history, len(history)

@@ -285,3 +285,30 @@ def test_adjoint_reuses_the_factorisation_at_the_root(pkg, part, cuda):
     assert float(torch.linalg.norm(warm - cold)) <= 1e-12 * float(torch.linalg.norm(cold))
     other = release.adjoint(x0, u_star * (1.0 + 1e-9), c)
     assert release.factorizations == n0 + 2 and torch.isfinite(other).all()
+
+
+def test_compensation_reduces_the_springback(pkg, part, cuda):
+    """Adjoint-driven compensation on the 32 x 32 x 2 part: L-BFGS over the
+    20 x 20 control heights, every step one release solve and one adjoint,
+    pre-distorts the part so that its released top face comes back towards
+    the formed heights - the RMS deviation falls to at most half its
+    uncompensated value within 10 iterations and the best point found is the
+    one returned."""
+    mesh = part.mesh
+    x0 = torch.tensor(mesh.coords, device=cuda)
+    lo, hi = mesh.coords.min(axis=0), mesh.coords.max(axis=0)
+    grid = pkg.BicubicHeights(lo[0], hi[0], lo[1], hi[1], n=20)
+    stencil = grid.stencil(mesh.coords[:, :2], device=cuda)
+    top = torch.tensor(np.flatnonzero(np.isclose(mesh.coords[:, 2], hi[2])), device=cuda)
+    u_formed = torch.tensor(part.u, device=cuda)
+    target = x0[top, 2] + u_formed.reshape(-1, 3)[top, 2]
+    release = pkg.Release(mesh, part.material, part.state, part.alpha, pkg.supports_321(mesh))
+    p, history, solves = pkg.compensate(release, grid, stencil, x0, top, target, u_formed, iterations=10)
+    print(f"compensation: RMS {history[0]:.4e} m -> {min(history):.4e} m in {solves} release solves; "
+          f"history {[f'{h:.3e}' for h in history]}")
+    assert min(history) <= 0.5 * history[0]
+    lift = torch.zeros_like(x0)
+    lift[:, 2] = grid.heights(p, stencil)
+    with torch.no_grad():
+        j = float(pkg.springback_rms(x0 + lift, release.solve(x0 + lift, u_formed), top, target))
+    assert j <= 0.5 * history[0]
