@@ -66,7 +66,7 @@ UNIT = "elem/s"
 
 
 def oracle_module():
-    """The checker (test infrastructure), for the CPU-baseline legs only."""
+    """The oracle (test infrastructure), for the CPU-baseline legs only."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 

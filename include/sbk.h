@@ -33,7 +33,7 @@ enum sbk_status {
   SBK_ERR_MESH = 3,        /* MeshError: an element inverted at rest      */
   SBK_ERR_SOLVER = 4,      /* SolverError: see the failing element's code */
   SBK_ERR_CUDA = 5,        /* a CUDA call failed                          */
-  SBK_ERR_UNSUPPORTED = 6, /* a rule or a size this build does not take   */
+  SBK_ERR_UNSUPPORTED = 6, /* a rule or a size the library does not take */
   SBK_ERR_NO_EXTENSION = 7 /* no device: the library never falls back     */
 };
 
@@ -78,8 +78,8 @@ typedef struct sbk_material {
 
 /* The stiffness rule (include/sparlab/elements/Element.hpp:56-71):
  * stiffness_points per direction (1..4), thickness_points (0: the cube
- * rule; else 1..7 along thickness_axis 0/1/2). This build takes rules of at
- * most SBK_MAX_POINTS points. */
+ * rule; else 1..7 along thickness_axis 0/1/2). The library takes rules of
+ * at most SBK_MAX_POINTS points. */
 typedef struct sbk_rule {
   int stiffness_points, thickness_points, thickness_axis, reserved;
 } sbk_rule;

@@ -1,7 +1,7 @@
 // ORACLE — test infrastructure only. A plain CPU restatement of the
 // reference's element-level algorithms (sparlab, C++17/Eigen), used by the
-// tests, the smoke check and the CPU-baseline leg of bench.py as the checker
-// of the CUDA path. Nothing in the product links, includes or calls it.
+// tests, the smoke check and the CPU-baseline leg of bench.py to check the
+// results of the CUDA path. Nothing in the product links, includes or calls it.
 //
 // This header: the material point - hardening laws, the Hill48 yield
 // matrix, the J2 radial return, the general (Hill48 / Chaboche)
