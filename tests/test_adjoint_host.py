@@ -79,3 +79,31 @@ def test_supports_hold_six_dofs(pkg):
     corners = mesh.coords[np.unique(nodes)]
     assert np.allclose(corners[:, 2], 0.0)
     assert sorted(np.bincount(nodes)[np.unique(nodes)].tolist()) == [1, 2, 3]
+
+
+def test_bad_inputs_are_refused(pkg, adj):
+    with pytest.raises(ValueError):
+        adj.cubic_bspline_basis(np.array([0.5]), 3)
+    with pytest.raises(ValueError):
+        pkg.BicubicHeights(1.0, 1.0, 0.0, 1.0)
+    # A mesh with no node at a support corner (its corner element removed).
+    mesh = pkg.structured_hex_mesh(3, 3, 1, 0.3, 0.3, 0.01)
+    keep = np.ones(mesh.num_elements, dtype=bool)
+    keep[0] = False
+    conn = mesh.connectivity[keep]
+    used = np.unique(conn)
+    remap = -np.ones(mesh.num_nodes, dtype=np.int64)
+    remap[used] = np.arange(len(used))
+    holed = pkg.HexMesh(mesh.coords[used], remap[conn].astype(np.int32))
+    with pytest.raises(ValueError):
+        pkg.supports_321(holed)
+
+
+def test_heights_clamp_outside_the_footprint(pkg):
+    """Points outside the footprint take the edge's heights (the parameter
+    is clamped), so a mesh overhanging the grid stays defined."""
+    grid = pkg.BicubicHeights(0.0, 1.0, 0.0, 1.0, n=5)
+    p = torch.tensor(np.random.default_rng(3).standard_normal((5, 5)))
+    inside = grid.heights(p, grid.stencil(np.array([[0.0, 0.3], [1.0, 0.7]])))
+    outside = grid.heights(p, grid.stencil(np.array([[-0.2, 0.3], [1.4, 0.7]])))
+    np.testing.assert_array_equal(inside.numpy(), outside.numpy())
