@@ -49,18 +49,18 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 PKG = "springback-precomp_b200"
 METRIC = "Hex8 tangent+residual+assembly elem/s (FP64)"
-# DRAM bytes (read + write) per element of one element-kernel launch, from
-# the ncu capture of the same construction at 80,000 elements
-# (profiles/element_kernel_microbench.md: 0.69 + 5.28 GB / 80,000); the
+# DRAM bytes (read + write) per element of one element-kernel launch:
+# ncu's dram__bytes_read.sum + dram__bytes_write.sum over one launch of the
+# same construction at 80,000 elements (200 x 200 x 2), 0.69 + 5.28 GB; the
 # traffic grows with the elements, so a launch of ne elements moves about ne
 # times this.
 K1_DRAM_BYTES_PER_ELEMENT = (0.692594688e9 + 5.275133e9) / 80000
-# The same for the standard Hex8 kernel (profiles/standard_kernel_microbench.md:
-# 0.192 GB read + 1.610 GB written at 80,000 elements).
+# The same for the standard Hex8 kernel: 0.192 GB read + 1.610 GB written in
+# one launch at 80,000 elements.
 K1S_DRAM_BYTES_PER_ELEMENT = (0.191949568e9 + 1.610487e9) / 80000
-# DRAM bytes per block entry of one free-free gather (assemble), from the ncu
-# capture of the 200 x 200 x 2 sheet's block (profiles/free_free_partition.md:
-# 271.0 MB read + 139.0 MB written for 22,528,485 entries).
+# DRAM bytes per block entry of one free-free gather (assemble): the same ncu
+# metrics over one launch on the 200 x 200 x 2 sheet's block, 271.0 MB read +
+# 139.0 MB written for 22,528,485 entries.
 GATHER_DRAM_BYTES_PER_ENTRY = (271.010304e6 + 139.048192e6) / 22528485
 UNIT = "elem/s"
 
@@ -198,35 +198,78 @@ def measured_peaks():
 
 
 def run_reference(args, rank, world):
-    """The reference arm: the oracle port on all host cores."""
+    """The reference arm: the oracle port (the reference's CPU algorithm:
+    OpenMP static schedule over elements, serial scatter in element order)
+    built -O3 -march=native for this host's CPU, on all host cores, one
+    evaluation of a bounded sample of the same workload per step; beside it
+    the same on one thread on a smaller sample."""
     if rank != 0:
         return 0
     orc = oracle_module()
-    nx, ny, nz = args.sample_nx, args.sample_ny, args.nz
+    orc.use_variant("fast")
+    nx, ny, nz = args.ref_nx, args.ref_ny, args.nz
     prob, committed = oracle_problem(orc, nx, ny, nz, seed=7)
     cores = cpu_count()
     mesh, mat = prob.mesh, prob.material
     pat = orc.pattern(mesh.num_nodes, mesh.connectivity)
-    for _ in range(args.warmup):
-        orc.system_evaluate(mat.as_dict(), mesh.coords, mesh.connectivity, prob.u, committed, prob.alpha,
-                            threads=cores, pat=pat)
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        r = orc.system_evaluate(mat.as_dict(), mesh.coords, mesh.connectivity, prob.u, committed, prob.alpha,
+    std = args.element == "standard"
+    with orc.element(std, True):
+        for _ in range(args.warmup):
+            orc.system_evaluate(mat.as_dict(), mesh.coords, mesh.connectivity, prob.u, committed, prob.alpha,
                                 threads=cores, pat=pat)
-        assert r["code"] == 0
-    dt = (time.perf_counter() - t0) / args.steps
+        times = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            r = orc.system_evaluate(mat.as_dict(), mesh.coords, mesh.connectivity, prob.u, committed, prob.alpha,
+                                    threads=cores, pat=pat)
+            times.append(time.perf_counter() - t0)
+            assert r["code"] == 0
+    dt = sum(times) / len(times)
     value = mesh.num_elements / dt
+    # One thread, on the small sample (bounded to a few seconds).
+    small, small_committed = oracle_problem(orc, args.sample_nx, args.sample_ny, nz, seed=7)
+    with orc.element(std, True):
+        one_rate, n_one = time_oracle(orc, small, small_committed, 1, 4.0)
     sample = (f"{mesh.num_elements} elements ({nx}x{ny}x{nz} of the same sheet, law and history construction) "
-              f"per step")
+              f"per step, {cores} threads; single thread on {small.mesh.num_elements} elements "
+              f"({args.sample_nx}x{args.sample_ny}x{nz}), median of {n_one} runs")
+    cpu = {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample,
+           "single_thread": one_rate, "median_step_ms": statistics.median(times) * 1e3,
+           "build": orc.FAST_FLAGS, "cpu": cpu_model()}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": config(args, world),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "config": config(args, world), "cpu_baseline": cpu,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def cpu_baseline_subprocess(args):
+    """The reference arm's measurement, run as its own process before this
+    process touches the GPU (so that no CUDA or torch thread shares the host
+    cores with it), with fewer steps; its cpu_baseline object."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--impl", "reference", "--steps", str(args.cpu_steps),
+           "--warmup", "3", "--nz", str(args.nz), "--ref-nx", str(args.ref_nx), "--ref-ny", str(args.ref_ny),
+           "--sample-nx", str(args.sample_nx), "--sample-ny", str(args.sample_ny), "--element", args.element]
+    env = dict(os.environ)
+    env["CUDA_VISIBLE_DEVICES"] = ""
+    out = subprocess.run(cmd, check=True, capture_output=True, text=True, env=env).stdout
+    line = json.loads([ln for ln in out.splitlines() if ln.startswith("{")][-1])
+    cpu = line["cpu_baseline"]
+    cpu["sample"] += f"; {args.cpu_steps} timed steps in a separate process before the GPU work"
+    return cpu
 
 
 def run_batched(args, rank, world):
@@ -608,6 +651,9 @@ def main():
     p.add_argument("--nz", type=int, default=2)
     p.add_argument("--sample-nx", type=int, default=50)
     p.add_argument("--sample-ny", type=int, default=40)
+    p.add_argument("--ref-nx", type=int, default=160, help="the CPU baseline's all-core sample: ref-nx x ref-ny x nz")
+    p.add_argument("--ref-ny", type=int, default=160)
+    p.add_argument("--cpu-steps", type=int, default=5, help="timed steps of the in-run CPU baseline")
     p.add_argument("--epb", type=int, default=0, help="elements per block of the element kernel (0: default)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -639,6 +685,10 @@ def main():
         return run_partition(args, rank, world)
     if args.workload == "adjoint":
         return run_adjoint(args, rank, world)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_subprocess(args)
 
     import torch
 
@@ -714,21 +764,12 @@ def main():
 
     line = None
     if rank == 0:
-        cpu = None
         flops_per_element = None
         if world == 1 and not args.no_cpu_baseline:
             orc = oracle_module()
             prob, committed = oracle_problem(orc, args.sample_nx, args.sample_ny, args.nz, seed=7)
-            cores = cpu_count()
             std = orc.element(args.element == "standard", True)
-            with std:
-                all_rate, n_all = time_oracle(orc, prob, committed, cores, 10.0)
-                one_rate, n_one = time_oracle(orc, prob, committed, 1, 5.0)
-            cpu = {"value": all_rate, "unit": UNIT, "cores": cores, "kind": "port",
-                   "sample": f"{prob.mesh.num_elements} elements ({args.sample_nx}x{args.sample_ny}x{args.nz} of the "
-                             f"same sheet, law and history construction), median of {n_all} runs on {cores} "
-                             f"threads", "single_thread": one_rate}
-            # Algorithmic flops per element (counting scalar) on the same sample.
+            # Algorithmic flops per element (counting scalar) on a sample.
             with std:
                 cnt = orc.count_flops(prob.material.as_dict(), prob.mesh.element_coordinates(),
                                       prob.mesh.gather(prob.u), committed, prob.alpha)
@@ -741,10 +782,8 @@ def main():
                         "frac": achieved / fp64_peak,
                         "traffic": (K1_DRAM_BYTES_PER_ELEMENT if args.element == "incompatible_modes"
                                     else K1S_DRAM_BYTES_PER_ELEMENT) * ne,
-                        "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on "
-                                           "the 200x200x2 case, scaled by elements (profiles/"
-                                           + ("element_kernel_microbench.md)" if args.element == "incompatible_modes"
-                                              else "standard_kernel_microbench.md)")),
+                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on "
+                                          "the 200x200x2 sheet (80,000 elements), scaled by elements",
                         "kernel": ("element_kernel (K1)" if args.element == "incompatible_modes"
                                    else "standard_kernel (K1s)"), "kernel_ms": el_ms,
                         "flops_per_element": flops_per_element,

@@ -390,9 +390,13 @@ int sbk_contact_history(const sbk_contact* c, int32_t k, int32_t max_entries, do
  *   summed element by element in element order; NULL: no tangent),
  *   trial_dev / alpha_out_dev / yield_dev (as sbk_element_batch), and
  *   summary_dev: 5 doubles - energy, gross, yielding points, the lowest
- *   failing element (-1 if none) and its sbk_element_code; an element whose
- *   connectivity names a node out of range fails with SBK_EL_BAD_NODE and is
- *   left out of the sums, and a mesh block the pattern lacks gives -2 and
+ *   failing element (-1 if none) and its sbk_element_code. An element that
+ *   fails, for any reason, is left out of every sum (internal, values,
+ *   gross, energy, yield count) and its yield_dev bytes are not written;
+ *   an element whose connectivity names a node out of range fails with
+ *   SBK_EL_BAD_NODE before anything of it is read. An element naming one
+ *   node twice is added entry by entry, so both of its contributions to a
+ *   shared entry count. A mesh block the pattern lacks gives -2 and
  *   SBK_EL_BAD_NODE.
  * The call only enqueues work on `stream`; read summary_dev after it. The
  * first call on a device looks up the array's device address (with that

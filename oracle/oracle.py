@@ -18,6 +18,13 @@ LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 NF = 39  # per-point state layout: ep 6, beta 6, alpha 4x6, eqps, thick, loading
 
 _lib = None
+_libs = {}
+# "strict": the parity build (-O2, no contraction: every product and sum
+# separately rounded); "fast": the timed CPU baseline (-O3 -march=native,
+# fused multiply-adds allowed), built for the CPU it runs on.
+_variant = "strict"
+FAST_FLAGS = "-O3 -march=native -fopenmp (fused multiply-adds allowed)"
+STRICT_FLAGS = "-O2 -fopenmp -ffp-contract=off"
 
 
 def build() -> str:
@@ -26,13 +33,61 @@ def build() -> str:
     return LIB_PATH
 
 
+def cpu_key() -> str:
+    """A name for this host's CPU (model and instruction-set flags), so that
+    a -march=native build is only loaded on the CPU it was built for."""
+    import hashlib
+    import platform
+
+    text = platform.machine()
+    try:
+        with open("/proc/cpuinfo") as f:
+            lines = f.read().splitlines()
+        model = next((ln for ln in lines if ln.startswith("model name")), "")
+        flags = next((ln for ln in lines if ln.startswith("flags")), "")
+        text += model + flags
+    except OSError:
+        pass
+    return hashlib.sha1(text.encode()).hexdigest()[:12]
+
+
+def fast_path() -> str:
+    return os.path.join(HERE, "_build", "fast-" + cpu_key(), "liboracle.so")
+
+
+def build_fast() -> str:
+    """Compile the timed CPU baseline for this host's CPU (make fast)."""
+    path = fast_path()
+    subprocess.run(["make", "-s", "-C", HERE, "fast", f"FAST_OUT={path}"], check=True)
+    return path
+
+
+def use_variant(name: str) -> str:
+    """Route every binding of this module through the "strict" (parity) or
+    the "fast" (timed baseline) build; returns the previous variant."""
+    global _variant, _lib
+    if name not in ("strict", "fast"):
+        raise ValueError(name)
+    prev = _variant
+    _variant = name
+    _lib = None
+    return prev
+
+
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            build()
-        _lib = ctypes.CDLL(LIB_PATH)
-        _declare(_lib)
+        if _variant == "fast":
+            path = build_fast()
+        else:
+            path = LIB_PATH
+            if not os.path.exists(LIB_PATH):
+                build()
+        if path not in _libs:
+            handle = ctypes.CDLL(path)
+            _declare(handle)
+            _libs[path] = handle
+        _lib = _libs[path]
     return _lib
 
 

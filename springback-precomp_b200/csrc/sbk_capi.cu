@@ -1,8 +1,8 @@
 // The C ABI (include/sbk.h): materials and rules, the element batch, and the
 // system that stands in for detail::NonlinearSystem
-// (src/fem/NonlinearSystem.hpp:85-334) with its Assembler pattern
-// (src/fem/Assembler.cpp:86-173). Every device buffer belongs to a handle;
-// no exception crosses the ABI.
+// (src/fem/NonlinearSystem.hpp:85-334), whose Assembler pattern
+// (src/fem/Assembler.cpp:86-173) sbk_pattern.cu builds on the device. Every
+// device buffer belongs to a handle; no exception crosses the ABI.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -15,6 +15,7 @@
 #include "sbk.h"
 #include "sbk_element.h"
 #include "sbk_params.h"
+#include "sbk_pattern.h"
 
 using sbk::Params;
 
@@ -438,106 +439,6 @@ void free_system(sbk_system* s) {
   delete s;
 }
 
-// Assembler::build_pattern (src/fem/Assembler.cpp:86-173) and the gather
-// maps of the assembly kernels, on the host (once per mesh).
-struct HostPattern {
-  std::vector<int32_t> outer, inner;
-  std::vector<int32_t> block_col, block_ptr, block_src, node_ptr, node_src;
-  std::vector<int64_t> block_value;
-};
-
-int build_pattern(int64_t nn, int64_t ne, const int32_t* conn, HostPattern& hp) {
-  std::vector<int64_t> inc_ptr(static_cast<size_t>(nn) + 1, 0);
-  for (int64_t e = 0; e < ne; ++e)
-    for (int a = 0; a < 8; ++a) {
-      const int32_t n = conn[e * 8 + a];
-      if (n < 0 || n >= nn) return fail(SBK_ERR_MESH, "connectivity names a node out of range");
-      ++inc_ptr[static_cast<size_t>(n) + 1];
-    }
-  for (int64_t n = 0; n < nn; ++n) inc_ptr[n + 1] += inc_ptr[n];
-  // Incidences (node -> e * 8 + a), ascending element order.
-  hp.node_ptr.assign(inc_ptr.begin(), inc_ptr.end());
-  hp.node_src.assign(static_cast<size_t>(ne) * 8, 0);
-  {
-    std::vector<int64_t> fill(inc_ptr.begin(), inc_ptr.end() - 1);
-    for (int64_t e = 0; e < ne; ++e)
-      for (int a = 0; a < 8; ++a) hp.node_src[fill[conn[e * 8 + a]]++] = static_cast<int32_t>(e * 8 + a);
-  }
-  // Sorted neighbourhoods (the node itself included).
-  std::vector<int64_t> nbr_ptr(static_cast<size_t>(nn) + 1, 0);
-  std::vector<int32_t> nbr;
-  nbr.reserve(static_cast<size_t>(nn) * 27);
-  {
-    std::vector<int32_t> marker(static_cast<size_t>(nn), -1), list;
-    for (int64_t b = 0; b < nn; ++b) {
-      list.clear();
-      for (int64_t k = inc_ptr[b]; k < inc_ptr[b + 1]; ++k) {
-        const int32_t* nodes = conn + static_cast<int64_t>(hp.node_src[k] >> 3) * 8;
-        for (int a = 0; a < 8; ++a)
-          if (marker[nodes[a]] != b) {
-            marker[nodes[a]] = static_cast<int32_t>(b);
-            list.push_back(nodes[a]);
-          }
-      }
-      std::sort(list.begin(), list.end());
-      nbr.insert(nbr.end(), list.begin(), list.end());
-      nbr_ptr[b + 1] = static_cast<int64_t>(nbr.size());
-    }
-  }
-  const int64_t n = nn * 3;
-  hp.outer.assign(static_cast<size_t>(n) + 1, 0);
-  int64_t total = 0;
-  for (int64_t b = 0; b < nn; ++b) {
-    const int64_t deg = nbr_ptr[b + 1] - nbr_ptr[b];
-    for (int kb = 0; kb < 3; ++kb) {
-      total += deg * 3;
-      if (total > 0x7fffffffLL) return fail(SBK_ERR_UNSUPPORTED, "the pattern exceeds 2^31 entries (int32 indices)");
-      hp.outer[static_cast<size_t>(b * 3 + kb) + 1] = static_cast<int32_t>(total);
-    }
-  }
-  hp.inner.resize(static_cast<size_t>(total));
-  for (int64_t b = 0; b < nn; ++b)
-    for (int kb = 0; kb < 3; ++kb) {
-      int64_t q = hp.outer[static_cast<size_t>(b * 3 + kb)];
-      for (int64_t k = nbr_ptr[b]; k < nbr_ptr[b + 1]; ++k)
-        for (int ka = 0; ka < 3; ++ka) hp.inner[static_cast<size_t>(q++)] = nbr[k] * 3 + ka;
-    }
-  // Node blocks in CSC order and their element contributions.
-  const int64_t nb = static_cast<int64_t>(nbr.size());
-  hp.block_col.resize(static_cast<size_t>(nb));
-  hp.block_value.resize(static_cast<size_t>(nb));
-  for (int64_t b = 0; b < nn; ++b)
-    for (int64_t k = nbr_ptr[b]; k < nbr_ptr[b + 1]; ++k) {
-      hp.block_col[k] = static_cast<int32_t>(b);
-      hp.block_value[k] = hp.outer[static_cast<size_t>(b * 3)] + 3 * (k - nbr_ptr[b]);
-    }
-  std::vector<int64_t> bcount(static_cast<size_t>(nb) + 1, 0);
-  std::vector<int32_t> where(static_cast<size_t>(ne) * 64);
-  for (int64_t e = 0; e < ne; ++e) {
-    const int32_t* nodes = conn + e * 8;
-    for (int b = 0; b < 8; ++b) {
-      const int32_t* begin = nbr.data() + nbr_ptr[nodes[b]];
-      const int32_t* end = nbr.data() + nbr_ptr[nodes[b] + 1];
-      for (int a = 0; a < 8; ++a) {
-        const int32_t* hit = std::lower_bound(begin, end, nodes[a]);
-        const int64_t blk = (hit - nbr.data());
-        where[e * 64 + a * 8 + b] = static_cast<int32_t>(blk);
-        ++bcount[static_cast<size_t>(blk) + 1];
-      }
-    }
-  }
-  for (int64_t b = 0; b < nb; ++b) bcount[b + 1] += bcount[b];
-  if (bcount[nb] > 0x7fffffffLL) return fail(SBK_ERR_UNSUPPORTED, "too many element blocks for int32 maps");
-  hp.block_ptr.assign(bcount.begin(), bcount.end());
-  hp.block_src.resize(static_cast<size_t>(bcount[nb]));
-  {
-    std::vector<int64_t> fill(bcount.begin(), bcount.end() - 1);
-    for (int64_t e = 0; e < ne; ++e)
-      for (int ab = 0; ab < 64; ++ab) hp.block_src[fill[where[e * 64 + ab]]++] = static_cast<int32_t>(e * 64 + ab);
-  }
-  return SBK_OK;
-}
-
 template <class T>
 int upload(T** dst, const std::vector<T>& src, cudaStream_t s) {
   int rc = dalloc(dst, src.size());
@@ -627,14 +528,6 @@ int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const 
     free_system(s);
     return fail(SBK_ERR_UNSUPPORTED, "too many points");
   }
-  HostPattern hp;
-  rc = build_pattern(s->nn, s->ne, mesh->connectivity, hp);
-  if (rc) {
-    free_system(s);
-    return rc;
-  }
-  s->nnz = static_cast<int64_t>(hp.inner.size());
-  s->num_blocks = static_cast<int64_t>(hp.block_col.size());
   const int64_t npts = s->ne * p.nq;
   const size_t state_size = static_cast<size_t>(npts) * p.nfields;
   std::vector<double> coords(mesh->coords, mesh->coords + 3 * s->nn);
@@ -649,6 +542,22 @@ int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const 
   } while (0)
   TRY(upload(&s->coords, coords, nullptr));
   TRY(upload(&s->conn, conn, nullptr));
+  {
+    // The reference's pattern and the assembly's gather maps, built on the
+    // device from the connectivity (sbk_pattern.cu).
+    sbk::DevicePattern dp;
+    TRY(sbk::build_device_pattern(s->nn, s->ne, s->conn, dp, nullptr));
+    s->outer = dp.outer;
+    s->inner = dp.inner;
+    s->block_col = dp.block_col;
+    s->block_value = dp.block_value;
+    s->block_ptr = dp.block_ptr;
+    s->block_src = dp.block_src;
+    s->node_ptr = dp.node_ptr;
+    s->node_src = dp.node_src;
+    s->nnz = dp.nnz;
+    s->num_blocks = dp.num_blocks;
+  }
   TRY(dalloc(&s->committed, state_size));
   TRY(dalloc(&s->trial, state_size));
   TRY(dalloc(&s->alpha_c, static_cast<size_t>(s->ne) * 9));
@@ -660,8 +569,6 @@ int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const 
   TRY(dalloc(&s->iters, static_cast<size_t>(s->ne)));
   TRY(dalloc(&s->code, static_cast<size_t>(s->ne)));
   TRY(dalloc(&s->first_fail, 1));
-  TRY(upload(&s->outer, hp.outer, nullptr));
-  TRY(upload(&s->inner, hp.inner, nullptr));
   TRY(dalloc(&s->values, static_cast<size_t>(s->nnz)));
   TRY(dalloc(&s->internal, static_cast<size_t>(s->nn) * 3));
   TRY(dalloc(&s->product, static_cast<size_t>(s->nn) * 3));
@@ -670,12 +577,6 @@ int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const 
   TRY(dalloc(&s->scratch, sbk::assemble_scratch_doubles()));
   TRY(dalloc(&s->scalars, 4));
   TRY(dalloc(&s->missing, 1));
-  TRY(upload(&s->block_col, hp.block_col, nullptr));
-  TRY(upload(&s->block_value, hp.block_value, nullptr));
-  TRY(upload(&s->block_ptr, hp.block_ptr, nullptr));
-  TRY(upload(&s->block_src, hp.block_src, nullptr));
-  TRY(upload(&s->node_ptr, hp.node_ptr, nullptr));
-  TRY(upload(&s->node_src, hp.node_src, nullptr));
 #undef TRY
   // Virgin points and zero modes (initialise_history).
   cudaMemset(s->committed, 0, state_size * sizeof(double));

@@ -14,7 +14,9 @@
 // with that device current) by the first call made on it, which should
 // therefore come before any stream capture. Calls share the array: two calls
 // that overlap on the GPU (on different streams) race; calls on one stream
-// are ordered. Each call clears what it accumulates before using it.
+// are ordered. Each call clears what it accumulates before using it, and
+// reads an element's slots only when the element kernel of the same call
+// reported it evaluated (code 0).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -63,10 +65,28 @@ int scratch_address(Scratch** out) {
   return SBK_OK;
 }
 
+// Position of (row, col) in the CSC pattern, or -1 if the pattern lacks it.
+__device__ __forceinline__ int32_t csc_position(const int32_t* __restrict__ outer, const int32_t* __restrict__ inner,
+                                                int32_t row, int32_t col) {
+  int32_t lo = outer[col], hi = outer[col + 1];
+  const int32_t end = hi;
+  while (lo < hi) {
+    const int32_t mid = lo + (hi - lo) / 2;
+    if (inner[mid] < row) lo = mid + 1; else hi = mid;
+  }
+  return (lo < end && inner[lo] == row) ? lo : -1;
+}
+
 // One block: the element tangents and forces added into the CSC values,
 // f_int and the gross sums element by element in element order (the
 // reference's Assembler::scatter order, src/fem/Assembler.cpp:184-215), then
-// the energy (in element order), the yield count and the gross norm.
+// the energy (in element order), the yield count and the gross norm. The
+// element kernel writes code[e] for every element (0: evaluated); a failed
+// element wrote none of its force, tangent, energy or yield flags, so its
+// slots hold an earlier call's values, and it is left out of every sum. An
+// element naming one node twice sends two of its blocks to one CSC entry:
+// such an element is added by one thread, entry after entry in row-major
+// block order, so no addition is lost.
 __global__ void __launch_bounds__(576) scatter_small_kernel(
     int32_t nn, int32_t ne, int nq, const int32_t* __restrict__ conn, const int32_t* __restrict__ outer,
     const int32_t* __restrict__ inner, int64_t nnz, const Scratch* __restrict__ s, double* __restrict__ gross,
@@ -87,30 +107,45 @@ __global__ void __launch_bounds__(576) scatter_small_kernel(
   __syncthreads();
   for (int e = 0; e < ne; ++e) {
     const int32_t* nodes = conn + 8 * (int64_t)e;
-    // An element naming a node out of range (failed by the element kernel)
-    // is left out; a block the caller's pattern lacks is reported.
-    bool inside = true;
+    // A failed element (a node out of range among the reasons) is left out;
+    // a block the caller's pattern lacks is reported. Both tests give the
+    // same answer in every thread.
+    if (s->code[e] != 0) continue;
+    bool repeated = false;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) inside = inside && nodes[k] >= 0 && nodes[k] < nn;
-    if (!inside) continue;  // the same for every thread
-    if (values) {
-      const int32_t row = 3 * nodes[a] + ka, col = 3 * nodes[b] + kb;
-      int32_t lo = outer[col], hi = outer[col + 1];
-      const int32_t end = hi;
-      while (lo < hi) {
-        const int32_t mid = lo + (hi - lo) / 2;
-        if (inner[mid] < row) lo = mid + 1; else hi = mid;
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = i + 1; j < 8; ++j) repeated = repeated || nodes[i] == nodes[j];
+    if (!repeated) {
+      if (values) {
+        const int32_t pos = csc_position(outer, inner, 3 * nodes[a] + ka, 3 * nodes[b] + kb);
+        if (pos >= 0)
+          values[pos] += s->tangent[(int64_t)e * 576 + (8 * a + b) * 9 + 3 * ka + kb];
+        else
+          mismatch = 1;
       }
-      if (lo < end && inner[lo] == row)
-        values[lo] += s->tangent[(int64_t)e * 576 + (8 * a + b) * 9 + 3 * ka + kb];
-      else
-        mismatch = 1;
-    }
-    if (t < 24) {
-      const int32_t dof = 3 * nodes[t / 3] + t % 3;
-      const double f = s->force[(int64_t)e * 24 + t];
-      internal[dof] += f;
-      gross[dof] += fabs(f);
+      if (t < 24) {
+        const int32_t dof = 3 * nodes[t / 3] + t % 3;
+        const double f = s->force[(int64_t)e * 24 + t];
+        internal[dof] += f;
+        gross[dof] += fabs(f);
+      }
+    } else if (t == 0) {
+      for (int i = 0; i < 576 && values; ++i) {
+        const int ra = i / 24, cb = i % 24;
+        const int aa = ra / 3, kka = ra % 3, bb = cb / 3, kkb = cb % 3;
+        const int32_t pos = csc_position(outer, inner, 3 * nodes[aa] + kka, 3 * nodes[bb] + kkb);
+        if (pos >= 0)
+          values[pos] += s->tangent[(int64_t)e * 576 + (8 * aa + bb) * 9 + 3 * kka + kkb];
+        else
+          mismatch = 1;
+      }
+      for (int i = 0; i < 24; ++i) {
+        const int32_t dof = 3 * nodes[i / 3] + i % 3;
+        const double f = s->force[(int64_t)e * 24 + i];
+        internal[dof] += f;
+        gross[dof] += fabs(f);
+      }
     }
     __syncthreads();
   }
@@ -126,6 +161,7 @@ __global__ void __launch_bounds__(576) scatter_small_kernel(
     double en = 0.0;
     int64_t y = 0;
     for (int e = 0; e < ne; ++e) {
+      if (s->code[e] != 0) continue;
       en += s->energy[e];
       for (int q = 0; q < nq; ++q) y += yield[(int64_t)e * nq + q];
     }

@@ -127,15 +127,34 @@ def evaluate_noalloc(material: Material, coords: torch.Tensor, connectivity: tor
     memory; every buffer is the caller's (device tensors), the library
     allocates nothing. Results land in the given tensors on `stream`;
     summary (5 doubles): energy, gross, yielding points, lowest failing
-    element (-1: none), its code."""
+    element (-1: none), its code. The tensors must all live on one CUDA
+    device (the call runs with it current), be contiguous and have the C
+    ABI's types: float64 for the coordinates, displacements, states, modes
+    and outputs, int32 for the connectivity and the pattern, uint8 for the
+    yield flags."""
+    f64 = {"coords": coords, "u": u, "state": state, "alpha": alpha, "internal": internal, "values": values,
+           "trial": trial, "alpha_out": alpha_out, "summary": summary}
+    i32 = {"connectivity": connectivity, "outer": outer, "inner": inner}
+    dev = coords.device
+    for group, dtype in ((f64, torch.float64), (i32, torch.int32), ({"yielding": yielding}, torch.uint8)):
+        for name, t in group.items():
+            if t is None:
+                continue
+            if t.dtype != dtype:
+                raise TypeError(f"evaluate_noalloc: {name} is {t.dtype}, expected {dtype}")
+            if t.device != dev or t.device.type != "cuda":
+                raise ValueError(f"evaluate_noalloc: {name} is on {t.device}, expected the CUDA device {dev}")
+            if not t.is_contiguous():
+                raise ValueError(f"evaluate_noalloc: {name} is not contiguous")
     mat = material.to_c()
     rule = rule_c(stiffness_points, thickness_points, thickness_axis)
-    st = _capi.lib().sbk_evaluate_noalloc(
-        ctypes.byref(mat), ctypes.byref(rule), _capi.KINEMATICS[kinematics], int(coords.numel() // 3),
-        int(connectivity.numel() // 8), _ptr(coords), _ptr(connectivity), _ptr(u), _ptr(state),
-        _ptr(alpha) if alpha is not None else None, _ptr(outer), _ptr(inner), int(inner.numel()), _ptr(internal),
-        _ptr(values) if values is not None else None, _ptr(trial), _ptr(alpha_out), _ptr(yielding), _ptr(summary),
-        _stream_ptr(stream))
+    with torch.cuda.device(dev):
+        st = _capi.lib().sbk_evaluate_noalloc(
+            ctypes.byref(mat), ctypes.byref(rule), _capi.KINEMATICS[kinematics], int(coords.numel() // 3),
+            int(connectivity.numel() // 8), _ptr(coords), _ptr(connectivity), _ptr(u), _ptr(state),
+            _ptr(alpha) if alpha is not None else None, _ptr(outer), _ptr(inner), int(inner.numel()),
+            _ptr(internal), _ptr(values) if values is not None else None, _ptr(trial), _ptr(alpha_out),
+            _ptr(yielding), _ptr(summary), _stream_ptr(stream))
     _capi.check(st)
 
 

@@ -86,6 +86,13 @@ class StepResult:
     u: np.ndarray
     increments: int
     tool_fz: list
+    # The step-end element fields the reference writes
+    # (step_<k>_<s>_elements.csv): the largest equivalent plastic strain of
+    # each element's points and the von Mises stress of its point-averaged
+    # Cauchy stress, from the package's stress recovery at the end of the step
+    # (Forming.cpp:1266-1281).
+    eq_plastic_strain: np.ndarray = None
+    von_mises: np.ndarray = None
 
 
 class FormingRun:
@@ -223,7 +230,7 @@ class FormingRun:
                 t = t1
             assert t == te, (t, te)
             self.t = te
-            return StepResult(u=self.u.copy(), increments=len(times), tool_fz=fz_list)
+            return self._step_end(StepResult(u=self.u.copy(), increments=len(times), tool_fz=fz_list))
         while True:
             station = next(s for s in stations if s > t)
             h = min(dt, dt_max)
@@ -240,7 +247,15 @@ class FormingRun:
             if s1 >= 1.0:
                 break
         self.t = te
-        return StepResult(u=self.u.copy(), increments=count, tool_fz=fz_list)
+        return self._step_end(StepResult(u=self.u.copy(), increments=count, tool_fz=fz_list))
+
+    def _step_end(self, res: StepResult) -> StepResult:
+        """The step-end stress recovery of every element at the converged
+        displacement and the committed history."""
+        st = self.system.stress(torch.tensor(self.u, device=self.dev))
+        res.eq_plastic_strain = st.max_plastic_strain.cpu().numpy()
+        res.von_mises = st.von_mises.cpu().numpy()
+        return res
 
     def _newton(self, t0, t1, s1, free, r0, active):
         """One increment: Newton's method as Forming.cpp:900-1135 runs it -

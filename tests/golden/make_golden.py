@@ -14,14 +14,16 @@ the mesh, the parts of its deck the element loop and the contact read
 (material, model and element formulation, mean dilatation, kinematics,
 tool, steps and their boundary regions), the nodal
 displacements at the end of each step (17 significant digits in the
-reference's CSV output) and the tool force of every forming increment.
+reference's CSV output), the step-end element fields (largest equivalent
+plastic strain of the element's points, von Mises stress of its averaged
+Cauchy stress) and the tool force of every forming increment.
 
 kin_h0833.json + kin_h0833.npz: the reference's forming run
 benchmarks/physics_audit/challenge/cases/kin_h0833 - a 48 x 48 x 1
 incompatible-mode sheet with the 2 x 2 x 5 rule, Hill48 with two Chaboche
 backstresses and Voce hardening, a spherical tool on a 113-knot spiral
 path - the deck's parts in the JSON (the tool path read from its CSV), the
-mesh and the step-end displacements in the npz.
+mesh, the step-end displacements and element fields in the npz.
 
 materials.json: the hardening parameters the reference's own Python
 (python/precomp/materials.py) derives - its built-in library (Hollomon
@@ -75,7 +77,8 @@ def strip(ref_root: str, case: str = "strip_h2_im_nz4") -> None:
         rows = list(csv.DictReader(open(os.path.join(base, "out", f"step_{k}_{st['name']}_nodes.csv"))))
         steps.append({"deck": st, "u": [[float(r["ux"]), float(r["uy"]), float(r["uz"])] for r in rows],
                       "increments": summary["steps"][k - 1]["increments"],
-                      "cuts": summary["steps"][k - 1]["cuts"]})
+                      "cuts": summary["steps"][k - 1]["cuts"],
+                      "elements": element_fields(os.path.join(base, "out"), k, st["name"])})
     forces = [{k: r[k] for k in ("step", "increment", "t", "cx", "cz", "fx", "fz", "active_nodes")}
               for r in csv.DictReader(open(os.path.join(base, "out", "tool_forces.csv")))]
     out = {"source": os.path.relpath(base, ref_root), "nodes": mesh["nodes_m"], "elements": mesh["elements"],
@@ -87,6 +90,18 @@ def strip(ref_root: str, case: str = "strip_h2_im_nz4") -> None:
     with open(os.path.join(HERE, f"{case}.json"), "w") as f:
         json.dump(out, f, separators=(",", ":"))
         f.write("\n")
+
+
+def element_fields(out_dir: str, k: int, name: str) -> dict:
+    """The step-end element fields the reference writes
+    (step_<k>_<s>_elements.csv: element, eq_plastic_strain, von_mises_Pa;
+    include/sparlab/io/FormingWriter.hpp:1-12), in element order."""
+    import csv
+
+    rows = list(csv.DictReader(open(os.path.join(out_dir, f"step_{k}_{name}_elements.csv"))))
+    assert [int(r["element"]) for r in rows] == list(range(len(rows)))
+    return {"eq_plastic_strain": [float(r["eq_plastic_strain"]) for r in rows],
+            "von_mises_Pa": [float(r["von_mises_Pa"]) for r in rows]}
 
 
 def challenge(ref_root: str, case: str = "kin_h0833") -> None:
@@ -107,10 +122,13 @@ def challenge(ref_root: str, case: str = "kin_h0833") -> None:
             t["trajectory"] = {"times": [float(r["t"]) for r in rows],
                                "points": [[float(r["x"]), float(r["y"]), float(r["z"])] for r in rows]}
         tools.append(t)
-    steps, us = [], []
+    steps, us, eqps, vm = [], [], [], []
     for k, st in enumerate(deck["forming"]["steps"], start=1):
         rows = list(csv.DictReader(open(os.path.join(base, "output", f"step_{k}_{st['name']}_nodes.csv"))))
         us.append([[float(r["ux"]), float(r["uy"]), float(r["uz"])] for r in rows])
+        fields = element_fields(os.path.join(base, "output"), k, st["name"])
+        eqps.append(fields["eq_plastic_strain"])
+        vm.append(fields["von_mises_Pa"])
         steps.append({"deck": st, "increments": summary["steps"][k - 1]["increments"],
                       "cuts": summary["steps"][k - 1]["cuts"]})
     forces = [{k: r[k] for k in ("step", "increment", "t", "cx", "cz", "fx", "fz", "active_nodes")}
@@ -122,11 +140,14 @@ def challenge(ref_root: str, case: str = "kin_h0833") -> None:
         json.dump(out, f, separators=(",", ":"))
         f.write("\n")
     np.savez_compressed(os.path.join(HERE, f"{case}.npz"), nodes=np.array(mesh["nodes_m"], dtype=np.float64),
-                        elements=np.array(mesh["elements"], dtype=np.int32), u=np.array(us, dtype=np.float64))
+                        elements=np.array(mesh["elements"], dtype=np.int32), u=np.array(us, dtype=np.float64),
+                        eq_plastic_strain=np.array(eqps, dtype=np.float64), von_mises=np.array(vm, dtype=np.float64))
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <root of the reference's checkout>")
+    root = sys.argv[1]
     main(root)
     for case in ("strip_h2_im_nz4", "strip_h1_im_nz4", "plate_h2_im_mu0.1_drag3", "strip_h2_std_mu0.1",
                  "plate_h2_std_mu0.1_drag3", "strip_h2_nobbar_mu0.1"):

@@ -54,6 +54,7 @@ def load_fixture(case):
         fx["nodes"], fx["elements"] = a["nodes"], a["elements"]
         for k, st in enumerate(fx["steps"]):
             st["u"] = a["u"][k]
+            st["elements"] = {"eq_plastic_strain": a["eq_plastic_strain"][k], "von_mises_Pa": a["von_mises"][k]}
     return fx
 
 
@@ -88,3 +89,31 @@ def test_tool_force_history_matches_the_reference(run):
     got = np.array(results[0].tool_fz)
     assert len(got) == len(ref)
     assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
+
+
+# Step-end element fields: the von Mises stress within 1e-9 of the largest
+# in the step, the largest equivalent plastic strain within 1e-10 (absolute;
+# the fields are O(0.1) at most).
+VM_TOL = 1.0e-9
+EQPS_TOL = 1.0e-10
+
+
+@pytest.mark.parametrize("k,name", [(0, "form"), (1, "unload"), (2, "release")])
+def test_step_element_fields_match_the_reference(run, k, name):
+    """The step-end stress recovery (elastoplastic_stress of every element,
+    IncompatibleModes.cpp:602-664 / Elastoplastic.cpp:342-430, called at
+    Forming.cpp:1266-1281) against the element fields the reference wrote
+    for the same step (step_<k>_<s>_elements.csv: eq_plastic_strain,
+    von_mises_Pa)."""
+    fx, results = run
+    ref = fx["steps"][k]["elements"]
+    vm_ref = np.asarray(ref["von_mises_Pa"], dtype=np.float64)
+    ep_ref = np.asarray(ref["eq_plastic_strain"], dtype=np.float64)
+    vm, ep = results[k].von_mises, results[k].eq_plastic_strain
+    assert vm.shape == vm_ref.shape and ep.shape == ep_ref.shape
+    vm_err = np.abs(vm - vm_ref).max() / np.abs(vm_ref).max()
+    ep_err = np.abs(ep - ep_ref).max()
+    print(f"{name}: von Mises rel. {vm_err:.2e} (largest {np.abs(vm_ref).max():.4e} Pa), eq. plastic strain "
+          f"{ep_err:.2e} (largest {ep_ref.max():.4e})")
+    assert vm_err <= VM_TOL, vm_err
+    assert ep_err <= EQPS_TOL, ep_err

@@ -84,29 +84,116 @@ def test_noalloc_refuses_a_mesh_beyond_its_maximum(pkg, cuda):
     assert err.value.status == 6 and "2048" in str(err.value)
 
 
-def test_noalloc_fails_an_element_naming_a_node_out_of_range(pkg, cuda):
-    """The caller's device connectivity is not checked on the host: an
-    element naming a node out of range fails (SBK_EL_BAD_NODE) before
-    anything of it is read, and the sums leave it out."""
+def _buffers(mesh, state, alpha, nnz, cuda):
+    internal = torch.empty(mesh.num_dofs, dtype=torch.float64, device=cuda)
+    values = torch.empty(nnz, dtype=torch.float64, device=cuda)
+    trial = torch.empty_like(state)
+    alpha_out = torch.empty_like(alpha)
+    summary = torch.empty(5, dtype=torch.float64, device=cuda)
+    return internal, values, trial, alpha_out, summary
+
+
+def _dense(values, outer, inner, n):
+    import scipy.sparse as sp
+    return sp.csc_matrix((values, inner, outer), shape=(n, n)).toarray()
+
+
+@pytest.mark.parametrize("bad", ["node_out_of_range", "repeated_node"])
+def test_noalloc_leaves_a_failed_element_out_of_the_sums(pkg, cuda, bad):
+    """A failed element is left out of every sum even though the shared
+    scratch still holds an earlier call's values in its slots: a good call
+    first fills the scratch, then element 5 fails - by naming a node out of
+    range (SBK_EL_BAD_NODE before anything of it is read), or by naming one
+    node twice, which collapses it (SBK_EL_MESH_INVERTED) - and the sums must
+    equal the allocating path's on the mesh without element 5. The caller's
+    yield bytes of the failed element are garbage and must not count."""
     wl = importlib.import_module("springback-precomp_b200.workload")
     system = importlib.import_module("springback-precomp_b200.system")
+    mesh_mod = importlib.import_module("springback-precomp_b200.mesh")
     prob = wl.make_problem(6, 4, 1, seed=3, sample=24)
     mesh, mat = prob.mesh, prob.material
     sysm = pkg.NonlinearSystem(mesh, mat, kinematics="logarithmic")
     u = torch.tensor(prob.u, device=cuda)
     coords = torch.tensor(mesh.coords, device=cuda)
     conn = torch.tensor(mesh.connectivity, device=cuda)
-    conn[5, 3] = mesh.num_nodes  # one past the last node
     state = torch.tensor(prob.state, device=cuda)
     alpha = torch.tensor(prob.alpha, device=cuda)
-    internal = torch.empty(mesh.num_dofs, dtype=torch.float64, device=cuda)
-    values = torch.empty(sysm.nnz, dtype=torch.float64, device=cuda)
-    trial = torch.empty_like(state)
-    alpha_out = torch.empty_like(alpha)
+    outer, inner = sysm.outer.clone(), sysm.inner.clone()
+    internal, values, trial, alpha_out, summary = _buffers(mesh, state, alpha, sysm.nnz, cuda)
     yielding = torch.zeros((mesh.num_elements, 8), dtype=torch.uint8, device=cuda)
-    summary = torch.empty(5, dtype=torch.float64, device=cuda)
-    system.evaluate_noalloc(mat, coords, conn, u, state, alpha, sysm.outer.clone(), sysm.inner.clone(), internal,
-                            values, trial, alpha_out, yielding, summary)
+    system.evaluate_noalloc(mat, coords, conn, u, state, alpha, outer, inner, internal, values, trial, alpha_out,
+                            yielding, summary)
+    torch.cuda.synchronize()
+    assert summary[3].item() == -1.0
+
+    if bad == "node_out_of_range":
+        conn[5, 3] = mesh.num_nodes  # one past the last node
+        expected_code = 9  # SBK_EL_BAD_NODE
+    else:
+        conn[5, 3] = conn[5, 0]
+        expected_code = None
+    yielding.fill_(1)  # what the caller's buffer held before: must not be counted for element 5
+    system.evaluate_noalloc(mat, coords, conn, u, state, alpha, outer, inner, internal, values, trial, alpha_out,
+                            yielding, summary)
     torch.cuda.synchronize()
     s = summary.cpu().numpy()
-    assert s[3] == 5.0 and int(s[4]) == 9, s
+    assert s[3] == 5.0, s
+    if expected_code is not None:
+        assert int(s[4]) == expected_code, s
+    else:
+        assert int(s[4]) != 0, s
+
+    # The allocating path on the mesh without element 5.
+    keep = np.array([e for e in range(mesh.num_elements) if e != 5])
+    sub = mesh_mod.HexMesh(mesh.coords, np.ascontiguousarray(mesh.connectivity[keep]))
+    ref = pkg.NonlinearSystem(sub, mat, kinematics="logarithmic")
+    ref.set_committed(np.ascontiguousarray(prob.state[:, keep, :]))
+    ref.set_internal(np.ascontiguousarray(prob.alpha[keep]))
+    ev = ref.evaluate(u, 0.0, True)
+    torch.cuda.synchronize()
+    tol = 1e-11
+    assert abs(s[0] - ev.energy) <= tol * abs(ev.energy), (s[0], ev.energy)
+    assert abs(s[1] - ev.gross) <= tol * ev.gross, (s[1], ev.gross)
+    assert int(s[2]) == ev.yielding_points + 0, (s[2], ev.yielding_points)
+    assert torch.linalg.norm(internal - ev.internal) <= tol * ev.gross
+    n = mesh.num_dofs
+    got = _dense(values.cpu().numpy(), outer.cpu().numpy(), inner.cpu().numpy(), n)
+    want = _dense(ev.tangent.cpu().numpy(), ref.outer.cpu().numpy(), ref.inner.cpu().numpy(), n)
+    assert np.linalg.norm(got - want) <= tol * np.linalg.norm(want)
+
+
+def test_noalloc_adds_both_blocks_of_an_element_naming_a_node_twice(pkg, cuda):
+    """An element whose connectivity names a node twice - a hexahedron with
+    one vertical edge collapsed into its neighbour, a wedge that still
+    evaluates - sends two of its blocks to one CSC entry and two of its
+    force rows to one DOF: both contributions must count, as in the
+    allocating path on the same connectivity."""
+    wl = importlib.import_module("springback-precomp_b200.workload")
+    system = importlib.import_module("springback-precomp_b200.system")
+    mesh_mod = importlib.import_module("springback-precomp_b200.mesh")
+    prob = wl.make_problem(4, 2, 1, seed=7, sample=8)
+    conn = prob.mesh.connectivity.copy()
+    conn[0, 3] = conn[0, 2]  # corner 3 onto corner 2 (bottom face)
+    conn[0, 7] = conn[0, 6]  # and its top twin
+    mesh = mesh_mod.HexMesh(prob.mesh.coords, conn)
+    mat = prob.material
+    sysm = pkg.NonlinearSystem(mesh, mat, kinematics="logarithmic")
+    sysm.set_committed(prob.state)
+    sysm.set_internal(prob.alpha)
+    u = torch.tensor(prob.u, device=cuda)
+    ev = sysm.evaluate(u, 0.0, True)
+    torch.cuda.synchronize()
+    state = torch.tensor(prob.state, device=cuda)
+    alpha = torch.tensor(prob.alpha, device=cuda)
+    internal, values, trial, alpha_out, summary = _buffers(mesh, state, alpha, sysm.nnz, cuda)
+    yielding = torch.zeros((mesh.num_elements, 8), dtype=torch.uint8, device=cuda)
+    outer, inner = sysm.outer.clone(), sysm.inner.clone()
+    system.evaluate_noalloc(mat, torch.tensor(mesh.coords, device=cuda), torch.tensor(conn, device=cuda), u, state,
+                            alpha, outer, inner, internal, values, trial, alpha_out, yielding, summary)
+    torch.cuda.synchronize()
+    s = summary.cpu().numpy()
+    assert s[3] == -1.0, s
+    tol = 1e-11
+    assert torch.linalg.norm(internal - ev.internal) <= tol * ev.gross
+    assert torch.linalg.norm(values - ev.tangent) <= tol * torch.linalg.norm(ev.tangent)
+    assert abs(s[1] - ev.gross) <= tol * ev.gross
