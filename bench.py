@@ -655,6 +655,8 @@ def main():
     p.add_argument("--ref-ny", type=int, default=160)
     p.add_argument("--cpu-steps", type=int, default=5, help="timed steps of the in-run CPU baseline")
     p.add_argument("--epb", type=int, default=0, help="elements per block of the element kernel (0: default)")
+    p.add_argument("--local-iteration", default="phases", choices=["phases", "single"],
+                   help="the local iteration as phase kernels over the mesh (default) or one kernel per element")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--workload", default="microbench", choices=["microbench", "batched", "partition", "adjoint"],
@@ -709,6 +711,7 @@ def main():
         sysm.set_element("standard", "auto")
     if args.epb:
         sysm.set_elements_per_block(args.epb)
+    sysm.set_local_iteration(args.local_iteration)
     sysm.set_timing(True)
     setup_s = time.perf_counter() - t_setup
 

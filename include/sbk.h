@@ -165,6 +165,23 @@ int sbk_system_element(const sbk_system* sys, int* element, int* averaged);
  * hold; the batch autotuner sets it). */
 int sbk_system_set_elements_per_block(sbk_system* sys, int elements_per_block);
 
+/* How the incompatible-mode Hex8's local iteration runs on the GPU (no
+ * counterpart in the reference; no result depends on it - both give the
+ * same outputs to the bit). SBK_LOCAL_PHASES (the default): phase kernels
+ * over the whole mesh - each round a pass over the elements still
+ * iterating, then their element-level step - with the elements that need a
+ * line search, the shifted direction or Levenberg-Marquardt handed to the
+ * single kernel; rules of up to 8 points (the others always take the single
+ * kernel). SBK_LOCAL_SINGLE_KERNEL: one kernel runs each element from start
+ * to finish. The phase kernels keep per-element records on the device
+ * (about 6.7 KB per element, allocated by the system when it is made or its
+ * element changes). sbk_set_local_iteration sets what sbk_element_batch
+ * uses and what new systems start with. */
+#define SBK_LOCAL_PHASES 0
+#define SBK_LOCAL_SINGLE_KERNEL 1
+int sbk_set_local_iteration(int mode);
+int sbk_system_set_local_iteration(sbk_system* sys, int mode);
+
 /* The element schedule (no counterpart in the reference, whose OpenMP loop
  * takes the elements in mesh order): with by_cost = 1 (the default) every
  * evaluate after the first walks the elements grouped by the cost of their

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -404,6 +405,9 @@ struct sbk_system {
   bool has_trial = false;
   bool has_values = false;  // values hold the tangent of the last evaluate
   bool timing = false;
+  int local_mode = SBK_LOCAL_PHASES;
+  void* wave_mem = nullptr;  // the phase kernels' records (one allocation)
+  sbk::WaveBuffers wave{};
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   double last_ms[3] = {0.0, 0.0, 0.0};
 
@@ -431,12 +435,41 @@ void free_system(sbk_system* s) {
                   s->tangent, s->energy_e, s->yield, s->iters, s->code, s->first_fail, s->outer,
                   s->inner, s->values, s->internal, s->scratch, s->scalars, s->missing, s->block_col,
                   s->block_value, s->block_ptr, s->block_src, s->node_ptr, s->node_src, s->product,
-                  s->order, s->sched};
+                  s->order, s->sched, s->wave_mem};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (cudaEvent_t e : s->ev)
     if (e) cudaEventDestroy(e);
   delete s;
+}
+
+std::atomic<int> g_local_mode{SBK_LOCAL_PHASES};
+
+// The phase kernels' records of a system whose element takes them
+// (allocated once, outside any stream capture).
+int ensure_wave(sbk_system* s) {
+  if (s->wave_mem || !sbk::wave_applies(s->p)) return SBK_OK;
+  const size_t bytes = sbk::wave_buffer_bytes(s->ne);
+  cudaError_t e = cudaMalloc(&s->wave_mem, bytes);
+  if (e != cudaSuccess) {
+    s->wave_mem = nullptr;
+    return fail(SBK_ERR_CUDA, std::string("cudaMalloc (local-iteration records): ") + cudaGetErrorString(e));
+  }
+  sbk::wave_buffers_carve(s->wave_mem, s->ne, s->wave);
+  return SBK_OK;
+}
+
+// K1 of a system: the phase kernels where they apply, else the single kernel.
+int system_elements(sbk_system* sys, const double* u_dev, int want_tangent, cudaStream_t st) {
+  const int32_t* order = sys->schedule && sys->order_valid ? sys->order : nullptr;
+  if (sys->local_mode == SBK_LOCAL_PHASES && sys->wave_mem && sbk::wave_applies(sys->p))
+    return sbk::launch_elements_wave(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c,
+                                     want_tangent, sys->force, sys->tangent, sys->energy_e, sys->trial, sys->alpha_t,
+                                     sys->yield, sys->iters, sys->code, sys->first_fail, false, order, sys->wave, st);
+  return sbk::launch_elements(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c,
+                              want_tangent, sys->force, sys->tangent, sys->energy_e, sys->trial, sys->alpha_t,
+                              sys->yield, sys->iters, sys->code, sys->first_fail, false, sys->elements_per_block, order,
+                              st);
 }
 
 template <class T>
@@ -499,6 +532,20 @@ int sbk_element_batch(const sbk_material* material, const sbk_rule* rule, int ki
     return fail(SBK_ERR_ARGUMENT, "null device buffer");
   if (ne * p.nq > 0x7fffffffLL) return fail(SBK_ERR_UNSUPPORTED, "too many points for one batch");
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (g_local_mode.load() == SBK_LOCAL_PHASES && sbk::wave_applies(p)) {
+    // The phase kernels' records, stream-ordered on the caller's stream.
+    void* mem = nullptr;
+    SBK_CUDA(cudaMallocAsync(&mem, sbk::wave_buffer_bytes(ne), s));
+    sbk::WaveBuffers w;
+    sbk::wave_buffers_carve(mem, ne, w);
+    rc = sbk::launch_elements_wave(p, ne, x_dev, nullptr, u_dev, state_dev, alpha_dev, tangent_dev != nullptr,
+                                   force_dev, tangent_dev, energy_dev, trial_dev, alpha_out_dev, yield_dev,
+                                   iterations_dev, code_dev, nullptr, true, nullptr, w, s);
+    cudaError_t e = cudaFreeAsync(mem, s);
+    if (rc) return fail(SBK_ERR_CUDA, std::string("element kernels: ") + cudaGetErrorString((cudaError_t)rc));
+    if (e != cudaSuccess) return fail(SBK_ERR_CUDA, std::string("cudaFreeAsync: ") + cudaGetErrorString(e));
+    return SBK_OK;
+  }
   rc = sbk::launch_elements(p, ne, x_dev, nullptr, u_dev, state_dev, alpha_dev, tangent_dev != nullptr, force_dev,
                             tangent_dev, energy_dev, trial_dev, alpha_out_dev, yield_dev, iterations_dev, code_dev,
                             nullptr, true, 0, nullptr, s);
@@ -577,6 +624,8 @@ int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const 
   TRY(dalloc(&s->scratch, sbk::assemble_scratch_doubles()));
   TRY(dalloc(&s->scalars, 4));
   TRY(dalloc(&s->missing, 1));
+  s->local_mode = g_local_mode.load();
+  TRY(ensure_wave(s));
 #undef TRY
   // Virgin points and zero modes (initialise_history).
   cudaMemset(s->committed, 0, state_size * sizeof(double));
@@ -628,7 +677,11 @@ int sbk_system_set_element(sbk_system* sys, int element, int mean_dilatation) {
                         ? 1
                         : 0;
   sys->order_valid = false;
-  return SBK_OK;
+  if (!sbk::wave_applies(sys->p) && sys->wave_mem) {
+    cudaFree(sys->wave_mem);
+    sys->wave_mem = nullptr;
+  }
+  return sys->local_mode == SBK_LOCAL_PHASES ? ensure_wave(sys) : SBK_OK;
 }
 
 int sbk_system_set_frozen(sbk_system* sys, int frozen) {
@@ -652,6 +705,19 @@ int sbk_system_element(const sbk_system* sys, int* element, int* averaged) {
   if (element) *element = sys->p.element ? SBK_ELEMENT_STANDARD : SBK_ELEMENT_INCOMPATIBLE_MODES;
   if (averaged) *averaged = sys->p.averaged;
   return SBK_OK;
+}
+
+int sbk_set_local_iteration(int mode) {
+  if (mode != SBK_LOCAL_PHASES && mode != SBK_LOCAL_SINGLE_KERNEL) return fail(SBK_ERR_ARGUMENT, "unknown mode");
+  g_local_mode.store(mode);
+  return SBK_OK;
+}
+
+int sbk_system_set_local_iteration(sbk_system* sys, int mode) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  if (mode != SBK_LOCAL_PHASES && mode != SBK_LOCAL_SINGLE_KERNEL) return fail(SBK_ERR_ARGUMENT, "unknown mode");
+  sys->local_mode = mode;
+  return mode == SBK_LOCAL_PHASES ? ensure_wave(sys) : SBK_OK;
 }
 
 int sbk_system_set_elements_per_block(sbk_system* sys, int epb) {
@@ -678,11 +744,7 @@ int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int
   out->failed_element = -1;
   SBK_CUDA(cudaMemsetAsync(sys->first_fail, 0x7f, sizeof(int32_t), st));
   if (sys->timing) SBK_CUDA(cudaEventRecord(sys->ev[0], st));
-  int rc = sbk::launch_elements(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c,
-                                want_tangent, sys->force, sys->tangent, sys->energy_e, sys->trial, sys->alpha_t,
-                                sys->yield, sys->iters, sys->code, sys->first_fail, false,
-                                sys->elements_per_block, sys->schedule && sys->order_valid ? sys->order : nullptr,
-                                st);
+  int rc = system_elements(sys, u_dev, want_tangent, st);
   if (rc) return fail(SBK_ERR_CUDA, std::string("element kernel: ") + cudaGetErrorString((cudaError_t)rc));
   if (sys->timing) SBK_CUDA(cudaEventRecord(sys->ev[1], st));
   // The assembly runs unconditionally; a failed element is reported after
@@ -778,11 +840,7 @@ int sbk_system_enqueue(sbk_system* sys, const double* u_dev, int want_tangent, d
   if (!sys || !u_dev || !summary_dev) return fail(SBK_ERR_ARGUMENT, "null argument");
   cudaStream_t st = sys->stream;
   SBK_CUDA(cudaMemsetAsync(sys->first_fail, 0x7f, sizeof(int32_t), st));
-  int rc = sbk::launch_elements(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c,
-                                want_tangent, sys->force, sys->tangent, sys->energy_e, sys->trial, sys->alpha_t,
-                                sys->yield, sys->iters, sys->code, sys->first_fail, false,
-                                sys->elements_per_block, sys->schedule && sys->order_valid ? sys->order : nullptr,
-                                st);
+  int rc = system_elements(sys, u_dev, want_tangent, st);
   if (rc) return fail(SBK_ERR_CUDA, std::string("element kernel: ") + cudaGetErrorString((cudaError_t)rc));
   rc = sbk::launch_assemble_forces(sys->maps(), sys->force, sys->energy_e, sys->yield, sys->p.nq, sys->internal,
                                    sys->scratch, sys->scalars, st);

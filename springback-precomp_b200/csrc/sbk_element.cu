@@ -189,10 +189,13 @@ __device__ __forceinline__ void vtensor(const double* slot, const double g[3], b
   }
 }
 
-template <int G>
+// The per-element context of a group: S is the shared-memory record of one
+// element, which differs between the single element kernel and the phase
+// kernels (each holds only the fields its stage reads).
+template <int G, class Rec = ElemShared<G>>
 struct Ctx {
   const Params* p;
-  ElemShared<G>* s;
+  Rec* s;
   int lane;
   unsigned mask;
   int64_t e;
@@ -206,8 +209,8 @@ struct Ctx {
 };
 
 // Mode gradients of point q: g~(i, m) = (det0 / det)(-2 xi_m) J0^-1(m, i).
-template <int G>
-__device__ __forceinline__ void mode_grads(const Ctx<G>& c, int q, double gt[9]) {
+template <int G, class Rec>
+__device__ __forceinline__ void mode_grads(const Ctx<G, Rec>& c, int q, double gt[9]) {
   const double ratio = c.s->geo[q][10];
   const double nat[3] = {c.p->qp[q][0], c.p->qp[q][1], c.p->qp[q][2]};
 #pragma unroll
@@ -218,8 +221,8 @@ __device__ __forceinline__ void mode_grads(const Ctx<G>& c, int q, double gt[9])
   }
 }
 // Gradient of node a at point q: g(i) = sum_c dN_a/dxi_c J^-1(c, i).
-template <int G>
-__device__ __forceinline__ void node_grad(const Ctx<G>& c, int q, int a, double g[3]) {
+template <int G, class Rec>
+__device__ __forceinline__ void node_grad(const Ctx<G, Rec>& c, int q, int a, double g[3]) {
   double dn[3];
   shape_grad(a, c.p->qp[q][0], c.p->qp[q][1], c.p->qp[q][2], dn);
   const double* ji = c.s->geo[q];
@@ -229,9 +232,9 @@ __device__ __forceinline__ void node_grad(const Ctx<G>& c, int q, int a, double 
 
 // Reference geometry (set_up, IncompatibleModes.cpp:134-192). Returns 0 or
 // SBK_EL_MESH_INVERTED (group-uniform).
-template <int G>
-__device__ int set_up(const Ctx<G>& c) {
-  ElemShared<G>& s = *c.s;
+template <int G, class Rec>
+__device__ int set_up(const Ctx<G, Rec>& c) {
+  Rec& s = *c.s;
   const Params& p = *c.p;
   // Centre Jacobian, every lane alike.
   double j0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -293,9 +296,9 @@ __device__ int set_up(const Ctx<G>& c) {
 // One pass (IncompatibleModes.cpp:337-342): the kinematics, the returns and
 // the sums at `at` (9 values, identical in every lane). Returns 0 or the
 // failure code of the first failing point in the reference's order.
-template <int G>
-__device__ __noinline__ int pass(const Ctx<G>& c, const double at[9]) {
-  ElemShared<G>& s = *c.s;
+template <int G, class Rec>
+__device__ __noinline__ int pass(const Ctx<G, Rec>& c, const double at[9]) {
+  Rec& s = *c.s;
   const Params& p = *c.p;
   const int q = c.lane;
   const bool active = q < p.nq;
@@ -532,8 +535,8 @@ __device__ __noinline__ int pass(const Ctx<G>& c, const double at[9]) {
 // scan takes it; rows, then columns exchanged; the column below the pivot
 // multiplied by its reciprocal, then the rank-one update. rowp / colp hold
 // the transpositions.
-template <int G>
-__device__ __noinline__ bool fullpiv_lu9_rows(const Ctx<G>& c, const double* a, double* lu, int* rowp, int* colp,
+template <int G, class CT>
+__device__ __noinline__ bool fullpiv_lu9_rows(const CT& c, const double* a, double* lu, int* rowp, int* colp,
                                               double* maxpivot_out) {
   const int lane = c.lane;
   _Pragma("unroll 1") for (int i = lane; i < 81; i += G) lu[i] = a[i];
@@ -717,8 +720,8 @@ __device__ __noinline__ bool llt9(double* a) {
 // diagonal by the lane of row k, then the rows below in parallel, each entry
 // the same dot product in the same order - the same factor and the same
 // answer.
-template <int G>
-__device__ __noinline__ bool llt9_rows(const Ctx<G>& c, double* a) {
+template <int G, class CT>
+__device__ __noinline__ bool llt9_rows(const CT& c, double* a) {
   const int lane = c.lane;
   _Pragma("unroll 1") for (int k = 0; k < 9; ++k) {
     int bad = 0;
@@ -1088,79 +1091,19 @@ struct Local {
 
 // ---- the condensation ---------------------------------------------------------
 
-template <int G>
-__global__ void __launch_bounds__(256) element_kernel(const __grid_constant__ Params p, int64_t ne, bool batch,
-                                                      const double* __restrict__ coords,
-                                                      const int32_t* __restrict__ conn, const double* __restrict__ u,
-                                                      const double* __restrict__ state,
-                                                      const double* __restrict__ alpha_n, int want_tangent,
-                                                      double* __restrict__ force, double* __restrict__ tangent,
-                                                      double* __restrict__ energy, double* __restrict__ trial,
-                                                      double* __restrict__ alpha_out, uint8_t* __restrict__ yield,
-                                                      int32_t* __restrict__ iterations, int32_t* __restrict__ code,
-                                                      int32_t* __restrict__ first_failure,
-                                                      const int32_t* __restrict__ order) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int epb = blockDim.x / G;
-  const int slot_in_block = threadIdx.x / G;
-  const int lane = threadIdx.x % G;
-  const int64_t slot = (int64_t)blockIdx.x * epb + slot_in_block;
-  ElemShared<G>* sh = reinterpret_cast<ElemShared<G>*>(smem_raw) + slot_in_block;
-  const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
-  const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
-  if (slot >= ne) return;  // whole groups leave together
-  // The element of this slot: the schedule's order (elements of alike cost
-  // side by side, so that the groups sharing a warp take alike paths), or
-  // the mesh order. Every output is indexed by the element, so the order
-  // changes no result.
-  const int64_t e = order ? (int64_t)order[slot] : slot;
-  double hu_lane[9];
-  double warm_lane[8];
-  warm_lane[7] = 0.0;  // no closest point yet
-  Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, trial, yield, hu_lane, warm_lane};
-  ElemShared<G>& s = *sh;
-  // Stage the element's coordinates and displacements (lane a: node a); a
-  // node index out of range fails the element before anything is read.
-  int bad_node = 0;
-  if (lane < 8) {
-    if (batch) {
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        s.X[3 * lane + k] = coords[e * 24 + 3 * lane + k];
-        s.U[3 * lane + k] = u[e * 24 + 3 * lane + k];
-      }
-    } else {
-      const int64_t node = conn[e * 8 + lane];
-      if (p.num_nodes > 0 && (node < 0 || node >= p.num_nodes)) {
-        bad_node = 1;
-      } else {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          s.X[3 * lane + k] = coords[node * 3 + k];
-          s.U[3 * lane + k] = u[node * 3 + k];
-        }
-      }
-    }
-  }
-  if (__any_sync(mask, bad_node)) {
-    if (lane == 0) {
-      code[e] = SBK_EL_BAD_NODE;
-      if (first_failure) atomicMin(first_failure, (int32_t)e);
-    }
-    return;
-  }
-  for (int i = lane; i < 9; i += G) s.alpha[i] = alpha_n ? alpha_n[e * 9 + i] : 0.0;
-  c.sync();
-  int status = set_up<G>(c);
-  Local<G> loc(c);
-  if (!status) status = loc.run();
-  if (status) {
-    if (lane == 0) {
-      code[e] = status;
-      if (first_failure) atomicMin(first_failure, (int32_t)e);
-    }
-    return;
-  }
+// The condensation (IncompatibleModes.cpp:549-561) after the local
+// iteration converged: lane a (a < 8) forms the rows of node a of K_ua (and
+// K_au), the coupling C = K_aa^-1 K_au, f* = f_u - K_ua K_aa^-1 r_a and, with
+// the tangent, K* = K_uu - K_ua C, symmetrised for a symmetric tangent. Reads
+// the group's shared record: the last pass's slots and sums (slot, r), the
+// factors of its K_aa (lu, rowp, colp) and the geometry; kc is overwritten.
+template <int G, class Rec>
+__device__ __forceinline__ void condense(const Ctx<G, Rec>& c, int want_tangent, double* __restrict__ force,
+                                         double* __restrict__ tangent) {
+  const Params& p = *c.p;
+  Rec& s = *c.s;
+  const int lane = c.lane;
+  const int64_t e = c.e;
   const bool sym = p.symmetric != 0;
   const bool geometric = p.kinematics != SBK_SMALL_STRAIN;
   const int nq = p.nq;
@@ -1286,12 +1229,526 @@ __global__ void __launch_bounds__(256) element_kernel(const __grid_constant__ Pa
       }
     }
   }
+}
+
+
+// One element of the single kernel, start to finish: staging, set_up, the
+// local iteration (Local::run), the condensation and the outputs.
+template <int G>
+__device__ __forceinline__ void element_body(const Params& p, int64_t ne, bool batch, int64_t e, ElemShared<G>* sh,
+                                             int lane, unsigned mask, const double* __restrict__ coords,
+                                             const int32_t* __restrict__ conn, const double* __restrict__ u,
+                                             const double* __restrict__ state, const double* __restrict__ alpha_n,
+                                             int want_tangent, double* __restrict__ force,
+                                             double* __restrict__ tangent, double* __restrict__ energy,
+                                             double* __restrict__ trial, double* __restrict__ alpha_out,
+                                             uint8_t* __restrict__ yield, int32_t* __restrict__ iterations,
+                                             int32_t* __restrict__ code, int32_t* __restrict__ first_failure) {
+  double hu_lane[9];
+  double warm_lane[8];
+  warm_lane[7] = 0.0;  // no closest point yet
+  Ctx<G> c{&p, sh, lane, mask, e, ne * p.nq, state, trial, yield, hu_lane, warm_lane};
+  ElemShared<G>& s = *sh;
+  // Stage the element's coordinates and displacements (lane a: node a); a
+  // node index out of range fails the element before anything is read.
+  int bad_node = 0;
+  if (lane < 8) {
+    if (batch) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        s.X[3 * lane + k] = coords[e * 24 + 3 * lane + k];
+        s.U[3 * lane + k] = u[e * 24 + 3 * lane + k];
+      }
+    } else {
+      const int64_t node = conn[e * 8 + lane];
+      if (p.num_nodes > 0 && (node < 0 || node >= p.num_nodes)) {
+        bad_node = 1;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          s.X[3 * lane + k] = coords[node * 3 + k];
+          s.U[3 * lane + k] = u[node * 3 + k];
+        }
+      }
+    }
+  }
+  if (__any_sync(mask, bad_node)) {
+    if (lane == 0) {
+      code[e] = SBK_EL_BAD_NODE;
+      if (first_failure) atomicMin(first_failure, (int32_t)e);
+    }
+    return;
+  }
+  for (int i = lane; i < 9; i += G) s.alpha[i] = alpha_n ? alpha_n[e * 9 + i] : 0.0;
+  c.sync();
+  int status = set_up<G>(c);
+  Local<G> loc(c);
+  if (!status) status = loc.run();
+  if (status) {
+    if (lane == 0) {
+      code[e] = status;
+      if (first_failure) atomicMin(first_failure, (int32_t)e);
+    }
+    return;
+  }
+  condense<G>(c, want_tangent, force, tangent);
   if (lane == 0) {
     energy[e] = s.energy;
     iterations[e] = loc.iterations;
     code[e] = 0;
   }
   for (int i = lane; i < 9; i += G) alpha_out[e * 9 + i] = s.alpha[i];
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) element_kernel(const __grid_constant__ Params p, int64_t ne, bool batch,
+                                                      const double* __restrict__ coords,
+                                                      const int32_t* __restrict__ conn, const double* __restrict__ u,
+                                                      const double* __restrict__ state,
+                                                      const double* __restrict__ alpha_n, int want_tangent,
+                                                      double* __restrict__ force, double* __restrict__ tangent,
+                                                      double* __restrict__ energy, double* __restrict__ trial,
+                                                      double* __restrict__ alpha_out, uint8_t* __restrict__ yield,
+                                                      int32_t* __restrict__ iterations, int32_t* __restrict__ code,
+                                                      int32_t* __restrict__ first_failure,
+                                                      const int32_t* __restrict__ order) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int epb = blockDim.x / G;
+  const int slot_in_block = threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  const int64_t slot = (int64_t)blockIdx.x * epb + slot_in_block;
+  ElemShared<G>* sh = reinterpret_cast<ElemShared<G>*>(smem_raw) + slot_in_block;
+  const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+  const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
+  if (slot >= ne) return;  // whole groups leave together
+  // The element of this slot: the schedule's order (elements of alike cost
+  // side by side, so that the groups sharing a warp take alike paths), or
+  // the mesh order. Every output is indexed by the element, so the order
+  // changes no result.
+  const int64_t e = order ? (int64_t)order[slot] : slot;
+  element_body<G>(p, ne, batch, e, sh, lane, mask, coords, conn, u, state, alpha_n, want_tangent, force, tangent,
+                  energy, trial, alpha_out, yield, iterations, code, first_failure);
+}
+
+// The single kernel over a device-counted list of elements (grid-stride):
+// the phase kernels hand it the elements that leave their common road.
+template <int G>
+__global__ void __launch_bounds__(256) element_list_kernel(const __grid_constant__ Params p, int64_t ne, bool batch,
+                                                           const double* __restrict__ coords,
+                                                           const int32_t* __restrict__ conn,
+                                                           const double* __restrict__ u,
+                                                           const double* __restrict__ state,
+                                                           const double* __restrict__ alpha_n, int want_tangent,
+                                                           double* __restrict__ force, double* __restrict__ tangent,
+                                                           double* __restrict__ energy, double* __restrict__ trial,
+                                                           double* __restrict__ alpha_out,
+                                                           uint8_t* __restrict__ yield,
+                                                           int32_t* __restrict__ iterations,
+                                                           int32_t* __restrict__ code,
+                                                           int32_t* __restrict__ first_failure,
+                                                           const int32_t* __restrict__ list,
+                                                           const int32_t* __restrict__ count) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int epb = blockDim.x / G;
+  const int slot_in_block = threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  ElemShared<G>* sh = reinterpret_cast<ElemShared<G>*>(smem_raw) + slot_in_block;
+  const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+  const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
+  const int64_t n = *count;
+  for (int64_t i = (int64_t)blockIdx.x * epb + slot_in_block; i < n; i += (int64_t)gridDim.x * epb) {
+    __syncwarp(mask);
+    element_body<G>(p, ne, batch, (int64_t)list[i], sh, lane, mask, coords, conn, u, state, alpha_n, want_tangent,
+                    force, tangent, energy, trial, alpha_out, yield, iterations, code, first_failure);
+  }
+}
+
+// ---- the local iteration as phase kernels over the whole mesh ------------------
+//
+// The same algorithm as element_kernel, split at its passes. Every element
+// of the mesh runs its local iteration in lockstep rounds; a round is two
+// launches over the elements still iterating:
+//
+//   wave_pass_kernel     one pass at each element's trial modes (the first
+//                        round: the geometry, then the pass at alpha_n);
+//   wave_control_kernel  the element-level step that follows a pass: the
+//                        full-pivoting LU of K_aa and the convergence test,
+//                        Newton's direction and the Cholesky test of the
+//                        symmetric part, the acceptance of a full step.
+//
+// Most elements take only that road - every trial a full Newton step that
+// the residual test accepts. An element that needs anything else (a step
+// the test rejects, a trial pass that fails, an indefinite K_aa, hence the
+// line searches, the shifted direction or Levenberg-Marquardt) is handed to
+// element_kernel, which runs it again from the start; an element that
+// converges goes to wave_condense_kernel, the condensation. Elements
+// continuing to the next round are compacted into the next round's list.
+// The passes, the factorisations, the tests and the condensation are the
+// single kernel's own functions on the same values, so every element's
+// outputs are bit-identical to element_kernel's (tested), and the rounds
+// end by construction: the first pass plus at most kMaxLocal Newton steps.
+//
+// Why: the single kernel runs set-up, passes, 9 x 9 algebra and
+// condensation back to back in one body of about 470 KB of code with 9.8 KB
+// of shared memory per element - one 4-warp block per SM, its warps at
+// different places in the code. Each phase kernel is a fraction of that
+// code, its record a fraction of that memory, and the warps of a launch all
+// run the same phase.
+
+constexpr int kWaveRounds = kMaxLocal + 1;
+constexpr int kKcStride = 88;  // K_aa as the reduce-scatter leaves it (81 used)
+
+template <int G>
+struct __align__(16) PassShared {
+  double X[24];
+  double U[24];
+  double jinv0[9];
+  double geo[G][12];
+  double slot[G][kSlot];
+  double kc[kKcStride];
+  double r[33];
+  double scale[9];
+  double flo[9];
+  double energy;
+};
+
+template <int G>
+struct __align__(16) ControlShared {
+  double kc[kKcStride];
+  double lu[81];
+  double work[243];
+  double r[33];
+  double scale[9];
+  double flo[9];
+  double alpha[9];
+  double dir[9];
+  double r0[9];
+  double maxpivot;
+  int rowp[9], colp[9];
+};
+
+template <int G>
+struct __align__(16) CondenseShared {
+  double jinv0[9];
+  double geo[G][12];
+  double slot[G][kSlot];
+  double kc[216];
+  double r[33];
+  double lu[81];
+  int rowp[9], colp[9];
+  double energy;
+};
+
+__device__ __forceinline__ double modes_norm(const double* r) {
+  double v = 0.0;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) v += r[24 + i] * r[24 + i];
+  return sqrt(v);
+}
+__device__ __forceinline__ double modes_inf(const double* r) {
+  double v = fabs(r[24]);
+#pragma unroll
+  for (int i = 1; i < 9; ++i) v = fmax(v, fabs(r[24 + i]));
+  return v;
+}
+__device__ __forceinline__ double abs_max9(const double* v) {
+  double m = fabs(v[0]);
+#pragma unroll
+  for (int i = 1; i < 9; ++i) m = fmax(m, fabs(v[i]));
+  return m;
+}
+
+// Warp-aggregated append of element e (by lane 0 of its group) to a list.
+__device__ __forceinline__ void append(int32_t* list, int32_t* count, int64_t e) {
+  const int pos = atomicAdd(count, 1);
+  list[pos] = (int32_t)e;
+}
+
+template <int G>
+__global__ void __launch_bounds__(128) wave_pass_kernel(const __grid_constant__ Params p, int64_t ne, int first,
+                                                        const int32_t* __restrict__ list,
+                                                        const int32_t* __restrict__ count, bool batch,
+                                                        const double* __restrict__ coords,
+                                                        const int32_t* __restrict__ conn,
+                                                        const double* __restrict__ u,
+                                                        const double* __restrict__ state,
+                                                        const double* __restrict__ alpha_n,
+                                                        double* __restrict__ trial, uint8_t* __restrict__ yield,
+                                                        const __grid_constant__ WaveBuffers w) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int epb = blockDim.x / G;
+  const int slot_in_block = threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  PassShared<G>* sh = reinterpret_cast<PassShared<G>*>(smem_raw) + slot_in_block;
+  const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+  const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
+  const int64_t n = count ? (int64_t)*count : ne;
+  const int nq = p.nq;
+  PassShared<G>& s = *sh;
+  for (int64_t i = (int64_t)blockIdx.x * epb + slot_in_block; i < n; i += (int64_t)gridDim.x * epb) {
+    const int64_t e = list ? (int64_t)list[i] : i;
+    double hu_lane[9];
+    double warm_lane[8];
+    Ctx<G, PassShared<G>> c{&p, sh, lane, mask, e, ne * nq, state, trial, yield, hu_lane, warm_lane};
+    __syncwarp(mask);
+    int status = 0;
+    double at[9];
+    if (first) {
+      // The single kernel's start: staging (a node out of range fails the
+      // element), alpha_n, set_up.
+      int bad_node = 0;
+      if (lane < 8) {
+        if (batch) {
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            s.X[3 * lane + k] = coords[e * 24 + 3 * lane + k];
+            s.U[3 * lane + k] = u[e * 24 + 3 * lane + k];
+          }
+        } else {
+          const int64_t node = conn[e * 8 + lane];
+          if (p.num_nodes > 0 && (node < 0 || node >= p.num_nodes)) {
+            bad_node = 1;
+          } else {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+              s.X[3 * lane + k] = coords[node * 3 + k];
+              s.U[3 * lane + k] = u[node * 3 + k];
+            }
+          }
+        }
+      }
+      if (__any_sync(mask, bad_node)) {
+        status = SBK_EL_BAD_NODE;
+      } else {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) at[k] = alpha_n ? alpha_n[e * 9 + k] : 0.0;
+        for (int k = lane; k < 9; k += G) w.alpha[e * 9 + k] = at[k];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) warm_lane[k] = 0.0;  // no closest point yet (warm_lane[7] == 0)
+        c.sync();
+        status = set_up<G>(c);
+        if (!status) {
+          if (lane < nq) {
+#pragma unroll
+            for (int f = 0; f < 12; ++f) w.geo[(e * 12 + f) * G + lane] = s.geo[lane][f];
+#pragma unroll
+            for (int f = 0; f < 9; ++f) w.hu[(e * 9 + f) * G + lane] = hu_lane[f];
+          }
+          for (int k = lane; k < 9; k += G) w.jinv0[e * 9 + k] = s.jinv0[k];
+        }
+      }
+    } else {
+      // A trial at alpha + 1 dir (Local::try_at with t = 1).
+#pragma unroll
+      for (int k = 0; k < 9; ++k) at[k] = w.alpha[e * 9 + k] + 1.0 * w.dir[e * 9 + k];
+      if (lane < nq) {
+#pragma unroll
+        for (int f = 0; f < 12; ++f) s.geo[lane][f] = w.geo[(e * 12 + f) * G + lane];
+#pragma unroll
+        for (int f = 0; f < 9; ++f) hu_lane[f] = w.hu[(e * 9 + f) * G + lane];
+#pragma unroll
+        for (int f = 0; f < 8; ++f) warm_lane[f] = w.warm[(e * 8 + f) * G + lane];
+      }
+      for (int k = lane; k < 9; k += G) s.jinv0[k] = w.jinv0[e * 9 + k];
+      c.sync();
+    }
+    if (!status) status = pass<G>(c, at);
+    if (lane == 0) w.pcode[e] = status;
+    if (!status) {
+      for (int k = lane; k < 81; k += G) w.kc[e * kKcStride + k] = s.kc[k];
+      for (int k = lane; k < 33; k += G) w.r[e * 33 + k] = s.r[k];
+      for (int k = lane; k < 9; k += G) {
+        w.sf[e * 19 + k] = s.scale[k];
+        w.sf[e * 19 + 9 + k] = s.flo[k];
+      }
+      if (lane == 0) w.sf[e * 19 + 18] = s.energy;
+      if (lane < nq) {
+#pragma unroll 6
+        for (int f = 0; f < kSlot; ++f) w.slot[(e * kSlot + f) * G + lane] = s.slot[lane][f];
+#pragma unroll
+        for (int f = 0; f < 8; ++f) w.warm[(e * 8 + f) * G + lane] = warm_lane[f];
+      }
+    }
+  }
+}
+
+// A failed element: its status and the lowest failing element, as the
+// single kernel reports them.
+__device__ __forceinline__ void wave_fail(int32_t* code, int32_t* first_failure, int64_t e, int status) {
+  code[e] = status;
+  if (first_failure) atomicMin(first_failure, (int32_t)e);
+}
+
+template <int G>
+__global__ void __launch_bounds__(128) wave_control_kernel(const __grid_constant__ Params p, int64_t ne, int first,
+                                                           const int32_t* __restrict__ list,
+                                                           const int32_t* __restrict__ count,
+                                                           const __grid_constant__ WaveBuffers w,
+                                                           int32_t* __restrict__ next, int32_t* __restrict__ next_count,
+                                                           int32_t* __restrict__ code,
+                                                           int32_t* __restrict__ first_failure) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int epb = blockDim.x / G;
+  const int slot_in_block = threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  ControlShared<G>* sh = reinterpret_cast<ControlShared<G>*>(smem_raw) + slot_in_block;
+  const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+  const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
+  const int64_t n = count ? (int64_t)*count : ne;
+  ControlShared<G>& s = *sh;
+  int32_t* done_list = w.done;
+  int32_t* done_count = w.counts + kWaveRounds + 1;
+  int32_t* fallback_list = w.fallback;
+  int32_t* fallback_count = w.counts + kWaveRounds + 2;
+  for (int64_t i = (int64_t)blockIdx.x * epb + slot_in_block; i < n; i += (int64_t)gridDim.x * epb) {
+    const int64_t e = list ? (int64_t)list[i] : i;
+    Ctx<G, ControlShared<G>> c{&p, sh, lane, mask, e, 0, nullptr, nullptr, nullptr, nullptr, nullptr};
+    __syncwarp(mask);
+    const int pc = w.pcode[e];
+    if (pc) {
+      // A failed first pass fails the element (Local::run); a failed trial
+      // is the line search's business.
+      if (lane == 0) {
+        if (first) wave_fail(code, first_failure, e, pc);
+        else append(fallback_list, fallback_count, e);
+      }
+      continue;
+    }
+    for (int k = lane; k < 81; k += G) s.kc[k] = w.kc[e * kKcStride + k];
+    for (int k = lane; k < 33; k += G) s.r[k] = w.r[e * 33 + k];
+    for (int k = lane; k < 9; k += G) {
+      s.scale[k] = w.sf[e * 19 + k];
+      s.flo[k] = w.sf[e * 19 + 9 + k];
+      s.alpha[k] = w.alpha[e * 9 + k];
+      s.dir[k] = w.dir[e * 9 + k];
+    }
+    int iterations = first ? 0 : w.iters[e];
+    double residual = first ? 0.0 : w.res[e];
+    c.sync();
+    if (first) {
+      residual = modes_norm(s.r);
+    } else {
+      // line_search's full step (IncompatibleModes.cpp:398-410): accepted
+      // when it reduces the residual enough or meets the tolerance.
+      const double full = modes_norm(s.r);
+      if (full <= kFullStepReduction * residual ||
+          modes_inf(s.r) <= kLocalTolerance * abs_max9(s.scale) + kLocalRoundOff * abs_max9(s.flo)) {
+        c.sync();
+        if (lane == 0)
+#pragma unroll
+          for (int k = 0; k < 9; ++k) s.alpha[k] += 1.0 * s.dir[k];
+        c.sync();
+        residual = full;
+      } else {
+        if (lane == 0) append(fallback_list, fallback_count, e);
+        continue;
+      }
+    }
+    // The head of solve_and_condense's loop (IncompatibleModes.cpp:353-397).
+    const double largest = modes_inf(s.r);
+    const double scale = abs_max9(s.scale);
+    const double floor_ = kLocalRoundOff * abs_max9(s.flo);
+    const bool invertible = fullpiv_lu9_rows<G>(c, s.kc, s.lu, s.rowp, s.colp, &s.maxpivot);
+    for (int k = lane; k < 81; k += G) s.work[k] = s.kc[k];
+    for (int k = lane; k < 9; k += G) s.r0[k] = s.r[24 + k];
+    c.sync();
+    if (!invertible) {
+      if (lane == 0) wave_fail(code, first_failure, e, SBK_EL_LOCAL_SINGULAR);
+      continue;
+    }
+    if (largest <= kLocalTolerance * scale + floor_ || largest == 0.0) {
+      // Converged: the factors of this K_aa for the condensation.
+      for (int k = lane; k < 81; k += G) w.kc[e * kKcStride + k] = s.lu[k];
+      for (int k = lane; k < 9; k += G) {
+        w.piv[e * 18 + k] = s.rowp[k];
+        w.piv[e * 18 + 9 + k] = s.colp[k];
+        w.alpha[e * 9 + k] = s.alpha[k];
+      }
+      if (lane == 0) {
+        w.iters[e] = iterations;
+        append(done_list, done_count, e);
+      }
+      continue;
+    }
+    if (iterations == kMaxLocal || !isfinite(largest)) {
+      if (lane == 0) wave_fail(code, first_failure, e, SBK_EL_LOCAL_NO_CONVERGE);
+      continue;
+    }
+    ++iterations;
+    for (int idx = lane; idx < 81; idx += G) {
+      const int a = idx / 9, b = idx % 9;
+      const double v = 0.5 * (s.work[a * 9 + b] + s.work[b * 9 + a]);
+      s.work[81 + idx] = v;
+      s.work[162 + idx] = v;
+    }
+    c.sync();
+    if (lane == 0) {
+      double nw[9];
+      fullpiv_solve9(s.lu, s.rowp, s.colp, s.r0, nw);
+      for (int k = 0; k < 9; ++k) s.dir[k] = -nw[k];
+    }
+    const bool positive = llt9_rows<G>(c, s.work + 162);
+    c.sync();
+    if (!positive) {
+      if (lane == 0) append(fallback_list, fallback_count, e);
+      continue;
+    }
+    for (int k = lane; k < 9; k += G) {
+      w.alpha[e * 9 + k] = s.alpha[k];
+      w.dir[e * 9 + k] = s.dir[k];
+    }
+    if (lane == 0) {
+      w.iters[e] = iterations;
+      w.res[e] = residual;
+      append(next, next_count, e);
+    }
+  }
+}
+
+template <int G>
+__global__ void __launch_bounds__(128) wave_condense_kernel(const __grid_constant__ Params p, int64_t ne,
+                                                            const __grid_constant__ WaveBuffers w, int want_tangent,
+                                                            double* __restrict__ force, double* __restrict__ tangent,
+                                                            double* __restrict__ energy,
+                                                            double* __restrict__ alpha_out,
+                                                            int32_t* __restrict__ iterations,
+                                                            int32_t* __restrict__ code) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int epb = blockDim.x / G;
+  const int slot_in_block = threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  CondenseShared<G>* sh = reinterpret_cast<CondenseShared<G>*>(smem_raw) + slot_in_block;
+  const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+  const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
+  const int64_t n = w.counts[kWaveRounds + 1];
+  const int nq = p.nq;
+  CondenseShared<G>& s = *sh;
+  for (int64_t i = (int64_t)blockIdx.x * epb + slot_in_block; i < n; i += (int64_t)gridDim.x * epb) {
+    const int64_t e = w.done[i];
+    Ctx<G, CondenseShared<G>> c{&p, sh, lane, mask, e, ne * nq, nullptr, nullptr, nullptr, nullptr, nullptr};
+    __syncwarp(mask);
+    if (lane < nq) {
+#pragma unroll
+      for (int f = 0; f < 12; ++f) s.geo[lane][f] = w.geo[(e * 12 + f) * G + lane];
+#pragma unroll 6
+      for (int f = 0; f < kSlot; ++f) s.slot[lane][f] = w.slot[(e * kSlot + f) * G + lane];
+    }
+    for (int k = lane; k < 9; k += G) {
+      s.jinv0[k] = w.jinv0[e * 9 + k];
+      s.rowp[k] = w.piv[e * 18 + k];
+      s.colp[k] = w.piv[e * 18 + 9 + k];
+    }
+    for (int k = lane; k < 81; k += G) s.lu[k] = w.kc[e * kKcStride + k];
+    for (int k = lane; k < 33; k += G) s.r[k] = w.r[e * 33 + k];
+    c.sync();
+    condense<G>(c, want_tangent, force, tangent);
+    if (lane == 0) {
+      energy[e] = w.sf[e * 19 + 18];
+      iterations[e] = w.iters[e];
+      code[e] = 0;
+    }
+    for (int k = lane; k < 9; k += G) alpha_out[e * 9 + k] = w.alpha[e * 9 + k];
+  }
 }
 
 // ---- the shape derivative: lambda . d f* / d X ---------------------------------
@@ -2319,6 +2776,118 @@ int launch_vjp(const Params& p, int64_t ne, const double* coords, const int32_t*
                            stream);
   return launch_vjp_g<32>(p, ne, coords, conn, u, state, alpha_n, lambda, trial, yield, code, first_failure, out,
                           stream);
+}
+
+namespace {
+
+// The next array of `count` T at byte offset `at` of base (256-byte
+// aligned); advances `at`. With a null base only the offsets are counted.
+template <class T>
+T* carve(char* base, size_t& at, size_t count) {
+  T* out = base ? reinterpret_cast<T*>(base + at) : nullptr;
+  at += (count * sizeof(T) + 255) / 256 * 256;
+  return out;
+}
+
+// The shared-memory limit of a kernel raised once per device, so that a
+// launch inside a stream capture makes no attribute call.
+template <class K>
+int raise_smem(K kern, size_t smem, size_t* raised) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || raised[dev] < smem) {
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return (int)err;
+    if (dev >= 0 && dev < 64) raised[dev] = smem;
+  }
+  return 0;
+}
+
+}  // namespace
+
+namespace {
+
+size_t carve_all(char* base, int64_t ne, WaveBuffers& w) {
+  size_t at = 0;
+  const size_t n = (size_t)ne;
+  w.alpha = carve<double>(base, at, n * 9);
+  w.dir = carve<double>(base, at, n * 9);
+  w.res = carve<double>(base, at, n);
+  w.iters = carve<int32_t>(base, at, n);
+  w.pcode = carve<int32_t>(base, at, n);
+  w.kc = carve<double>(base, at, n * kKcStride);
+  w.r = carve<double>(base, at, n * 33);
+  w.sf = carve<double>(base, at, n * 19);
+  w.piv = carve<int32_t>(base, at, n * 18);
+  w.slot = carve<double>(base, at, n * kSlot * 8);
+  w.geo = carve<double>(base, at, n * 12 * 8);
+  w.jinv0 = carve<double>(base, at, n * 9);
+  w.hu = carve<double>(base, at, n * 9 * 8);
+  w.warm = carve<double>(base, at, n * 8 * 8);
+  w.list[0] = carve<int32_t>(base, at, n);
+  w.list[1] = carve<int32_t>(base, at, n);
+  w.done = carve<int32_t>(base, at, n);
+  w.fallback = carve<int32_t>(base, at, n);
+  w.counts = carve<int32_t>(base, at, kWaveRounds + 3);
+  return at;
+}
+
+}  // namespace
+
+size_t wave_buffer_bytes(int64_t ne) {
+  WaveBuffers w;
+  return carve_all(nullptr, ne, w);
+}
+
+void wave_buffers_carve(void* base, int64_t ne, WaveBuffers& w) { carve_all(static_cast<char*>(base), ne, w); }
+
+bool wave_applies(const Params& p) { return p.element == 0 && p.nq <= 8; }
+
+int launch_elements_wave(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
+                         const double* state, const double* alpha_n, int want_tangent, double* force,
+                         double* tangent, double* energy, double* trial, double* alpha_out, uint8_t* yield,
+                         int32_t* iterations, int32_t* code, int32_t* first_failure, bool batch,
+                         const int32_t* order, const WaveBuffers& w, cudaStream_t stream) {
+  constexpr int G = 8;
+  if (!wave_applies(p)) return (int)cudaErrorInvalidValue;
+  if (ne <= 0) return 0;
+  constexpr int epb = 16;  // 4 warps per block
+  const int threads = epb * G;
+  static size_t raised[4][64] = {};
+  const size_t smem_pass = sizeof(PassShared<G>) * epb;
+  const size_t smem_ctl = sizeof(ControlShared<G>) * epb;
+  const size_t smem_cond = sizeof(CondenseShared<G>) * epb;
+  const size_t smem_elem = sizeof(ElemShared<G>) * epb;
+  int rc = raise_smem(wave_pass_kernel<G>, smem_pass, raised[0]);
+  if (!rc) rc = raise_smem(wave_control_kernel<G>, smem_ctl, raised[1]);
+  if (!rc) rc = raise_smem(wave_condense_kernel<G>, smem_cond, raised[2]);
+  if (!rc) rc = raise_smem(element_list_kernel<G>, smem_elem, raised[3]);
+  if (rc) return rc;
+  const int64_t need = (ne + epb - 1) / epb;
+  // Grid-stride launches: enough blocks to fill every SM several times over
+  // in the first rounds, few enough that the late rounds (a handful of
+  // elements) cost little more than the launch.
+  const int64_t cap = 148 * 16;
+  const unsigned grid = (unsigned)(need < cap ? need : cap);
+  cudaError_t err = cudaMemsetAsync(w.counts, 0, (kWaveRounds + 3) * sizeof(int32_t), stream);
+  if (err != cudaSuccess) return (int)err;
+  for (int r = 0; r < kWaveRounds; ++r) {
+    const int32_t* list = r == 0 ? order : w.list[r & 1];
+    const int32_t* count = r == 0 ? nullptr : w.counts + r;
+    wave_pass_kernel<G><<<grid, threads, smem_pass, stream>>>(p, ne, r == 0, list, count, batch, coords, conn, u, state,
+                                                              alpha_n, trial, yield, w);
+    wave_control_kernel<G><<<grid, threads, smem_ctl, stream>>>(p, ne, r == 0, list, count, w, w.list[(r + 1) & 1],
+                                                                w.counts + r + 1, code, first_failure);
+  }
+  wave_condense_kernel<G><<<grid, threads, smem_cond, stream>>>(p, ne, w, want_tangent, force, tangent, energy,
+                                                                alpha_out, iterations, code);
+  // The elements that left the common road, by the single kernel from the
+  // start (one 4-warp block per SM holds its records).
+  const unsigned fgrid = (unsigned)(need < 148 * 2 ? need : 148 * 2);
+  element_list_kernel<G><<<fgrid, threads, smem_elem, stream>>>(
+      p, ne, batch, coords, conn, u, state, alpha_n, want_tangent, force, tangent, energy, trial, alpha_out, yield,
+      iterations, code, first_failure, w.fallback, w.counts + kWaveRounds + 2);
+  return (int)cudaGetLastError();
 }
 
 size_t element_smem_bytes(int group) {

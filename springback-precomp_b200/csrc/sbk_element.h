@@ -26,6 +26,44 @@ int launch_elements(const Params& p, int64_t ne, const double* coords, const int
                     int32_t* code, int32_t* first_failure, bool batch, int elements_per_block,
                     const int32_t* order, cudaStream_t stream);
 size_t element_smem_bytes(int group);
+
+// The local iteration of the incompatible-mode Hex8 (rules of up to 8
+// points) as phase kernels over the whole mesh (sbk_element.cu): per-element
+// records between the kernels. Field-major within an element where the
+// lanes of a group read alike fields (field f of point q at (e * F + f) * 8
+// + q).
+struct WaveBuffers {
+  double* alpha;    // ne x 9: the modes of the current iterate
+  double* dir;      // ne x 9: Newton's direction of the pending trial
+  double* res;      // ne: the residual norm of the current iterate
+  int32_t* iters;   // ne: local Newton steps
+  int32_t* pcode;   // ne: status of the last pass
+  double* kc;       // ne x 88: K_aa of the last pass, then its LU factors
+  double* r;        // ne x 33: f_u 24, r_a 9 of the last pass
+  double* sf;       // ne x 19: scale 9, floor 9, energy
+  int32_t* piv;     // ne x 18: the LU's row and column transpositions
+  double* slot;     // ne x 54 x 8: the points' material blocks
+  double* geo;      // ne x 12 x 8: J^-1, w det J, det0 / det per point
+  double* jinv0;    // ne x 9
+  double* hu;       // ne x 9 x 8: U G^T per point
+  double* warm;     // ne x 8 x 8: the points' last closest points
+  int32_t* list[2]; // ne each: the elements of a round
+  int32_t* done;    // ne: converged elements
+  int32_t* fallback;  // ne: elements handed to the single kernel
+  int32_t* counts;  // rounds + 3: each round's count, then done, fallback
+};
+// Bytes of one allocation that wave_buffers_carve splits for ne elements.
+size_t wave_buffer_bytes(int64_t ne);
+void wave_buffers_carve(void* base, int64_t ne, WaveBuffers& w);
+// Whether the phase kernels take this material, rule and element.
+bool wave_applies(const Params& p);
+// K1 by the phase kernels (mesh or batch mode, as launch_elements); no
+// host synchronisation, so it can be captured in a CUDA graph.
+int launch_elements_wave(const Params& p, int64_t ne, const double* coords, const int32_t* conn, const double* u,
+                         const double* state, const double* alpha_n, int want_tangent, double* force,
+                         double* tangent, double* energy, double* trial, double* alpha_out, uint8_t* yield,
+                         int32_t* iterations, int32_t* code, int32_t* first_failure, bool batch,
+                         const int32_t* order, const WaveBuffers& w, cudaStream_t stream);
 // The shape derivative: per element lambda . d f*/d X (24, node-major) into
 // out, at u with the committed points (state) and modes (alpha_n) as the
 // history and lambda a global DOF vector; the local iteration runs again to

@@ -112,6 +112,15 @@ def element_batch(material: Material, x: torch.Tensor, u: torch.Tensor, state: O
     return out
 
 
+LOCAL_ITERATION = {"phases": 0, "single": 1}
+
+
+def set_local_iteration(mode: str = "phases"):
+    """The local iteration of element_batch and of systems made from now on:
+    "phases" (the default) or "single" (see NonlinearSystem.set_local_iteration)."""
+    _capi.check(_capi.lib().sbk_set_local_iteration(LOCAL_ITERATION[mode]))
+
+
 NOALLOC_MAX_ELEMENTS = 2048
 NOALLOC_MAX_NODES = 16384
 
@@ -291,6 +300,14 @@ class NonlinearSystem:
         """Walk the elements grouped by the cost of their last evaluation (the
         default) or in mesh order; no result depends on it."""
         _capi.check(_capi.lib().sbk_system_set_schedule(self._h, 1 if by_cost else 0))
+
+    def set_local_iteration(self, mode: str = "phases"):
+        """How the incompatible-mode Hex8's local iteration runs: "phases"
+        (the default: phase kernels over the whole mesh, the elements that
+        need a line search or a fallback handed to the single kernel) or
+        "single" (one kernel per element from start to finish). No result
+        depends on it."""
+        _capi.check(_capi.lib().sbk_system_set_local_iteration(self._h, LOCAL_ITERATION[mode]))
 
     def set_elements_per_block(self, epb: int):
         _capi.check(_capi.lib().sbk_system_set_elements_per_block(self._h, int(epb)))

@@ -91,11 +91,12 @@ def test_tool_force_history_matches_the_reference(run):
     assert np.abs(got - ref).max() <= 1e-5 * np.abs(ref).max()
 
 
-# Step-end element fields: the von Mises stress within 1e-9 of the largest
-# in the step, the largest equivalent plastic strain within 1e-10 (absolute;
-# the fields are O(0.1) at most).
-VM_TOL = 1.0e-9
-EQPS_TOL = 1.0e-10
+# Step-end element fields: the von Mises stress within 1e-10 of the largest
+# in the step, the largest equivalent plastic strain within 1e-12 (absolute;
+# the fields are O(0.1) at most). Measured on a B200 over the seven runs:
+# 2.9e-12 and 2.2e-14.
+VM_TOL = 1.0e-10
+EQPS_TOL = 1.0e-12
 
 
 @pytest.mark.parametrize("k,name", [(0, "form"), (1, "unload"), (2, "release")])

@@ -230,3 +230,30 @@ def test_out_of_range_indices_are_refused(pkg, problem, cuda):
     free = torch.tensor([0, 1, mesh.num_dofs], dtype=torch.int32, device=cuda)
     with pytest.raises(pkg.SbkError):
         sys_.stiffness_gross(u, free)
+
+
+def test_system_phase_kernels_match_the_single_kernel_bit_for_bit(pkg, cuda):
+    """NonlinearSystem.evaluate through the phase kernels (the default) and
+    through the single kernel: the assembled tangent, f_int, the trial
+    states and modes bit-identical, on the microbenchmark construction, for
+    a first evaluation and for one under the element schedule."""
+    wl = importlib.import_module("springback-precomp_b200.workload")
+    prob = wl.make_problem(30, 16, 2, seed=11, sample=480)
+    out = {}
+    for mode in ("phases", "single"):
+        sysm = pkg.NonlinearSystem(prob.mesh, prob.material, kinematics="logarithmic")
+        sysm.set_local_iteration(mode)
+        sysm.set_committed(prob.state)
+        sysm.set_internal(prob.alpha)
+        u = torch.tensor(prob.u, device=cuda)
+        evs = []
+        for _ in range(2):  # the second walks the schedule
+            ev = sysm.evaluate(u, 0.0, True)
+            evs.append((ev.tangent.clone(), ev.internal.clone(), ev.energy, ev.yielding_points))
+        out[mode] = (evs, sysm.trial_states(), sysm.trial_modes())
+    (ea, sa, ma), (eb, sb, mb) = out["phases"], out["single"]
+    for (ka, fa, ena, ya), (kb, fb, enb, yb) in zip(ea, eb):
+        assert torch.equal(ka, kb) and torch.equal(fa, fb)
+        assert ena == enb and ya == yb
+    np.testing.assert_array_equal(sa, sb)
+    np.testing.assert_array_equal(ma, mb)

@@ -98,15 +98,16 @@ def _dense(values, outer, inner, n):
     return sp.csc_matrix((values, inner, outer), shape=(n, n)).toarray()
 
 
-@pytest.mark.parametrize("bad", ["node_out_of_range", "repeated_node"])
+@pytest.mark.parametrize("bad", ["node_out_of_range", "inverted"])
 def test_noalloc_leaves_a_failed_element_out_of_the_sums(pkg, cuda, bad):
     """A failed element is left out of every sum even though the shared
     scratch still holds an earlier call's values in its slots: a good call
     first fills the scratch, then element 5 fails - by naming a node out of
-    range (SBK_EL_BAD_NODE before anything of it is read), or by naming one
-    node twice, which collapses it (SBK_EL_MESH_INVERTED) - and the sums must
-    equal the allocating path's on the mesh without element 5. The caller's
-    yield bytes of the failed element are garbage and must not count."""
+    range (SBK_EL_BAD_NODE before anything of it is read), or by listing its
+    top face before its bottom face, which inverts it (SBK_EL_MESH_INVERTED,
+    after its nodes were read) - and the sums must equal the allocating
+    path's on the mesh without element 5. The caller's yield bytes of the
+    failed element are garbage and must not count."""
     wl = importlib.import_module("springback-precomp_b200.workload")
     system = importlib.import_module("springback-precomp_b200.system")
     mesh_mod = importlib.import_module("springback-precomp_b200.mesh")
@@ -130,18 +131,15 @@ def test_noalloc_leaves_a_failed_element_out_of_the_sums(pkg, cuda, bad):
         conn[5, 3] = mesh.num_nodes  # one past the last node
         expected_code = 9  # SBK_EL_BAD_NODE
     else:
-        conn[5, 3] = conn[5, 0]
-        expected_code = None
+        conn[5] = conn[5][[4, 5, 6, 7, 0, 1, 2, 3]]
+        expected_code = 6  # SBK_EL_MESH_INVERTED
     yielding.fill_(1)  # what the caller's buffer held before: must not be counted for element 5
     system.evaluate_noalloc(mat, coords, conn, u, state, alpha, outer, inner, internal, values, trial, alpha_out,
                             yielding, summary)
     torch.cuda.synchronize()
     s = summary.cpu().numpy()
     assert s[3] == 5.0, s
-    if expected_code is not None:
-        assert int(s[4]) == expected_code, s
-    else:
-        assert int(s[4]) != 0, s
+    assert int(s[4]) == expected_code, s
 
     # The allocating path on the mesh without element 5.
     keep = np.array([e for e in range(mesh.num_elements) if e != 5])
