@@ -465,7 +465,8 @@ int system_elements(sbk_system* sys, const double* u_dev, int want_tangent, cuda
   if (sys->local_mode == SBK_LOCAL_PHASES && sys->wave_mem && sbk::wave_applies(sys->p))
     return sbk::launch_elements_wave(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c,
                                      want_tangent, sys->force, sys->tangent, sys->energy_e, sys->trial, sys->alpha_t,
-                                     sys->yield, sys->iters, sys->code, sys->first_fail, false, order, sys->wave, st);
+                                     sys->yield, sys->iters, sys->code, sys->first_fail, false, order, sys->wave,
+                                     sys->elements_per_block, st);
   return sbk::launch_elements(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c,
                               want_tangent, sys->force, sys->tangent, sys->energy_e, sys->trial, sys->alpha_t,
                               sys->yield, sys->iters, sys->code, sys->first_fail, false, sys->elements_per_block, order,
@@ -540,7 +541,7 @@ int sbk_element_batch(const sbk_material* material, const sbk_rule* rule, int ki
     sbk::wave_buffers_carve(mem, ne, w);
     rc = sbk::launch_elements_wave(p, ne, x_dev, nullptr, u_dev, state_dev, alpha_dev, tangent_dev != nullptr,
                                    force_dev, tangent_dev, energy_dev, trial_dev, alpha_out_dev, yield_dev,
-                                   iterations_dev, code_dev, nullptr, true, nullptr, w, s);
+                                   iterations_dev, code_dev, nullptr, true, nullptr, w, 0, s);
     cudaError_t e = cudaFreeAsync(mem, s);
     if (rc) return fail(SBK_ERR_CUDA, std::string("element kernels: ") + cudaGetErrorString((cudaError_t)rc));
     if (e != cudaSuccess) return fail(SBK_ERR_CUDA, std::string("cudaFreeAsync: ") + cudaGetErrorString(e));

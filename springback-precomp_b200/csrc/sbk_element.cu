@@ -293,104 +293,107 @@ __device__ int set_up(const Ctx<G, Rec>& c) {
   return bad ? SBK_EL_MESH_INVERTED : 0;
 }
 
-// One pass (IncompatibleModes.cpp:337-342): the kinematics, the returns and
-// the sums at `at` (9 values, identical in every lane). Returns 0 or the
-// failure code of the first failing point in the reference's order.
+// The kinematics of point q at the modes `at` (kinematics_at,
+// IncompatibleModes.cpp:195-225): its mode gradients gt, F, the largest
+// |H| entry, the strain the return takes and, under logarithmic
+// kinematics, the spectral data L of the log strain. Returns 0, or a
+// point-failure code (an inverted point, a log strain out of range).
 template <int G, class Rec>
-__device__ __noinline__ int pass(const Ctx<G, Rec>& c, const double at[9]) {
-  Rec& s = *c.s;
+__device__ __forceinline__ int point_kinematics(const Ctx<G, Rec>& c, int q, const double at[9], double gt[9],
+                                                double F[9], double& hmax, double strain[6], LogKin& L) {
   const Params& p = *c.p;
-  const int q = c.lane;
-  const bool active = q < p.nq;
-  const bool geometric = p.kinematics != SBK_SMALL_STRAIN;
-  int fail = 0;  // (stage << 8) | q, stage 1 kinematics, 2 return
   int code = 0;
-  double gt[9], F[9], hmax = 0.0;
-  double kbuf[G];
-  double M[36], S[6];
-  double w = 0.0;
-  if (active) {
-    w = s.geo[q][9];
-    mode_grads(c, q, gt);
-    double h[9];
+  mode_grads(c, q, gt);
+  double h[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      double v = c.hu[i * 3 + j];
+#pragma unroll
+      for (int m = 0; m < 3; ++m) v += at[3 * m + i] * gt[j * 3 + m];
+      h[i * 3 + j] = v;
+    }
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    hmax = fmax(hmax, fabs(h[i]));
+    F[i] = h[i] + ((i % 4) == 0 ? 1.0 : 0.0);
+  }
+  if (p.kinematics == SBK_SMALL_STRAIN) {
+    strain[0] = h[0];
+    strain[1] = h[4];
+    strain[2] = h[8];
+    strain[3] = h[1] + h[3];
+    strain[4] = h[5] + h[7];
+    strain[5] = h[6] + h[2];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) F[i] = (i % 4) == 0 ? 1.0 : 0.0;
+  } else {
+    double E[9];
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        double v = c.hu[i * 3 + j];
+      for (int j = 0; j < 3; ++j)
+        E[i * 3 + j] = 0.5 * (h[i * 3 + j] + h[j * 3 + i] + h[0 * 3 + i] * h[0 * 3 + j] +
+                              h[1 * 3 + i] * h[1 * 3 + j] + h[2 * 3 + i] * h[2 * 3 + j]);
+    double green[6] = {E[0], E[4], E[8], 2.0 * E[1], 2.0 * E[5], 2.0 * E[6]};
+    if (p.kinematics == SBK_FINITE) {
 #pragma unroll
-        for (int m = 0; m < 3; ++m) v += at[3 * m + i] * gt[j * 3 + m];
-        h[i * 3 + j] = v;
-      }
-#pragma unroll
-    for (int i = 0; i < 9; ++i) {
-      hmax = fmax(hmax, fabs(h[i]));
-      F[i] = h[i] + ((i % 4) == 0 ? 1.0 : 0.0);
-    }
-    double strain[6];
-    LogKin L;
-    if (p.kinematics == SBK_SMALL_STRAIN) {
-      strain[0] = h[0];
-      strain[1] = h[4];
-      strain[2] = h[8];
-      strain[3] = h[1] + h[3];
-      strain[4] = h[5] + h[7];
-      strain[5] = h[6] + h[2];
-#pragma unroll
-      for (int i = 0; i < 9; ++i) F[i] = (i % 4) == 0 ? 1.0 : 0.0;
+      for (int i = 0; i < 6; ++i) strain[i] = green[i];
     } else {
-      double E[9];
-#pragma unroll
-      for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j)
-          E[i * 3 + j] = 0.5 * (h[i * 3 + j] + h[j * 3 + i] + h[0 * 3 + i] * h[0 * 3 + j] +
-                                h[1 * 3 + i] * h[1 * 3 + j] + h[2 * 3 + i] * h[2 * 3 + j]);
-      double green[6] = {E[0], E[4], E[8], 2.0 * E[1], 2.0 * E[5], 2.0 * E[6]};
-      if (p.kinematics == SBK_FINITE) {
-#pragma unroll
-        for (int i = 0; i < 6; ++i) strain[i] = green[i];
+      if (!(det3(F) > 0.0)) {
+        code = SBK_EL_INVERTED_POINT;
       } else {
-        if (!(det3(F) > 0.0)) {
-          code = SBK_EL_INVERTED_POINT;
-        } else {
-          code = log_strain(green, L, strain);
-        }
-        if (code) fail = (1 << 8) | q;
-      }
-    }
-    if (!fail) {
-      PointState st{c.state + c.e * p.nq + q, c.trial + c.e * p.nq + q, c.npts};
-      Response r;
-      code = p.general ? general_return(p, strain, st, r, c.warm) : radial_return(p, strain, st, r);
-      if (code) {
-        fail = (2 << 8) | q;
-      } else {
-        c.yield[c.e * p.nq + q] = r.yielding ? 1 : 0;
-#pragma unroll
-        for (int i = 0; i < 36; ++i) M[i] = r.C[i];
-        if (p.kinematics == SBK_FINITE_LOGARITHMIC) {
-          log_transform(L, r.stress, S, M);
-        } else {
-#pragma unroll
-          for (int i = 0; i < 6; ++i) S[i] = r.stress[i];
-        }
-        double mmax = 0.0;
-#pragma unroll
-        for (int i = 0; i < 36; ++i) {
-          s.slot[q][i] = M[i];
-          mmax = fmax(mmax, fabs(M[i]));
-        }
-#pragma unroll
-        for (int i = 0; i < 6; ++i) s.slot[q][kSlotS + i] = S[i];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) s.slot[q][kSlotF + i] = F[i];
-        s.slot[q][kSlotW] = w;
-        s.slot[q][kSlotE] = r.energy;
-        s.slot[q][kSlotFl] = w * mmax * hmax * (1.0 + hmax);
+        code = log_strain(green, L, strain);
       }
     }
   }
+  return code;
+}
+
+// After the point's response r: its yield flag, the material block M and
+// stress S in the strain measure of the element (the logarithmic map, or
+// as they are), and its slot for the group sums.
+template <int G, class Rec>
+__device__ __forceinline__ void point_slot(const Ctx<G, Rec>& c, int q, const Response& r, const LogKin& L,
+                                           const double F[9], double w, double hmax, double M[36], double S[6]) {
+  const Params& p = *c.p;
+  Rec& s = *c.s;
+  c.yield[c.e * p.nq + q] = r.yielding ? 1 : 0;
+#pragma unroll
+  for (int i = 0; i < 36; ++i) M[i] = r.C[i];
+  if (p.kinematics == SBK_FINITE_LOGARITHMIC) {
+    log_transform(L, r.stress, S, M);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) S[i] = r.stress[i];
+  }
+  double mmax = 0.0;
+#pragma unroll
+  for (int i = 0; i < 36; ++i) {
+    s.slot[q][i] = M[i];
+    mmax = fmax(mmax, fabs(M[i]));
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) s.slot[q][kSlotS + i] = S[i];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) s.slot[q][kSlotF + i] = F[i];
+  s.slot[q][kSlotW] = w;
+  s.slot[q][kSlotE] = r.energy;
+  s.slot[q][kSlotFl] = w * mmax * hmax * (1.0 + hmax);
+}
+
+// The group's side of a pass after every point has its slot (or failed):
+// the first failure in the reference's order (the earliest stage, then the
+// lowest point), else K_aa and the force, scale and floor sums. fail =
+// (stage << 8) | q of this lane's failure (0: none), code its code.
+template <int G, class Rec>
+__device__ __forceinline__ int pass_sums(const Ctx<G, Rec>& c, bool active, int fail, int code, const double gt[9],
+                                         const double F[9], const double M[36], const double S[6], double w) {
+  Rec& s = *c.s;
+  const Params& p = *c.p;
+  const bool geometric = p.kinematics != SBK_SMALL_STRAIN;
+  double kbuf[G];
   // The failure of the group: the first point of the earliest stage.
   int key = fail ? fail : 0x7fffffff;
 #pragma unroll
@@ -523,6 +526,40 @@ __device__ __noinline__ int pass(const Ctx<G, Rec>& c, const double at[9]) {
   }
   c.sync();
   return 0;
+}
+
+
+// One pass (IncompatibleModes.cpp:337-342): the kinematics, the returns and
+// the sums at `at` (9 values, identical in every lane). Returns 0 or the
+// failure code of the first failing point in the reference's order.
+template <int G, class Rec>
+__device__ __noinline__ int pass(const Ctx<G, Rec>& c, const double at[9]) {
+  const Params& p = *c.p;
+  const int q = c.lane;
+  const bool active = q < p.nq;
+  int fail = 0;  // (stage << 8) | q, stage 1 kinematics, 2 return
+  int code = 0;
+  double gt[9], F[9], hmax = 0.0;
+  double M[36], S[6];
+  double w = 0.0;
+  if (active) {
+    w = c.s->geo[q][9];
+    double strain[6];
+    LogKin L;
+    code = point_kinematics(c, q, at, gt, F, hmax, strain, L);
+    if (code) fail = (1 << 8) | q;
+    if (!fail) {
+      PointState st{c.state + c.e * p.nq + q, c.trial + c.e * p.nq + q, c.npts};
+      Response r;
+      code = p.general ? general_return(p, strain, st, r, c.warm) : radial_return(p, strain, st, r);
+      if (code) {
+        fail = (2 << 8) | q;
+      } else {
+        point_slot(c, q, r, L, F, w, hmax, M, S);
+      }
+    }
+  }
+  return pass_sums(c, active, fail, code, gt, F, M, S, w);
 }
 
 // ---- element-level helpers (lane 0, shared memory) ---------------------------
@@ -1464,17 +1501,82 @@ __device__ __forceinline__ void append(int32_t* list, int32_t* count, int64_t e)
   list[pos] = (int32_t)e;
 }
 
+// Fields of a point's record between the three pass kernels (field f of
+// point q of element e at (e * kPw + f) * 8 + q).
+constexpr int kPwF = 0;        // F 9
+constexpr int kPwHmax = 9;     // the largest |H| entry
+constexpr int kPwL = 10;       // LogKin: axes 9, mu 3, first 6
+constexpr int kPwStrain = 28;  // the strain the return takes, 6
+constexpr int kPwStress = 34;  // the response: stress 6
+constexpr int kPwC = 40;       // C 36
+constexpr int kPwEnergy = 76;
+constexpr int kPwYield = 77;
+constexpr int kPw = 78;
+
+__device__ __forceinline__ double* pw_at(const WaveBuffers& w, int64_t e, int f, int q) {
+  return w.pw + (e * kPw + f) * 8 + q;
+}
+
+// Whether the general return will take its plastic branch for this strain
+// (the trial test of return_general_3d, Plasticity.cpp:337-352, as
+// general_return computes it). Only a guess for the work split: the
+// return itself decides, so a point sent either way gets the same answer.
+__device__ __forceinline__ bool general_is_plastic(const Params& p, const double strain[6], const PointState& st) {
+  if (!p.enabled) return false;
+  const double g = p.G;
+  const int nt = p.nterms;
+  double el[6], xi_tr[6];
+#pragma unroll
+  for (int i = 0; i < 6; ++i) el[i] = strain[i] - st.get(kFieldEp + i);
+  const double vol = el[0] + el[1] + el[2];
+  const double mean = vol / 3.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) xi_tr[i] = 2.0 * g * (el[i] - mean);
+#pragma unroll
+  for (int i = 3; i < 6; ++i) xi_tr[i] = g * el[i];
+#pragma unroll
+  for (int t = 0; t < SBK_MAX_BACKSTRESSES; ++t)
+    if (t < nt)
+#pragma unroll
+      for (int i = 0; i < 6; ++i) xi_tr[i] -= st.get(kFieldAlpha + 6 * t + i);
+  const double sy_n = yield_of(p, st.get(field_eqps(nt)));
+  double q = 0.0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    double v = 0.0;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) v += p.P[i * 6 + j] * xi_tr[j];
+    q += xi_tr[i] * v;
+  }
+  const double f_trial = sqrt(fmax(q, 0.0)) - sy_n;
+  return !(f_trial <= 1.0e-12 * sy_n);
+}
+
+__device__ __forceinline__ void store_response(const WaveBuffers& w, int64_t e, int q, const Response& r) {
+#pragma unroll
+  for (int i = 0; i < 6; ++i) *pw_at(w, e, kPwStress + i, q) = r.stress[i];
+#pragma unroll
+  for (int i = 0; i < 36; ++i) *pw_at(w, e, kPwC + i, q) = r.C[i];
+  *pw_at(w, e, kPwEnergy, q) = r.energy;
+  *pw_at(w, e, kPwYield, q) = r.yielding ? 1.0 : 0.0;
+}
+
+// Pass, first kernel: per point the kinematics at the trial modes and the
+// log strain; the response of every point the return takes elastically,
+// here; the points that will yield listed for wave_return_kernel. The first
+// round also stages the element and runs set_up.
 template <int G>
-__global__ void __launch_bounds__(128) wave_pass_kernel(const __grid_constant__ Params p, int64_t ne, int first,
-                                                        const int32_t* __restrict__ list,
-                                                        const int32_t* __restrict__ count, bool batch,
-                                                        const double* __restrict__ coords,
-                                                        const int32_t* __restrict__ conn,
-                                                        const double* __restrict__ u,
-                                                        const double* __restrict__ state,
-                                                        const double* __restrict__ alpha_n,
-                                                        double* __restrict__ trial, uint8_t* __restrict__ yield,
-                                                        const __grid_constant__ WaveBuffers w) {
+__global__ void __launch_bounds__(256) wave_pre_kernel(const __grid_constant__ Params p, int64_t ne, int first,
+                                                       const int32_t* __restrict__ list,
+                                                       const int32_t* __restrict__ count, bool batch,
+                                                       const double* __restrict__ coords,
+                                                       const int32_t* __restrict__ conn,
+                                                       const double* __restrict__ u, const double* __restrict__ state,
+                                                       const double* __restrict__ alpha_n,
+                                                       double* __restrict__ trial, uint8_t* __restrict__ yield,
+                                                       int32_t* __restrict__ plastic,
+                                                       int32_t* __restrict__ plastic_count,
+                                                       const __grid_constant__ WaveBuffers w) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int epb = blockDim.x / G;
   const int slot_in_block = threadIdx.x / G;
@@ -1488,8 +1590,8 @@ __global__ void __launch_bounds__(128) wave_pass_kernel(const __grid_constant__ 
   for (int64_t i = (int64_t)blockIdx.x * epb + slot_in_block; i < n; i += (int64_t)gridDim.x * epb) {
     const int64_t e = list ? (int64_t)list[i] : i;
     double hu_lane[9];
-    double warm_lane[8];
-    Ctx<G, PassShared<G>> c{&p, sh, lane, mask, e, ne * nq, state, trial, yield, hu_lane, warm_lane};
+    double* warm = w.warm + (e * 8 + lane) * 8;
+    Ctx<G, PassShared<G>> c{&p, sh, lane, mask, e, ne * nq, state, trial, yield, hu_lane, warm};
     __syncwarp(mask);
     int status = 0;
     double at[9];
@@ -1523,8 +1625,9 @@ __global__ void __launch_bounds__(128) wave_pass_kernel(const __grid_constant__ 
 #pragma unroll
         for (int k = 0; k < 9; ++k) at[k] = alpha_n ? alpha_n[e * 9 + k] : 0.0;
         for (int k = lane; k < 9; k += G) w.alpha[e * 9 + k] = at[k];
+        if (lane < 8)
 #pragma unroll
-        for (int k = 0; k < 8; ++k) warm_lane[k] = 0.0;  // no closest point yet (warm_lane[7] == 0)
+          for (int k = 0; k < 8; ++k) warm[k] = 0.0;  // no closest point yet (warm[7] == 0)
         c.sync();
         status = set_up<G>(c);
         if (!status) {
@@ -1546,13 +1649,156 @@ __global__ void __launch_bounds__(128) wave_pass_kernel(const __grid_constant__ 
         for (int f = 0; f < 12; ++f) s.geo[lane][f] = w.geo[(e * 12 + f) * G + lane];
 #pragma unroll
         for (int f = 0; f < 9; ++f) hu_lane[f] = w.hu[(e * 9 + f) * G + lane];
-#pragma unroll
-        for (int f = 0; f < 8; ++f) warm_lane[f] = w.warm[(e * 8 + f) * G + lane];
       }
       for (int k = lane; k < 9; k += G) s.jinv0[k] = w.jinv0[e * 9 + k];
       c.sync();
     }
-    if (!status) status = pass<G>(c, at);
+    // An element that failed before its points: every point's record says
+    // so (stage 0 sorts before the points' own failures).
+    int fail = status ? 1 : 0, code = status;
+    bool deferred = false;
+    const int q = lane;
+    if (!status && q < nq) {
+      double gt[9], F[9], hmax = 0.0, strain[6];
+      LogKin L;
+      code = point_kinematics(c, q, at, gt, F, hmax, strain, L);
+      if (code) fail = (1 << 8) | q;
+      if (!fail) {
+        PointState st{state + e * nq + q, trial + e * nq + q, ne * nq};
+        if (p.general && general_is_plastic(p, strain, st)) {
+          deferred = true;
+#pragma unroll
+          for (int k = 0; k < 6; ++k) *pw_at(w, e, kPwStrain + k, q) = strain[k];
+        } else {
+          Response r;
+          code = p.general ? general_return(p, strain, st, r, warm) : radial_return(p, strain, st, r);
+          if (code) fail = (2 << 8) | q;
+          else store_response(w, e, q, r);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) *pw_at(w, e, kPwF + k, q) = F[k];
+      *pw_at(w, e, kPwHmax, q) = hmax;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) *pw_at(w, e, kPwL + k, q) = L.q[k];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) *pw_at(w, e, kPwL + 9 + k, q) = L.mu[k];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) *pw_at(w, e, kPwL + 12 + k, q) = L.first[k];
+    }
+    if (q < 8) {
+      w.pfail[e * 8 + q] = fail;
+      w.pcodes[e * 8 + q] = code;
+    }
+    // The group's deferred points, appended together.
+    const unsigned ballot = __ballot_sync(mask, deferred);
+    int base = 0;
+    if (ballot) {
+      const unsigned mine = ballot >> ((threadIdx.x % 32) / G * G);
+      if (lane == 0) base = atomicAdd(plastic_count, __popc(mine));
+      base = __shfl_sync(mask, base, 0, G);
+      if (deferred) plastic[base + __popc(mine & ((1u << lane) - 1u))] = (int32_t)(e * 8 + q);
+    }
+  }
+}
+
+// Pass, second kernel: the general return of every listed point, a thread
+// each, so that a warp's 32 lanes all run the closest-point iteration.
+__global__ void __launch_bounds__(128) wave_return_kernel(const __grid_constant__ Params p, int64_t ne,
+                                                          const int32_t* __restrict__ plastic,
+                                                          const int32_t* __restrict__ plastic_count,
+                                                          const double* __restrict__ state,
+                                                          double* __restrict__ trial,
+                                                          const __grid_constant__ WaveBuffers w) {
+  const int64_t n = *plastic_count;
+  const int nq = p.nq;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t pt = plastic[i];
+    const int64_t e = pt >> 3;
+    const int q = (int)(pt & 7);
+    double strain[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) strain[k] = *pw_at(w, e, kPwStrain + k, q);
+    PointState st{state + e * nq + q, trial + e * nq + q, ne * nq};
+    Response r;
+    const int code = general_return(p, strain, st, r, w.warm + pt * 8);
+    if (code) {
+      w.pfail[pt] = (2 << 8) | q;
+      w.pcodes[pt] = code;
+    } else {
+      store_response(w, e, q, r);
+    }
+  }
+}
+
+// Pass, third kernel: per point the yield flag, the logarithmic map of the
+// response and the slot; per element the first failure, K_aa and the sums
+// (pass_sums) into the element's record.
+template <int G>
+__global__ void __launch_bounds__(256) wave_post_kernel(const __grid_constant__ Params p, int64_t ne,
+                                                        const int32_t* __restrict__ list,
+                                                        const int32_t* __restrict__ count,
+                                                        uint8_t* __restrict__ yield,
+                                                        const __grid_constant__ WaveBuffers w) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int epb = blockDim.x / G;
+  const int slot_in_block = threadIdx.x / G;
+  const int lane = threadIdx.x % G;
+  PassShared<G>* sh = reinterpret_cast<PassShared<G>*>(smem_raw) + slot_in_block;
+  const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
+  const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
+  const int64_t n = count ? (int64_t)*count : ne;
+  const int nq = p.nq;
+  PassShared<G>& s = *sh;
+  for (int64_t i = (int64_t)blockIdx.x * epb + slot_in_block; i < n; i += (int64_t)gridDim.x * epb) {
+    const int64_t e = list ? (int64_t)list[i] : i;
+    Ctx<G, PassShared<G>> c{&p, sh, lane, mask, e, ne * nq, nullptr, nullptr, yield, nullptr, nullptr};
+    __syncwarp(mask);
+    const int q = lane;
+    const bool active = q < nq;
+    int fail = 0, code = 0;
+    if (q < 8) {
+      fail = w.pfail[e * 8 + q];
+      code = w.pcodes[e * 8 + q];
+    }
+    // A failure before the points (stage 0): the whole element.
+    const int early = __shfl_sync(mask, fail == 1 ? code : 0, 0, G);
+    if (early) {
+      if (lane == 0) w.pcode[e] = early;
+      continue;
+    }
+    if (active) {
+#pragma unroll
+      for (int f = 0; f < 12; ++f) s.geo[q][f] = w.geo[(e * 12 + f) * G + q];
+    }
+    for (int k = lane; k < 9; k += G) s.jinv0[k] = w.jinv0[e * 9 + k];
+    c.sync();
+    double gt[9], F[9], M[36], S[6], w_q = 0.0;
+    if (active) {
+      w_q = s.geo[q][9];
+      mode_grads(c, q, gt);
+#pragma unroll
+      for (int k = 0; k < 9; ++k) F[k] = *pw_at(w, e, kPwF + k, q);
+      if (!fail) {
+        Response r;
+        LogKin L;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) r.stress[k] = *pw_at(w, e, kPwStress + k, q);
+#pragma unroll
+        for (int k = 0; k < 36; ++k) r.C[k] = *pw_at(w, e, kPwC + k, q);
+        r.energy = *pw_at(w, e, kPwEnergy, q);
+        r.yielding = *pw_at(w, e, kPwYield, q) != 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) L.q[k] = *pw_at(w, e, kPwL + k, q);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) L.mu[k] = *pw_at(w, e, kPwL + 9 + k, q);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) L.first[k] = *pw_at(w, e, kPwL + 12 + k, q);
+        const double hmax = *pw_at(w, e, kPwHmax, q);
+        point_slot(c, q, r, L, F, w_q, hmax, M, S);
+      }
+    }
+    const int status = pass_sums(c, active, fail, code, gt, F, M, S, w_q);
     if (lane == 0) w.pcode[e] = status;
     if (!status) {
       for (int k = lane; k < 81; k += G) w.kc[e * kKcStride + k] = s.kc[k];
@@ -1562,11 +1808,9 @@ __global__ void __launch_bounds__(128) wave_pass_kernel(const __grid_constant__ 
         w.sf[e * 19 + 9 + k] = s.flo[k];
       }
       if (lane == 0) w.sf[e * 19 + 18] = s.energy;
-      if (lane < nq) {
+      if (active) {
 #pragma unroll 6
-        for (int f = 0; f < kSlot; ++f) w.slot[(e * kSlot + f) * G + lane] = s.slot[lane][f];
-#pragma unroll
-        for (int f = 0; f < 8; ++f) w.warm[(e * 8 + f) * G + lane] = warm_lane[f];
+        for (int f = 0; f < kSlot; ++f) w.slot[(e * kSlot + f) * G + q] = s.slot[q][f];
       }
     }
   }
@@ -2824,11 +3068,15 @@ size_t carve_all(char* base, int64_t ne, WaveBuffers& w) {
   w.jinv0 = carve<double>(base, at, n * 9);
   w.hu = carve<double>(base, at, n * 9 * 8);
   w.warm = carve<double>(base, at, n * 8 * 8);
+  w.pw = carve<double>(base, at, n * kPw * 8);
+  w.pfail = carve<int32_t>(base, at, n * 8);
+  w.pcodes = carve<int32_t>(base, at, n * 8);
+  w.plastic = carve<int32_t>(base, at, n * 8);
   w.list[0] = carve<int32_t>(base, at, n);
   w.list[1] = carve<int32_t>(base, at, n);
   w.done = carve<int32_t>(base, at, n);
   w.fallback = carve<int32_t>(base, at, n);
-  w.counts = carve<int32_t>(base, at, kWaveRounds + 3);
+  w.counts = carve<int32_t>(base, at, 2 * kWaveRounds + 3);
   return at;
 }
 
@@ -2847,18 +3095,22 @@ int launch_elements_wave(const Params& p, int64_t ne, const double* coords, cons
                          const double* state, const double* alpha_n, int want_tangent, double* force,
                          double* tangent, double* energy, double* trial, double* alpha_out, uint8_t* yield,
                          int32_t* iterations, int32_t* code, int32_t* first_failure, bool batch,
-                         const int32_t* order, const WaveBuffers& w, cudaStream_t stream) {
+                         const int32_t* order, const WaveBuffers& w, int pass_epb, cudaStream_t stream) {
   constexpr int G = 8;
   if (!wave_applies(p)) return (int)cudaErrorInvalidValue;
   if (ne <= 0) return 0;
   constexpr int epb = 16;  // 4 warps per block
   const int threads = epb * G;
-  static size_t raised[4][64] = {};
-  const size_t smem_pass = sizeof(PassShared<G>) * epb;
+  // The pass kernel's block: pass_epb elements (0: 16).
+  const int pepb = pass_epb > 0 ? (pass_epb > 32 ? 32 : pass_epb) : 16;
+  static size_t raised[5][64] = {};
+  const size_t smem_pass = sizeof(PassShared<G>) * pepb;
+  const size_t smem_post = sizeof(PassShared<G>) * epb;
   const size_t smem_ctl = sizeof(ControlShared<G>) * epb;
   const size_t smem_cond = sizeof(CondenseShared<G>) * epb;
   const size_t smem_elem = sizeof(ElemShared<G>) * epb;
-  int rc = raise_smem(wave_pass_kernel<G>, smem_pass, raised[0]);
+  int rc = raise_smem(wave_pre_kernel<G>, smem_pass, raised[0]);
+  if (!rc) rc = raise_smem(wave_post_kernel<G>, smem_post, raised[4]);
   if (!rc) rc = raise_smem(wave_control_kernel<G>, smem_ctl, raised[1]);
   if (!rc) rc = raise_smem(wave_condense_kernel<G>, smem_cond, raised[2]);
   if (!rc) rc = raise_smem(element_list_kernel<G>, smem_elem, raised[3]);
@@ -2869,13 +3121,21 @@ int launch_elements_wave(const Params& p, int64_t ne, const double* coords, cons
   // elements) cost little more than the launch.
   const int64_t cap = 148 * 16;
   const unsigned grid = (unsigned)(need < cap ? need : cap);
-  cudaError_t err = cudaMemsetAsync(w.counts, 0, (kWaveRounds + 3) * sizeof(int32_t), stream);
+  const int64_t pneed = (ne + pepb - 1) / pepb;
+  const unsigned pgrid = (unsigned)(pneed < cap ? pneed : cap);
+  const int64_t rneed = (ne * 8 + 127) / 128;
+  const unsigned rgrid = (unsigned)(rneed < 148 * 8 ? rneed : 148 * 8);
+  cudaError_t err = cudaMemsetAsync(w.counts, 0, (2 * kWaveRounds + 3) * sizeof(int32_t), stream);
   if (err != cudaSuccess) return (int)err;
   for (int r = 0; r < kWaveRounds; ++r) {
     const int32_t* list = r == 0 ? order : w.list[r & 1];
     const int32_t* count = r == 0 ? nullptr : w.counts + r;
-    wave_pass_kernel<G><<<grid, threads, smem_pass, stream>>>(p, ne, r == 0, list, count, batch, coords, conn, u, state,
-                                                              alpha_n, trial, yield, w);
+    int32_t* plastic_count = w.counts + kWaveRounds + 3 + r;
+    wave_pre_kernel<G><<<pgrid, pepb * G, smem_pass, stream>>>(p, ne, r == 0, list, count, batch, coords, conn, u,
+                                                               state, alpha_n, trial, yield, w.plastic, plastic_count,
+                                                               w);
+    wave_return_kernel<<<rgrid, 128, 0, stream>>>(p, ne, w.plastic, plastic_count, state, trial, w);
+    wave_post_kernel<G><<<grid, threads, smem_post, stream>>>(p, ne, list, count, yield, w);
     wave_control_kernel<G><<<grid, threads, smem_ctl, stream>>>(p, ne, r == 0, list, count, w, w.list[(r + 1) & 1],
                                                                 w.counts + r + 1, code, first_failure);
   }

@@ -46,11 +46,15 @@ struct WaveBuffers {
   double* geo;      // ne x 12 x 8: J^-1, w det J, det0 / det per point
   double* jinv0;    // ne x 9
   double* hu;       // ne x 9 x 8: U G^T per point
-  double* warm;     // ne x 8 x 8: the points' last closest points
+  double* warm;     // ne x 8 x 8: the points' last closest points (8 per point, together)
+  double* pw;       // ne x 78 x 8: the points' records between the pass kernels
+  int32_t* pfail;   // ne x 8: (stage << 8) | point of a point's failure (1: the element's, before its points)
+  int32_t* pcodes;  // ne x 8: its code
+  int32_t* plastic; // ne x 8: points (e * 8 + q) listed for the return kernel
   int32_t* list[2]; // ne each: the elements of a round
   int32_t* done;    // ne: converged elements
   int32_t* fallback;  // ne: elements handed to the single kernel
-  int32_t* counts;  // rounds + 3: each round's count, then done, fallback
+  int32_t* counts;  // 2 rounds + 3: each round's count, done, fallback, each round's listed points
 };
 // Bytes of one allocation that wave_buffers_carve splits for ne elements.
 size_t wave_buffer_bytes(int64_t ne);
@@ -63,7 +67,8 @@ int launch_elements_wave(const Params& p, int64_t ne, const double* coords, cons
                          const double* state, const double* alpha_n, int want_tangent, double* force,
                          double* tangent, double* energy, double* trial, double* alpha_out, uint8_t* yield,
                          int32_t* iterations, int32_t* code, int32_t* first_failure, bool batch,
-                         const int32_t* order, const WaveBuffers& w, cudaStream_t stream);
+                         const int32_t* order, const WaveBuffers& w, int pass_elements_per_block,
+                         cudaStream_t stream);
 // The shape derivative: per element lambda . d f*/d X (24, node-major) into
 // out, at u with the committed points (state) and modes (alpha_n) as the
 // history and lambda a global DOF vector; the local iteration runs again to

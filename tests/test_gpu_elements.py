@@ -237,22 +237,35 @@ def _batch_both_ways(pkg, mat, X, ue, state_dev, alpha, cuda, rule=(2, 0)):
     return out["phases"], out["single"]
 
 
-def _assert_bit_identical(a, b):
+# The phase kernels and the single kernel run the same functions on the same
+# values, compiled into different kernels: the compiler may fuse a product
+# into a sum across a function boundary in one and not in the other, so
+# results may differ in the last bits. Every decision must be the same.
+SAME_TOL = 1.0e-13
+
+
+def _assert_same(a, b):
     for name in ("code", "iterations", "yielding"):
         assert torch.equal(getattr(a, name), getattr(b, name)), name
     ok = a.code == 0
     for name in ("force", "tangent", "energy", "alpha"):
         x, y = getattr(a, name)[ok], getattr(b, name)[ok]
-        assert torch.equal(x, y), (name, (x - y).abs().max().item())
-    assert torch.equal(a.states[:, ok], b.states[:, ok])
+        scale = y.abs().max().item() + 1e-300
+        assert (x - y).abs().max().item() <= SAME_TOL * scale, (name, (x - y).abs().max().item() / scale)
+    x, y = a.states[:, ok], b.states[:, ok]
+    for f in range(x.shape[0]):
+        scale = y[f].abs().max().item() + 1e-300
+        assert (x[f] - y[f]).abs().max().item() <= SAME_TOL * scale, f
 
 
-def test_phase_kernels_are_bit_identical_to_the_single_kernel(pkg, orc, cuda):
-    """The local iteration as phase kernels over all elements gives every
-    output of the single kernel to the bit: seeded microbenchmark elements
-    (most on the full-Newton-step road, a few handed back to the single
-    kernel) and the reference's reversal cases (line searches, shifted
-    direction, Levenberg-Marquardt) side by side, plus a failing element."""
+def test_phase_kernels_give_the_single_kernels_results(pkg, orc, cuda):
+    """The local iteration as phase kernels over all elements takes every
+    decision of the single kernel - status, local iteration count, yield
+    flag of every point - and gives its outputs to 1e-13 of their scale:
+    seeded microbenchmark elements (most on the full-Newton-step road, a few
+    handed back to the single kernel) and the reference's reversal cases
+    (line searches, shifted direction, Levenberg-Marquardt) side by side,
+    plus a failing element."""
     wl = importlib.import_module("springback-precomp_b200.workload")
     prob = wl.make_problem(40, 20, 2, seed=3, sample=512)
     mesh, mat = prob.mesh, prob.material
@@ -260,7 +273,7 @@ def test_phase_kernels_are_bit_identical_to_the_single_kernel(pkg, orc, cuda):
     ue = mesh.gather(prob.u)
     a, b = _batch_both_ways(pkg, mat, X, ue, prob.state, prob.alpha, cuda)
     assert int((a.code == 0).sum()) == mesh.num_elements
-    _assert_bit_identical(a, b)
+    _assert_same(a, b)
     # Reversals of several times the first strain, one element each, with a
     # crushed element beside them.
     for law in ("perfect", "chaboche", "hill", "j2"):
@@ -277,4 +290,4 @@ def test_phase_kernels_are_bit_identical_to_the_single_kernel(pkg, orc, cuda):
         al = np.repeat(first["alpha"].reshape(1, 9), 4, axis=0)
         a, b = _batch_both_ways(pkg, m, Xs, ues, st, al, cuda)
         assert int(a.code[3]) != 0
-        _assert_bit_identical(a, b)
+        _assert_same(a, b)
