@@ -1449,6 +1449,33 @@ struct __align__(16) PassShared {
   double energy;
 };
 
+// The first pass kernel's record: the staged element and its geometry.
+template <int G>
+struct __align__(16) PreShared {
+  double X[24];
+  double U[24];
+  double jinv0[9];
+  double geo[G][12];
+};
+
+// Minimum resident blocks per SM (128 threads each) the compiler is told
+// to fit, which bounds the registers of a thread: 2 allows 255, 3 170, 4
+// 128. Measured on the 1M-element microbenchmark: the return kernel gains
+// 11 % at 4 (more warps hide its latency, its spills stay small); the other
+// three lose 15-65 % at 3 or 4 (their spills grow).
+#ifndef SBK_MINB_PRE
+#define SBK_MINB_PRE 2
+#endif
+#ifndef SBK_MINB_RETURN
+#define SBK_MINB_RETURN 4
+#endif
+#ifndef SBK_MINB_POST
+#define SBK_MINB_POST 2
+#endif
+#ifndef SBK_MINB_CONDENSE
+#define SBK_MINB_CONDENSE 2
+#endif
+
 template <int G>
 struct __align__(16) ControlShared {
   double kc[kKcStride];
@@ -1517,41 +1544,6 @@ __device__ __forceinline__ double* pw_at(const WaveBuffers& w, int64_t e, int f,
   return w.pw + (e * kPw + f) * 8 + q;
 }
 
-// Whether the general return will take its plastic branch for this strain
-// (the trial test of return_general_3d, Plasticity.cpp:337-352, as
-// general_return computes it). Only a guess for the work split: the
-// return itself decides, so a point sent either way gets the same answer.
-__device__ __forceinline__ bool general_is_plastic(const Params& p, const double strain[6], const PointState& st) {
-  if (!p.enabled) return false;
-  const double g = p.G;
-  const int nt = p.nterms;
-  double el[6], xi_tr[6];
-#pragma unroll
-  for (int i = 0; i < 6; ++i) el[i] = strain[i] - st.get(kFieldEp + i);
-  const double vol = el[0] + el[1] + el[2];
-  const double mean = vol / 3.0;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) xi_tr[i] = 2.0 * g * (el[i] - mean);
-#pragma unroll
-  for (int i = 3; i < 6; ++i) xi_tr[i] = g * el[i];
-#pragma unroll
-  for (int t = 0; t < SBK_MAX_BACKSTRESSES; ++t)
-    if (t < nt)
-#pragma unroll
-      for (int i = 0; i < 6; ++i) xi_tr[i] -= st.get(kFieldAlpha + 6 * t + i);
-  const double sy_n = yield_of(p, st.get(field_eqps(nt)));
-  double q = 0.0;
-#pragma unroll
-  for (int i = 0; i < 6; ++i) {
-    double v = 0.0;
-#pragma unroll
-    for (int j = 0; j < 6; ++j) v += p.P[i * 6 + j] * xi_tr[j];
-    q += xi_tr[i] * v;
-  }
-  const double f_trial = sqrt(fmax(q, 0.0)) - sy_n;
-  return !(f_trial <= 1.0e-12 * sy_n);
-}
-
 __device__ __forceinline__ void store_response(const WaveBuffers& w, int64_t e, int q, const Response& r) {
 #pragma unroll
   for (int i = 0; i < 6; ++i) *pw_at(w, e, kPwStress + i, q) = r.stress[i];
@@ -1566,7 +1558,7 @@ __device__ __forceinline__ void store_response(const WaveBuffers& w, int64_t e, 
 // here; the points that will yield listed for wave_return_kernel. The first
 // round also stages the element and runs set_up.
 template <int G>
-__global__ void __launch_bounds__(256) wave_pre_kernel(const __grid_constant__ Params p, int64_t ne, int first,
+__global__ void __launch_bounds__(128, SBK_MINB_PRE) wave_pre_kernel(const __grid_constant__ Params p, int64_t ne, int first,
                                                        const int32_t* __restrict__ list,
                                                        const int32_t* __restrict__ count, bool batch,
                                                        const double* __restrict__ coords,
@@ -1581,17 +1573,17 @@ __global__ void __launch_bounds__(256) wave_pre_kernel(const __grid_constant__ P
   const int epb = blockDim.x / G;
   const int slot_in_block = threadIdx.x / G;
   const int lane = threadIdx.x % G;
-  PassShared<G>* sh = reinterpret_cast<PassShared<G>*>(smem_raw) + slot_in_block;
+  PreShared<G>* sh = reinterpret_cast<PreShared<G>*>(smem_raw) + slot_in_block;
   const unsigned lanes_mask = (G == 32) ? 0xffffffffu : ((1u << G) - 1u);
   const unsigned mask = lanes_mask << ((threadIdx.x % 32) / G * G);
   const int64_t n = count ? (int64_t)*count : ne;
   const int nq = p.nq;
-  PassShared<G>& s = *sh;
+  PreShared<G>& s = *sh;
   for (int64_t i = (int64_t)blockIdx.x * epb + slot_in_block; i < n; i += (int64_t)gridDim.x * epb) {
     const int64_t e = list ? (int64_t)list[i] : i;
     double hu_lane[9];
     double* warm = w.warm + (e * 8 + lane) * 8;
-    Ctx<G, PassShared<G>> c{&p, sh, lane, mask, e, ne * nq, state, trial, yield, hu_lane, warm};
+    Ctx<G, PreShared<G>> c{&p, sh, lane, mask, e, ne * nq, state, trial, yield, hu_lane, warm};
     __syncwarp(mask);
     int status = 0;
     double at[9];
@@ -1665,16 +1657,26 @@ __global__ void __launch_bounds__(256) wave_pre_kernel(const __grid_constant__ P
       if (code) fail = (1 << 8) | q;
       if (!fail) {
         PointState st{state + e * nq + q, trial + e * nq + q, ne * nq};
-        if (p.general && general_is_plastic(p, strain, st)) {
-          deferred = true;
+        Response r;
+        if (p.general) {
+          // The return's own trial test: its elastic branch here, its
+          // plastic branch (the whole return again) in wave_return_kernel.
+          GTrial T;
+          general_trial(p, strain, st, T);
+          if (!isfinite(T.f_trial)) {
+            code = kFailReturn;
+          } else if (general_is_elastic(p, T)) {
+            code = general_elastic(p, T, st, r);
+          } else {
+            deferred = true;
 #pragma unroll
-          for (int k = 0; k < 6; ++k) *pw_at(w, e, kPwStrain + k, q) = strain[k];
+            for (int k = 0; k < 6; ++k) *pw_at(w, e, kPwStrain + k, q) = strain[k];
+          }
         } else {
-          Response r;
-          code = p.general ? general_return(p, strain, st, r, warm) : radial_return(p, strain, st, r);
-          if (code) fail = (2 << 8) | q;
-          else store_response(w, e, q, r);
+          code = radial_return(p, strain, st, r);
         }
+        if (code) fail = (2 << 8) | q;
+        else if (!deferred) store_response(w, e, q, r);
       }
 #pragma unroll
       for (int k = 0; k < 9; ++k) *pw_at(w, e, kPwF + k, q) = F[k];
@@ -1704,7 +1706,7 @@ __global__ void __launch_bounds__(256) wave_pre_kernel(const __grid_constant__ P
 
 // Pass, second kernel: the general return of every listed point, a thread
 // each, so that a warp's 32 lanes all run the closest-point iteration.
-__global__ void __launch_bounds__(128) wave_return_kernel(const __grid_constant__ Params p, int64_t ne,
+__global__ void __launch_bounds__(128, SBK_MINB_RETURN) wave_return_kernel(const __grid_constant__ Params p, int64_t ne,
                                                           const int32_t* __restrict__ plastic,
                                                           const int32_t* __restrict__ plastic_count,
                                                           const double* __restrict__ state,
@@ -1735,7 +1737,7 @@ __global__ void __launch_bounds__(128) wave_return_kernel(const __grid_constant_
 // response and the slot; per element the first failure, K_aa and the sums
 // (pass_sums) into the element's record.
 template <int G>
-__global__ void __launch_bounds__(256) wave_post_kernel(const __grid_constant__ Params p, int64_t ne,
+__global__ void __launch_bounds__(128, SBK_MINB_POST) wave_post_kernel(const __grid_constant__ Params p, int64_t ne,
                                                         const int32_t* __restrict__ list,
                                                         const int32_t* __restrict__ count,
                                                         uint8_t* __restrict__ yield,
@@ -1950,7 +1952,7 @@ __global__ void __launch_bounds__(128) wave_control_kernel(const __grid_constant
 }
 
 template <int G>
-__global__ void __launch_bounds__(128) wave_condense_kernel(const __grid_constant__ Params p, int64_t ne,
+__global__ void __launch_bounds__(128, SBK_MINB_CONDENSE) wave_condense_kernel(const __grid_constant__ Params p, int64_t ne,
                                                             const __grid_constant__ WaveBuffers w, int want_tangent,
                                                             double* __restrict__ force, double* __restrict__ tangent,
                                                             double* __restrict__ energy,
@@ -3101,10 +3103,11 @@ int launch_elements_wave(const Params& p, int64_t ne, const double* coords, cons
   if (ne <= 0) return 0;
   constexpr int epb = 16;  // 4 warps per block
   const int threads = epb * G;
-  // The pass kernel's block: pass_epb elements (0: 16).
-  const int pepb = pass_epb > 0 ? (pass_epb > 32 ? 32 : pass_epb) : 16;
+  // The first pass kernel's block: pass_epb elements (0: 16), at most 16
+  // (its launch bounds assume 128 threads).
+  const int pepb = pass_epb > 0 ? (pass_epb > 16 ? 16 : pass_epb) : 16;
   static size_t raised[5][64] = {};
-  const size_t smem_pass = sizeof(PassShared<G>) * pepb;
+  const size_t smem_pass = sizeof(PreShared<G>) * pepb;
   const size_t smem_post = sizeof(PassShared<G>) * epb;
   const size_t smem_ctl = sizeof(ControlShared<G>) * epb;
   const size_t smem_cond = sizeof(CondenseShared<G>) * epb;

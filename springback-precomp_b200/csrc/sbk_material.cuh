@@ -422,6 +422,99 @@ __device__ __forceinline__ void gr_newton_step(const Params& p, const GPoint& e,
   j_solve(p, e, jf, r, -e.res[6], step);
 }
 
+// The trial state of the general return (Plasticity.cpp:337-352): the
+// elastic strain, the trial deviator and relative stress, the committed
+// terms, the yield stress and the overstress f_trial.
+struct GTrial {
+  double ep[6], el[6], s_trial[6], xi_tr[6];
+  Terms tn;
+  double vol, a_n, sy_n, eq_trial, f_trial;
+  bool loading_n;
+};
+
+__device__ __forceinline__ void general_trial(const Params& p, const double strain[6], const PointState& st,
+                                              GTrial& T) {
+  const double g = p.G;
+  const int nt = p.nterms;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    T.ep[i] = st.get(kFieldEp + i);
+    T.el[i] = strain[i] - T.ep[i];
+  }
+  T.vol = T.el[0] + T.el[1] + T.el[2];
+  {
+    const double mean = T.vol / 3.0;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) T.s_trial[i] = 2.0 * g * (T.el[i] - mean);
+#pragma unroll
+    for (int i = 3; i < 6; ++i) T.s_trial[i] = g * T.el[i];
+  }
+#pragma unroll
+  for (int i = 0; i < 6; ++i) T.xi_tr[i] = T.s_trial[i];
+#pragma unroll
+  for (int t = 0; t < SBK_MAX_BACKSTRESSES; ++t) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+      T.tn.a[t][i] = t < nt ? st.get(kFieldAlpha + 6 * t + i) : 0.0;
+      T.xi_tr[i] -= T.tn.a[t][i];
+    }
+  }
+  T.a_n = st.get(field_eqps(nt));
+  T.loading_n = st.get(field_loading(nt)) != 0.0;
+  T.sy_n = yield_of(p, T.a_n);
+  double q = 0.0;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) {
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) s += p.P[i * 6 + j] * T.xi_tr[j];
+    q += T.xi_tr[i] * s;
+  }
+  T.eq_trial = sqrt(fmax(q, 0.0));
+  T.f_trial = T.eq_trial - T.sy_n;
+}
+
+// Whether the return takes its elastic branch at this trial state.
+__device__ __forceinline__ bool general_is_elastic(const Params& p, const GTrial& T) {
+  return !p.enabled || T.f_trial <= 1.0e-12 * T.sy_n;
+}
+
+__device__ __forceinline__ double kinematic_energy(const Params& p, const double (*a)[6]) {
+  double o = 0.0;
+#pragma unroll
+  for (int t = 0; t < SBK_MAX_BACKSTRESSES; ++t) {
+    if (t < p.nterms) {
+      const double n = tnorm(a[t]);
+      o += 0.75 * n * n / p.termC[t];
+    }
+  }
+  return o;
+}
+
+// The elastic branch: the trial stress, the elastic tangent (the general
+// tangent at dl = 0 inside the loading window), the committed state with
+// the loading flag.
+__device__ __forceinline__ int general_elastic(const Params& p, const GTrial& T, const PointState& st, Response& out) {
+  const double g = p.G, k = p.K;
+  const int nt = p.nterms;
+#pragma unroll
+  for (int i = 0; i < 6; ++i) out.stress[i] = T.s_trial[i] + (i < 3 ? k * T.vol : 0.0);
+  elastic_C(p, out.C);
+  out.energy = 0.5 * k * T.vol * T.vol + g * dev_norm2(T.el) + isotropic_energy_of(p, T.a_n) + kinematic_energy(p, T.tn.a);
+  out.yielding = false;
+  bool loading = false;
+  if (p.enabled && T.loading_n && T.f_trial > -1.0e-10 * T.sy_n && T.eq_trial > 0.0) {
+    loading = true;
+    GPoint e;
+    if (gr_evaluate(p, T.s_trial, T.tn, T.a_n, T.xi_tr, 0.0, e)) gr_tangent(p, e, T.a_n, 0.0, out.C);
+  }
+  // The committed state with the loading flag.
+  const int nf = state_fields(nt);
+  for (int f = 0; f < nf - 1; ++f) st.put(f, st.get(f));
+  st.put(field_loading(nt), loading ? 1.0 : 0.0);
+  return 0;
+}
+
 // warm: the point's last converged closest point (xi 6, dl, valid flag) in
 // this element's local iteration, or NULL. The Newton iteration starts from
 // whichever of it and the trial state has the smaller residual; the converged
@@ -429,79 +522,16 @@ __device__ __forceinline__ void gr_newton_step(const Params& p, const GPoint& e,
 // one local iteration the warm start takes fewer steps. If a warm start does
 // not converge, the return runs again from the trial state, as the
 // reference's always does.
-__device__ __forceinline__ int general_return(const Params& p, const double strain[6], const PointState& st,
-                                           Response& out, double* warm = nullptr) {
+__device__ __forceinline__ int general_plastic(const Params& p, const GTrial& T, const PointState& st, Response& out,
+                                               double* warm) {
   const double g = p.G, k = p.K;
   const int nt = p.nterms;
-  double ep[6], el[6], s_trial[6];
-#pragma unroll
-  for (int i = 0; i < 6; ++i) {
-    ep[i] = st.get(kFieldEp + i);
-    el[i] = strain[i] - ep[i];
-  }
-  const double vol = el[0] + el[1] + el[2];
-  {
-    const double mean = vol / 3.0;
-#pragma unroll
-    for (int i = 0; i < 3; ++i) s_trial[i] = 2.0 * g * (el[i] - mean);
-#pragma unroll
-    for (int i = 3; i < 6; ++i) s_trial[i] = g * el[i];
-  }
-  Terms tn;
-  double xi_tr[6];
-#pragma unroll
-  for (int i = 0; i < 6; ++i) xi_tr[i] = s_trial[i];
-#pragma unroll
-  for (int t = 0; t < SBK_MAX_BACKSTRESSES; ++t) {
-#pragma unroll
-    for (int i = 0; i < 6; ++i) {
-      tn.a[t][i] = t < nt ? st.get(kFieldAlpha + 6 * t + i) : 0.0;
-      xi_tr[i] -= tn.a[t][i];
-    }
-  }
-  const double a_n = st.get(field_eqps(nt));
-  const bool loading_n = st.get(field_loading(nt)) != 0.0;
-  const double sy_n = yield_of(p, a_n);
-  double q = 0.0;
-#pragma unroll
-  for (int i = 0; i < 6; ++i) {
-    double s = 0.0;
-#pragma unroll
-    for (int j = 0; j < 6; ++j) s += p.P[i * 6 + j] * xi_tr[j];
-    q += xi_tr[i] * s;
-  }
-  const double eq_trial = sqrt(fmax(q, 0.0));
-  const double f_trial = eq_trial - sy_n;
-  if (!isfinite(f_trial)) return kFailReturn;
-  auto kin_energy = [&](const double (*a)[6]) {
-    double o = 0.0;
-#pragma unroll
-    for (int t = 0; t < SBK_MAX_BACKSTRESSES; ++t) {
-      if (t < nt) {
-        const double n = tnorm(a[t]);
-        o += 0.75 * n * n / p.termC[t];
-      }
-    }
-    return o;
-  };
-  if (!p.enabled || f_trial <= 1.0e-12 * sy_n) {
-#pragma unroll
-    for (int i = 0; i < 6; ++i) out.stress[i] = s_trial[i] + (i < 3 ? k * vol : 0.0);
-    elastic_C(p, out.C);
-    out.energy = 0.5 * k * vol * vol + g * dev_norm2(el) + isotropic_energy_of(p, a_n) + kin_energy(tn.a);
-    out.yielding = false;
-    bool loading = false;
-    if (p.enabled && loading_n && f_trial > -1.0e-10 * sy_n && eq_trial > 0.0) {
-      loading = true;
-      GPoint e;
-      if (gr_evaluate(p, s_trial, tn, a_n, xi_tr, 0.0, e)) gr_tangent(p, e, a_n, 0.0, out.C);
-    }
-    // The committed state with the loading flag.
-    const int nf = state_fields(nt);
-    for (int f = 0; f < nf - 1; ++f) st.put(f, st.get(f));
-    st.put(field_loading(nt), loading ? 1.0 : 0.0);
-    return 0;
-  }
+  const double* ep = T.ep;
+  const double* el = T.el;
+  const double* s_trial = T.s_trial;
+  const double* xi_tr = T.xi_tr;
+  const Terms& tn = T.tn;
+  const double vol = T.vol, a_n = T.a_n, sy_n = T.sy_n;
   double scale = sy_n;
 #pragma unroll
   for (int i = 0; i < 6; ++i) scale = fmax(scale, fmax(fabs(s_trial[i]), fabs(xi_tr[i])));
@@ -635,9 +665,19 @@ __device__ __forceinline__ int general_return(const Params& p, const double stra
       for (int i = 0; i < 6; ++i) st.put(kFieldAlpha + 6 * t + i, anew[t][i]);
   st.put(field_eqps(nt), a_n + dl);
   st.put(field_loading(nt), 1.0);
-  out.energy = 0.5 * k * vol * vol + g * dev_norm2(el_new) + isotropic_energy_of(p, a_n + dl) + kin_energy(anew);
+  out.energy = 0.5 * k * vol * vol + g * dev_norm2(el_new) + isotropic_energy_of(p, a_n + dl) + kinematic_energy(p, anew);
   gr_tangent(p, e, a_n, dl, out.C);
   return 0;
+}
+
+
+__device__ __forceinline__ int general_return(const Params& p, const double strain[6], const PointState& st,
+                                              Response& out, double* warm = nullptr) {
+  GTrial T;
+  general_trial(p, strain, st, T);
+  if (!isfinite(T.f_trial)) return kFailReturn;
+  if (general_is_elastic(p, T)) return general_elastic(p, T, st, out);
+  return general_plastic(p, T, st, out, warm);
 }
 
 // ---------------------------------------------------------------------------
