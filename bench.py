@@ -49,12 +49,16 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 PKG = "springback-precomp_b200"
 METRIC = "Hex8 tangent+residual+assembly elem/s (FP64)"
-# DRAM bytes (read + write) per element of one element-kernel launch:
-# ncu's dram__bytes_read.sum + dram__bytes_write.sum over one launch of the
-# same construction at 80,000 elements (200 x 200 x 2), 0.69 + 5.28 GB; the
-# traffic grows with the elements, so a launch of ne elements moves about ne
-# times this.
-K1_DRAM_BYTES_PER_ELEMENT = (0.692594688e9 + 5.275133e9) / 80000
+# DRAM bytes (read + write) per element of one evaluation's K1: ncu's
+# dram__bytes_read.sum + dram__bytes_write.sum summed over the phase kernels
+# of one evaluation of the same construction at 80,000 elements (200 x 200 x
+# 2): 23.79 GB (pre 8.13, return 8.01, post 5.85, control 0.51, condense
+# 0.93, the single kernel's share 0.37); the traffic grows with the
+# elements, so an evaluation of ne elements moves about ne times this.
+K1_DRAM_BYTES_PER_ELEMENT = 23.79e9 / 80000
+# The single kernel (--local-iteration single): 0.69 + 5.28 GB in one launch
+# at 80,000 elements.
+K1_SINGLE_DRAM_BYTES_PER_ELEMENT = (0.692594688e9 + 5.275133e9) / 80000
 # The same for the standard Hex8 kernel: 0.192 GB read + 1.610 GB written in
 # one launch at 80,000 elements.
 K1S_DRAM_BYTES_PER_ELEMENT = (0.191949568e9 + 1.610487e9) / 80000
@@ -795,10 +799,12 @@ def main():
             achieved = flops_per_element * ne / (el_ms / 1e3) / 1e12
             roofline = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                         "frac": achieved / fp64_peak,
-                        "traffic": (K1_DRAM_BYTES_PER_ELEMENT if args.element == "incompatible_modes"
-                                    else K1S_DRAM_BYTES_PER_ELEMENT) * ne,
-                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on "
-                                          "the 200x200x2 sheet (80,000 elements), scaled by elements",
+                        "traffic": (K1S_DRAM_BYTES_PER_ELEMENT if args.element != "incompatible_modes"
+                                    else K1_DRAM_BYTES_PER_ELEMENT if phases
+                                    else K1_SINGLE_DRAM_BYTES_PER_ELEMENT) * ne,
+                        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of K1's launches in "
+                                          "one evaluation of the 200x200x2 sheet (80,000 elements), scaled by "
+                                          "elements",
                         "kernel": k1_name, "kernel_ms": el_ms,
                         "flops_per_element": flops_per_element,
                         "peak_source": "measured in this run: cuBLAS FP64 GEMM 8192^3 burst (FP64 has no entry in "
