@@ -384,6 +384,19 @@ int sbk_contact_anticipate(sbk_contact* c, const double* u_dev, const double* du
                            double* residual_dev, int32_t* added, sbk_contact_result* out);
 /* ToolContact::commit (RigidTool.cpp:605-611). */
 int sbk_contact_commit(sbk_contact* c);
+/* How begin finds an increment's candidates (no counterpart in the
+ * reference, which scans every slave node, RigidTool.cpp:345-393; no result
+ * depends on it - the same test, the same set, the same order).
+ * SBK_SEARCH_GRID (the default): a spherical tool with a finite margin tests
+ * only the slave nodes of a uniform-grid hash's cells (edge R + margin) near
+ * its swept segment; other tools scan every slave. SBK_SEARCH_SCAN: every
+ * tool scans every slave node. */
+#define SBK_SEARCH_GRID 0
+#define SBK_SEARCH_SCAN 1
+int sbk_contact_set_search(sbk_contact* c, int mode);
+/* The candidate count of tool k from the last begin (host). */
+int sbk_contact_candidates(const sbk_contact* c, int32_t k, int32_t* count);
+
 /* The committed history of tool k (host): count, then per slave node in
  * contact (node, force xyz, relative xyz). */
 int sbk_contact_history(const sbk_contact* c, int32_t k, int32_t max_entries, double* out,

@@ -139,6 +139,8 @@ SIGNATURES = {
     "sbk_contact_anticipate": (_I, [_P, _P, _P, _D, _P, ctypes.POINTER(_I32), ctypes.POINTER(sbk_contact_result)]),
     "sbk_contact_commit": (_I, [_P]),
     "sbk_contact_history": (_I, [_P, _I32, _I32, ctypes.POINTER(_D), ctypes.POINTER(_I32)]),
+    "sbk_contact_set_search": (_I, [_P, _I]),
+    "sbk_contact_candidates": (_I, [_P, _I32, ctypes.POINTER(_I32)]),
     "sbk_evaluate_noalloc": (_I, [ctypes.POINTER(sbk_material), ctypes.POINTER(sbk_rule), _I, _I32, _I32]
                              + [_P] * 7 + [_I64] + [_P] * 7),
     "sbk_partition_create": (_I, [_I64, _P, _P, _I64, _I32, _P, ctypes.POINTER(_P)]),

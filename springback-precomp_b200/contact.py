@@ -105,6 +105,18 @@ class ToolContact:
     def set_stream(self, stream=None):
         _capi.check(_capi.lib().sbk_contact_set_stream(self._h, _stream_ptr(stream)))
 
+    def set_search(self, mode: str = "grid"):
+        """How begin_increment finds the candidates: "grid" (the default: a
+        uniform-grid hash of the slave nodes for spherical tools) or "scan"
+        (every slave node tested). The same candidates either way."""
+        _capi.check(_capi.lib().sbk_contact_set_search(self._h, {"grid": 0, "scan": 1}[mode]))
+
+    def candidates(self, k: int) -> int:
+        """Tool k's candidate count from the last begin_increment."""
+        n = ctypes.c_int32(0)
+        _capi.check(_capi.lib().sbk_contact_candidates(self._h, int(k), ctypes.byref(n)))
+        return int(n.value)
+
     def begin_increment(self, u0: torch.Tensor, t0: float, t1: float, active: Sequence[bool], margin: float):
         act = (ctypes.c_uint8 * max(1, len(self.tools)))(*[1 if a else 0 for a in active])
         _capi.check(_capi.lib().sbk_contact_begin(self._h, _ptr(u0.contiguous()), float(t0), float(t1), act,

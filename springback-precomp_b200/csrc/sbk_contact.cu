@@ -4,16 +4,23 @@
 // node-diagonal tangent, the semismooth anticipation and the friction
 // history.
 //
-// One thread per slave node and tool. The candidate test over all slave
-// nodes is a flat parallel scan (each node is tested once per tool and
-// increment, so no spatial hash is needed for the reference's few tools).
-// Results are compacted in slave order - the reference's order - so the
-// block list and every per-node sum match it; the gap and the candidate
-// distances use explicitly rounded products and sums (no fused
-// multiply-add), as a plain IEEE CPU build computes them, so the active set
-// agrees bit for bit. The tool's reference point c(t) is interpolated on the
-// host, as the reference does.
+// One thread per slave node and tool. The candidate search of an increment
+// (the slave nodes within R + margin of the tool's swept segment,
+// RigidTool.cpp:345-393, a linear scan there) runs for a spherical tool on
+// a uniform-grid hash of the slave nodes: they are binned by their position
+// at the start of the increment into cells of edge R + margin, and only the
+// cells the segment's box, grown by R + margin, overlaps are tested - with
+// the reference's distance test, so the candidates are the same set. Other
+// shapes (a plane's half space, a cylinder's infinite axis) and unbounded
+// margins take the flat scan of every slave. Results are compacted in slave
+// order - the reference's order - so the block list and every per-node sum
+// match it; the gap and the candidate distances use explicitly rounded
+// products and sums (no fused multiply-add), as a plain IEEE CPU build
+// computes them, so the active set agrees bit for bit. The tool's reference
+// point c(t) is interpolated on the host, as the reference does.
 #include <cuda_runtime.h>
+
+#include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cmath>
@@ -83,18 +90,11 @@ __device__ __forceinline__ void position(const double* coords, const double* u, 
   for (int k = 0; k < 3; ++k) x[k] = __dadd_rn(coords[3 * (int64_t)node + k], u[3 * (int64_t)node + k]);
 }
 
-__global__ void candidates_kernel(DTool t, int n, const int32_t* __restrict__ nodes, const double* __restrict__ coords,
-                                  const double* __restrict__ u0, double c0x, double c0y, double c0z, double c1x,
-                                  double c1y, double c1z, double margin, uint8_t* __restrict__ flag) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double x[3];
-  position(coords, u0, nodes[i], x);
-  const double c0[3] = {c0x, c0y, c0z}, c1[3] = {c1x, c1y, c1z};
-  bool cand = false;
-  if (t.shape == 0) {
-    cand = segment_distance(x, c0, c1) <= __dadd_rn(t.radius, margin);
-  } else if (t.shape == 2) {
+// The reference's candidate test of one node at x (RigidTool.cpp:345-393).
+__device__ bool candidate_test(const DTool& t, const double x[3], const double c0[3], const double c1[3],
+                               double margin) {
+  if (t.shape == 0) return segment_distance(x, c0, c1) <= __dadd_rn(t.radius, margin);
+  if (t.shape == 2) {
     double px[3], pc[3];
     const double dx[3] = {__dsub_rn(x[0], c0[0]), __dsub_rn(x[1], c0[1]), __dsub_rn(x[2], c0[2])};
     const double dc[3] = {__dsub_rn(c1[0], c0[0]), __dsub_rn(c1[1], c0[1]), __dsub_rn(c1[2], c0[2])};
@@ -105,27 +105,115 @@ __global__ void candidates_kernel(DTool t, int n, const int32_t* __restrict__ no
       pc[r] = rn_dot3(pr, dc);
     }
     const double zero[3] = {0, 0, 0};
-    cand = segment_distance(px, zero, pc) <= __dadd_rn(t.radius, margin);
-  } else {
-    const double d0[3] = {__dsub_rn(x[0], c0[0]), __dsub_rn(x[1], c0[1]), __dsub_rn(x[2], c0[2])};
-    const double d1[3] = {__dsub_rn(x[0], c1[0]), __dsub_rn(x[1], c1[1]), __dsub_rn(x[2], c1[2])};
-    cand = fmin(rn_dot3(t.n, d0), rn_dot3(t.n, d1)) <= margin;
+    return segment_distance(px, zero, pc) <= __dadd_rn(t.radius, margin);
   }
-  flag[i] = cand ? 1 : 0;
+  const double d0[3] = {__dsub_rn(x[0], c0[0]), __dsub_rn(x[1], c0[1]), __dsub_rn(x[2], c0[2])};
+  const double d1[3] = {__dsub_rn(x[0], c1[0]), __dsub_rn(x[1], c1[1]), __dsub_rn(x[2], c1[2])};
+  return fmin(rn_dot3(t.n, d0), rn_dot3(t.n, d1)) <= margin;
 }
 
-// Ordered compaction in one block: out[k] = i for the k-th i with flag[i],
-// *count = their number (the list stays in slave order).
-__global__ void compact_kernel(int n, const uint8_t* __restrict__ flag, int32_t* __restrict__ out,
-                               int32_t* __restrict__ count) {
+// The flat scan: every slave node tested.
+__global__ void candidates_kernel(DTool t, int n, const int32_t* __restrict__ nodes, const double* __restrict__ coords,
+                                  const double* __restrict__ u0, double c0x, double c0y, double c0z, double c1x,
+                                  double c1y, double c1z, double margin, uint8_t* __restrict__ flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x[3];
+  position(coords, u0, nodes[i], x);
+  const double c0[3] = {c0x, c0y, c0z}, c1[3] = {c1x, c1y, c1z};
+  flag[i] = candidate_test(t, x, c0, c1, margin) ? 1 : 0;
+}
+
+// ---- the uniform-grid hash of the slave nodes ----------------------------------
+// Cell (ix, iy, iz) = floor(x / h) of a position; its bucket a hash of the
+// three integers into a power-of-two table (colliding cells share a bucket;
+// the exact test sorts their nodes out).
+__device__ __host__ __forceinline__ uint32_t cell_bucket(long long ix, long long iy, long long iz, uint32_t mask) {
+  const unsigned long long hx = (unsigned long long)ix * 73856093ull;
+  const unsigned long long hy = (unsigned long long)iy * 19349663ull;
+  const unsigned long long hz = (unsigned long long)iz * 83492791ull;
+  return (uint32_t)((hx ^ hy ^ hz) & mask);
+}
+
+// The cell index of a coordinate; positions far outside any query (or not a
+// number) share one sentinel cell.
+__device__ __forceinline__ long long cell_of(double v, double inv_h) {
+  const double f = floor(v * inv_h);
+  return (f > 4.0e15 || f < -4.0e15 || f != f) ? (long long)4e15 : (long long)f;
+}
+
+__global__ void bin_kernel(int n, const int32_t* __restrict__ nodes, const double* __restrict__ coords,
+                           const double* __restrict__ u0, double inv_h, uint32_t mask, int32_t* __restrict__ key,
+                           int32_t* __restrict__ count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double x[3];
+  position(coords, u0, nodes[i], x);
+  const uint32_t b = cell_bucket(cell_of(x[0], inv_h), cell_of(x[1], inv_h), cell_of(x[2], inv_h), mask);
+  key[i] = (int32_t)b;
+  atomicAdd(&count[b], 1);
+}
+
+__global__ void bin_place_kernel(int n, const int32_t* __restrict__ key, const int32_t* __restrict__ start,
+                                 int32_t* __restrict__ fill, int32_t* __restrict__ binned) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int32_t b = key[i];
+  binned[start[b] + atomicAdd(&fill[b], 1)] = i;
+}
+
+// One block per cell of the query box (first cell ix0, iy0, iz0, extents
+// nx, ny): the nodes of its bucket through the exact test.
+__global__ void grid_query_kernel(DTool t, long long ix0, long long iy0, long long iz0, int nx, int ny,
+                                  uint32_t mask, const int32_t* __restrict__ start,
+                                  const int32_t* __restrict__ binned, const int32_t* __restrict__ nodes,
+                                  const double* __restrict__ coords, const double* __restrict__ u0, double c0x,
+                                  double c0y, double c0z, double c1x, double c1y, double c1z, double margin,
+                                  uint8_t* __restrict__ flag) {
+  const int cell = blockIdx.x;
+  const long long ix = ix0 + cell % nx, iy = iy0 + (cell / nx) % ny, iz = iz0 + cell / (nx * ny);
+  const uint32_t b = cell_bucket(ix, iy, iz, mask);
+  const double c0[3] = {c0x, c0y, c0z}, c1[3] = {c1x, c1y, c1z};
+  const int32_t end = start[b + 1];
+  for (int j = start[b] + threadIdx.x; j < end; j += blockDim.x) {
+    const int i = binned[j];
+    double x[3];
+    position(coords, u0, nodes[i], x);
+    if (candidate_test(t, x, c0, c1, margin)) flag[i] = 1;
+  }
+}
+
+// ---- ordered compaction over many blocks ---------------------------------------
+// out[k] = i for the k-th i with flag[i], *count their number: per-block
+// counts, their offsets (one block), the placement by ballots - the list in
+// slave order, the reference's order.
+constexpr int kCompactBlock = 256;
+// A query box of more cells than this takes the flat scan.
+constexpr long long kMaxQueryCells = 1 << 16;
+
+__global__ void flag_count_kernel(int n, const uint8_t* __restrict__ flag, int32_t* __restrict__ block_count) {
+  __shared__ int32_t warp_count[kCompactBlock / 32];
+  const int i = blockIdx.x * kCompactBlock + threadIdx.x;
+  const unsigned ballot = __ballot_sync(0xffffffffu, i < n && flag[i]);
+  if ((threadIdx.x & 31) == 0) warp_count[threadIdx.x >> 5] = __popc(ballot);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int32_t s = 0;
+    for (int w = 0; w < kCompactBlock / 32; ++w) s += warp_count[w];
+    block_count[blockIdx.x] = s;
+  }
+}
+
+// Exclusive offsets of nb block counts, in place; the total into *count.
+__global__ void block_offsets_kernel(int nb, int32_t* __restrict__ block_count, int32_t* __restrict__ count) {
   __shared__ int32_t warp_sums[32];
   __shared__ int32_t carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int base = 0; base < n; base += blockDim.x) {
+  for (int base = 0; base < nb; base += blockDim.x) {
     const int i = base + threadIdx.x;
-    const int f = (i < n && flag[i]) ? 1 : 0;
+    const int f = i < nb ? block_count[i] : 0;
     int v = f;
     for (int o = 1; o < 32; o <<= 1) {
       const int y = __shfl_up_sync(0xffffffffu, v, o);
@@ -142,13 +230,45 @@ __global__ void compact_kernel(int n, const uint8_t* __restrict__ flag, int32_t*
       warp_sums[lane] = w;
     }
     __syncthreads();
-    const int before = carry + (warp > 0 ? warp_sums[warp - 1] : 0) + v - f;
-    if (f) out[before] = i;
+    if (i < nb) block_count[i] = carry + (warp > 0 ? warp_sums[warp - 1] : 0) + v - f;
     __syncthreads();
     if (threadIdx.x == 0) carry += warp_sums[(blockDim.x >> 5) - 1];
     __syncthreads();
   }
   if (threadIdx.x == 0) *count = carry;
+}
+
+__global__ void flag_place_kernel(int n, const uint8_t* __restrict__ flag, const int32_t* __restrict__ block_offset,
+                                  int32_t* __restrict__ out) {
+  __shared__ int32_t warp_base[kCompactBlock / 32];
+  const int i = blockIdx.x * kCompactBlock + threadIdx.x;
+  const bool f = i < n && flag[i];
+  const unsigned ballot = __ballot_sync(0xffffffffu, f);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) warp_base[warp] = __popc(ballot);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int32_t s = block_offset[blockIdx.x];
+    for (int w = 0; w < kCompactBlock / 32; ++w) {
+      const int32_t c = warp_base[w];
+      warp_base[w] = s;
+      s += c;
+    }
+  }
+  __syncthreads();
+  if (f) out[warp_base[warp] + __popc(ballot & ((1u << lane) - 1u))] = i;
+}
+
+void ordered_compact(int n, const uint8_t* flag, int32_t* out, int32_t* count, int32_t* block_scratch,
+                     cudaStream_t st) {
+  const int nb = (n + kCompactBlock - 1) / kCompactBlock;
+  if (nb == 0) {
+    cudaMemsetAsync(count, 0, sizeof(int32_t), st);
+    return;
+  }
+  flag_count_kernel<<<nb, kCompactBlock, 0, st>>>(n, flag, block_scratch);
+  block_offsets_kernel<<<1, 1024, 0, st>>>(nb, block_scratch, count);
+  flag_place_kernel<<<nb, kCompactBlock, 0, st>>>(n, flag, block_scratch, out);
 }
 
 __global__ void moved_kernel(int n, const int32_t* __restrict__ nodes, const double* __restrict__ u,
@@ -474,6 +594,15 @@ struct HostTool {
   double* epscale = nullptr;
   int32_t* alist = nullptr;
   int32_t* nalist = nullptr;
+  int32_t* cblocks = nullptr;   // ordered compaction: per-block counts
+  // The uniform-grid hash of the slave nodes (rebuilt each increment).
+  uint32_t gmask = 0;           // table size - 1 (a power of two)
+  int32_t* gkey = nullptr;      // per slave: its bucket
+  int32_t* gcount = nullptr;    // per bucket (+1): count, then fill
+  int32_t* gstart = nullptr;    // per bucket (+1): first position in gbinned
+  int32_t* gbinned = nullptr;   // slaves by bucket
+  void* gscan = nullptr;        // the bucket scan's scratch
+  size_t gscan_bytes = 0;
 
   // ToolTrajectory::position (RigidTool.cpp:83-105), evaluated on the host.
   void position(double t, double out[3]) const {
@@ -527,6 +656,7 @@ struct sbk_contact {
   double* norms = nullptr;
   double* res_dev = nullptr;  // 6 per tool
   std::vector<double> resultants;
+  int search = SBK_SEARCH_GRID;
 };
 
 namespace {
@@ -542,7 +672,7 @@ void free_contact(sbk_contact* c) {
   for (HostTool& t : c->tools) {
     void* ptrs[] = {t.nodes, t.area, t.kappa, t.cflag, t.cand, t.ncand, t.h_flag, t.h_force, t.h_rel, t.t_flag,
                     t.t_force, t.t_rel, t.moved, t.act, t.slip, t.enode, t.eforce, t.ek, t.epen, t.epscale,
-                    t.alist, t.nalist};
+                    t.alist, t.nalist, t.cblocks, t.gkey, t.gcount, t.gstart, t.gbinned, t.gscan};
     for (void* p : ptrs)
       if (p) cudaFree(p);
   }
@@ -668,6 +798,22 @@ int sbk_contact_create(const sbk_mesh* mesh, int32_t num_tools, const sbk_tool* 
     TRYC(calloc_dev(&h.epscale, n));
     TRYC(calloc_dev(&h.alist, n));
     TRYC(calloc_dev(&h.nalist, 1));
+    TRYC(calloc_dev(&h.cblocks, (n + kCompactBlock - 1) / kCompactBlock + 1));
+    {
+      size_t table = 1024;
+      while (table < 2 * n) table <<= 1;
+      h.gmask = static_cast<uint32_t>(table - 1);
+      TRYC(calloc_dev(&h.gkey, n));
+      TRYC(calloc_dev(&h.gcount, table + 1));
+      TRYC(calloc_dev(&h.gstart, table + 1));
+      TRYC(calloc_dev(&h.gbinned, n));
+      if (cub::DeviceScan::ExclusiveSum(nullptr, h.gscan_bytes, h.gcount, h.gstart, static_cast<int>(table + 1)) !=
+          cudaSuccess) {
+        free_contact(c);
+        return cfail(SBK_ERR_CUDA, "grid scan size");
+      }
+      TRYC(calloc_dev(reinterpret_cast<char**>(&h.gscan), h.gscan_bytes));
+    }
     // Every slave a candidate until an increment is prepared.
     std::vector<int32_t> idx(n);
     for (size_t i = 0; i < n; ++i) idx[i] = static_cast<int32_t>(i);
@@ -720,11 +866,71 @@ int sbk_contact_begin(sbk_contact* c, const double* u0_dev, double t0, double t1
     double c0[3], c1[3];
     t.position(t0, c0);
     t.position(t1, c1);
-    candidates_kernel<<<(t.nslaves + 127) / 128, 128, 0, st>>>(t.d, t.nslaves, t.nodes, c->coords, u0_dev, c0[0],
-                                                              c0[1], c0[2], c1[0], c1[1], c1[2], margin, t.cflag);
-    compact_kernel<<<1, 1024, 0, st>>>(t.nslaves, t.cflag, t.cand, t.ncand);
+    // The grid for a sphere with a bounded reach: cells of edge R + margin,
+    // the query the cells of the segment's box grown by the reach (and by a
+    // hair more, for the rounding of the distance test).
+    const double reach = t.d.radius + margin;
+    bool grid = c->search == SBK_SEARCH_GRID && t.d.shape == 0 && std::isfinite(reach) && reach > 0.0;
+    long long lo[3] = {0, 0, 0}, ext[3] = {1, 1, 1};
+    const double inv_h = grid ? 1.0 / reach : 0.0;
+    if (grid) {
+      double scale = reach;
+      for (int k = 0; k < 3; ++k) scale = std::max(scale, std::max(std::fabs(c0[k]), std::fabs(c1[k])));
+      const double hair = 1.0e-9 * scale;
+      long long cells = 1;
+      for (int k = 0; k < 3; ++k) {
+        const double a = std::floor((std::min(c0[k], c1[k]) - reach - hair) * inv_h);
+        const double b = std::floor((std::max(c0[k], c1[k]) + reach + hair) * inv_h);
+        if (!std::isfinite(a) || !std::isfinite(b) || std::fabs(a) > 1.0e15 || std::fabs(b) > 1.0e15) {
+          grid = false;
+          break;
+        }
+        lo[k] = static_cast<long long>(a);
+        ext[k] = static_cast<long long>(b) - lo[k] + 1;
+        cells *= ext[k];
+        if (cells > kMaxQueryCells) {
+          grid = false;
+          break;
+        }
+      }
+    }
+    const int blocks = (t.nslaves + 127) / 128;
+    if (grid) {
+      const size_t table = static_cast<size_t>(t.gmask) + 1;
+      SBK_C(cudaMemsetAsync(t.gcount, 0, (table + 1) * sizeof(int32_t), st));
+      bin_kernel<<<blocks, 128, 0, st>>>(t.nslaves, t.nodes, c->coords, u0_dev, inv_h, t.gmask, t.gkey, t.gcount);
+      size_t bytes = t.gscan_bytes;
+      SBK_C(cub::DeviceScan::ExclusiveSum(t.gscan, bytes, t.gcount, t.gstart, static_cast<int>(table + 1), st));
+      SBK_C(cudaMemsetAsync(t.gcount, 0, table * sizeof(int32_t), st));
+      bin_place_kernel<<<blocks, 128, 0, st>>>(t.nslaves, t.gkey, t.gstart, t.gcount, t.gbinned);
+      SBK_C(cudaMemsetAsync(t.cflag, 0, t.nslaves, st));
+      const int cells = static_cast<int>(ext[0] * ext[1] * ext[2]);
+      grid_query_kernel<<<cells, 128, 0, st>>>(t.d, lo[0], lo[1], lo[2], static_cast<int>(ext[0]),
+                                               static_cast<int>(ext[1]), t.gmask, t.gstart, t.gbinned, t.nodes,
+                                               c->coords, u0_dev, c0[0], c0[1], c0[2], c1[0], c1[1], c1[2], margin,
+                                               t.cflag);
+    } else {
+      candidates_kernel<<<blocks, 128, 0, st>>>(t.d, t.nslaves, t.nodes, c->coords, u0_dev, c0[0], c0[1], c0[2],
+                                                c1[0], c1[1], c1[2], margin, t.cflag);
+    }
+    ordered_compact(t.nslaves, t.cflag, t.cand, t.ncand, t.cblocks, st);
   }
   SBK_C(cudaGetLastError());
+  return SBK_OK;
+}
+
+int sbk_contact_set_search(sbk_contact* c, int mode) {
+  if (!c) return cfail(SBK_ERR_ARGUMENT, "null contact");
+  if (mode != SBK_SEARCH_GRID && mode != SBK_SEARCH_SCAN) return cfail(SBK_ERR_ARGUMENT, "unknown search mode");
+  c->search = mode;
+  return SBK_OK;
+}
+
+int sbk_contact_candidates(const sbk_contact* c, int32_t k, int32_t* count) {
+  if (!c || !count || k < 0 || k >= static_cast<int32_t>(c->tools.size())) return cfail(SBK_ERR_ARGUMENT, "bad tool");
+  const HostTool& h = c->tools[k];
+  SBK_C(cudaMemcpyAsync(count, h.ncand, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+  SBK_C(cudaStreamSynchronize(c->stream));
   return SBK_OK;
 }
 
@@ -756,7 +962,7 @@ int sbk_contact_evaluate(sbk_contact* c, const double* u_dev, double t, int want
                                             c->margin, c->coords, u_dev, c->start, cc[0], cc[1], cc[2], c0[0],
                                             c0[1], c0[2], c->friction_tangent, h.h_flag, h.h_force, h.h_rel,
                                             h.t_flag, h.t_force, h.t_rel, h.ev(), c->flags);
-    compact_kernel<<<1, 1024, 0, st>>>(h.nslaves, h.act, h.alist, h.nalist);
+    ordered_compact(h.nslaves, h.act, h.alist, h.nalist, h.cblocks, st);
     // The block offset of this tool needs the count of the previous ones.
     SBK_C(cudaMemcpyAsync(&counts[k], h.nalist, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     SBK_C(cudaStreamSynchronize(st));
@@ -820,7 +1026,7 @@ int sbk_contact_anticipate(sbk_contact* c, const double* u_dev, const double* du
     SBK_C(cudaMemcpyAsync(&nc, h.ncand, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     SBK_C(cudaStreamSynchronize(st));
     if (nc < h.nslaves) SBK_C(cudaMemsetAsync(h.act + nc, 0, h.nslaves - nc, st));
-    compact_kernel<<<1, 1024, 0, st>>>(h.nslaves, h.act, h.alist, h.nalist);
+    ordered_compact(h.nslaves, h.act, h.alist, h.nalist, h.cblocks, st);
     int32_t n = 0;
     SBK_C(cudaMemcpyAsync(&n, h.nalist, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     SBK_C(cudaStreamSynchronize(st));

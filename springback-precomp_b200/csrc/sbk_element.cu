@@ -387,7 +387,42 @@ __device__ __forceinline__ void point_slot(const Ctx<G, Rec>& c, int q, const Re
 // the first failure in the reference's order (the earliest stage, then the
 // lowest point), else K_aa and the force, scale and floor sums. fail =
 // (stage << 8) | q of this lane's failure (0: none), code its code.
+// The nodal force f_u (24) and the energy of the pass from the points'
+// slots, in point order: lane a (a < 8) node a, lane 7 the energy.
 template <int G, class Rec>
+__device__ __forceinline__ void force_sums(const Ctx<G, Rec>& c) {
+  Rec& s = *c.s;
+  const Params& p = *c.p;
+  if (c.lane < 8) {
+    const int a = c.lane;
+    double ra[3] = {0, 0, 0}, en = 0.0;
+    for (int qq = 0; qq < p.nq; ++qq) {
+      const double* sl = s.slot[qq];
+      const double* Fq = sl + kSlotF;
+      const double* Sq = sl + kSlotS;
+      const double wq = sl[kSlotW];
+      double FS[9];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int j = 0; j < 3; ++j)
+          FS[k * 3 + j] = Fq[k * 3 + 0] * Sq[voigt(0, j)] + Fq[k * 3 + 1] * Sq[voigt(1, j)] + Fq[k * 3 + 2] * Sq[voigt(2, j)];
+      double g[3];
+      node_grad(c, qq, a, g);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) ra[k] += wq * (FS[k * 3 + 0] * g[0] + FS[k * 3 + 1] * g[1] + FS[k * 3 + 2] * g[2]);
+      if (a == 7) en += wq * sl[kSlotE];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) s.r[3 * a + k] = ra[k];
+    if (a == 7) s.energy = en;
+  }
+  c.sync();
+}
+
+// FORCES = false leaves out the nodal force and the energy (force_sums
+// gives them, the same sums, for the pass that ends the iteration).
+template <int G, class Rec, bool FORCES = true>
 __device__ __forceinline__ int pass_sums(const Ctx<G, Rec>& c, bool active, int fail, int code, const double gt[9],
                                          const double F[9], const double M[36], const double S[6], double w) {
   Rec& s = *c.s;
@@ -487,10 +522,12 @@ __device__ __forceinline__ int pass_sums(const Ctx<G, Rec>& c, bool active, int 
 #pragma unroll
         for (int j = 0; j < 3; ++j)
           FS[k * 3 + j] = Fq[k * 3 + 0] * Sq[voigt(0, j)] + Fq[k * 3 + 1] * Sq[voigt(1, j)] + Fq[k * 3 + 2] * Sq[voigt(2, j)];
-      double g[3];
-      node_grad(c, qq, a, g);
+      if (FORCES) {
+        double g[3];
+        node_grad(c, qq, a, g);
 #pragma unroll
-      for (int k = 0; k < 3; ++k) ra[k] += wq * (FS[k * 3 + 0] * g[0] + FS[k * 3 + 1] * g[1] + FS[k * 3 + 2] * g[2]);
+        for (int k = 0; k < 3; ++k) ra[k] += wq * (FS[k * 3 + 0] * g[0] + FS[k * 3 + 1] * g[1] + FS[k * 3 + 2] * g[2]);
+      }
       if (a < 3) {
         double gtq[9];
         mode_grads(c, qq, gtq);
@@ -510,10 +547,11 @@ __device__ __forceinline__ int pass_sums(const Ctx<G, Rec>& c, bool active, int 
           fl[k] += sl[kSlotFl] * s2;
         }
       }
-      if (a == 7) en += wq * sl[kSlotE];
+      if (FORCES && a == 7) en += wq * sl[kSlotE];
     }
+    if (FORCES)
 #pragma unroll
-    for (int k = 0; k < 3; ++k) s.r[3 * a + k] = ra[k];
+      for (int k = 0; k < 3; ++k) s.r[3 * a + k] = ra[k];
     if (a < 3) {
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
@@ -522,7 +560,7 @@ __device__ __forceinline__ int pass_sums(const Ctx<G, Rec>& c, bool active, int 
         s.flo[3 * a + k] = fl[k];
       }
     }
-    if (a == 7) s.energy = en;
+    if (FORCES && a == 7) s.energy = en;
   }
   c.sync();
   return 0;
@@ -1557,7 +1595,7 @@ __device__ __forceinline__ void store_response(const WaveBuffers& w, int64_t e, 
 // log strain; the response of every point the return takes elastically,
 // here; the points that will yield listed for wave_return_kernel. The first
 // round also stages the element and runs set_up.
-template <int G>
+template <int G, bool GENERAL>
 __global__ void __launch_bounds__(128, SBK_MINB_PRE) wave_pre_kernel(const __grid_constant__ Params p, int64_t ne, int first,
                                                        const int32_t* __restrict__ list,
                                                        const int32_t* __restrict__ count, bool batch,
@@ -1658,15 +1696,16 @@ __global__ void __launch_bounds__(128, SBK_MINB_PRE) wave_pre_kernel(const __gri
       if (!fail) {
         PointState st{state + e * nq + q, trial + e * nq + q, ne * nq};
         Response r;
-        if (p.general) {
-          // The return's own trial test: its elastic branch here, its
-          // plastic branch (the whole return again) in wave_return_kernel.
+        if (GENERAL) {
+          // The return's own trial test: its elastic branch outside the
+          // loading window here; the rest (the whole return again) in
+          // wave_return_kernel.
           GTrial T;
           general_trial(p, strain, st, T);
           if (!isfinite(T.f_trial)) {
             code = kFailReturn;
-          } else if (general_is_elastic(p, T)) {
-            code = general_elastic(p, T, st, r);
+          } else if (general_is_elastic(p, T) && !general_loading_window(p, T)) {
+            code = general_elastic<false>(p, T, st, r);
           } else {
             deferred = true;
 #pragma unroll
@@ -1800,16 +1839,18 @@ __global__ void __launch_bounds__(128, SBK_MINB_POST) wave_post_kernel(const __g
         point_slot(c, q, r, L, F, w_q, hmax, M, S);
       }
     }
-    const int status = pass_sums(c, active, fail, code, gt, F, M, S, w_q);
+    // The sums read the point's M, S and F back from its slot in shared
+    // memory, so that they need not stay in registers.
+    const double* sl = s.slot[q < nq ? q : 0];
+    const int status = pass_sums<G, PassShared<G>, false>(c, active, fail, code, gt, sl + kSlotF, sl, sl + kSlotS, w_q);
     if (lane == 0) w.pcode[e] = status;
     if (!status) {
       for (int k = lane; k < 81; k += G) w.kc[e * kKcStride + k] = s.kc[k];
-      for (int k = lane; k < 33; k += G) w.r[e * 33 + k] = s.r[k];
       for (int k = lane; k < 9; k += G) {
+        w.r[e * 33 + 24 + k] = s.r[24 + k];
         w.sf[e * 19 + k] = s.scale[k];
         w.sf[e * 19 + 9 + k] = s.flo[k];
       }
-      if (lane == 0) w.sf[e * 19 + 18] = s.energy;
       if (active) {
 #pragma unroll 6
         for (int f = 0; f < kSlot; ++f) w.slot[(e * kSlot + f) * G + q] = s.slot[q][f];
@@ -1985,11 +2026,12 @@ __global__ void __launch_bounds__(128, SBK_MINB_CONDENSE) wave_condense_kernel(c
       s.colp[k] = w.piv[e * 18 + 9 + k];
     }
     for (int k = lane; k < 81; k += G) s.lu[k] = w.kc[e * kKcStride + k];
-    for (int k = lane; k < 33; k += G) s.r[k] = w.r[e * 33 + k];
+    for (int k = lane; k < 9; k += G) s.r[24 + k] = w.r[e * 33 + 24 + k];
     c.sync();
+    force_sums(c);  // f_u and the energy of the last pass
     condense<G>(c, want_tangent, force, tangent);
     if (lane == 0) {
-      energy[e] = w.sf[e * 19 + 18];
+      energy[e] = s.energy;
       iterations[e] = w.iters[e];
       code[e] = 0;
     }
@@ -3106,13 +3148,14 @@ int launch_elements_wave(const Params& p, int64_t ne, const double* coords, cons
   // The first pass kernel's block: pass_epb elements (0: 16), at most 16
   // (its launch bounds assume 128 threads).
   const int pepb = pass_epb > 0 ? (pass_epb > 16 ? 16 : pass_epb) : 16;
-  static size_t raised[5][64] = {};
+  static size_t raised[6][64] = {};
   const size_t smem_pass = sizeof(PreShared<G>) * pepb;
   const size_t smem_post = sizeof(PassShared<G>) * epb;
   const size_t smem_ctl = sizeof(ControlShared<G>) * epb;
   const size_t smem_cond = sizeof(CondenseShared<G>) * epb;
   const size_t smem_elem = sizeof(ElemShared<G>) * epb;
-  int rc = raise_smem(wave_pre_kernel<G>, smem_pass, raised[0]);
+  auto pre = p.general ? wave_pre_kernel<G, true> : wave_pre_kernel<G, false>;
+  int rc = raise_smem(pre, smem_pass, raised[p.general ? 0 : 5]);
   if (!rc) rc = raise_smem(wave_post_kernel<G>, smem_post, raised[4]);
   if (!rc) rc = raise_smem(wave_control_kernel<G>, smem_ctl, raised[1]);
   if (!rc) rc = raise_smem(wave_condense_kernel<G>, smem_cond, raised[2]);
@@ -3134,9 +3177,8 @@ int launch_elements_wave(const Params& p, int64_t ne, const double* coords, cons
     const int32_t* list = r == 0 ? order : w.list[r & 1];
     const int32_t* count = r == 0 ? nullptr : w.counts + r;
     int32_t* plastic_count = w.counts + kWaveRounds + 3 + r;
-    wave_pre_kernel<G><<<pgrid, pepb * G, smem_pass, stream>>>(p, ne, r == 0, list, count, batch, coords, conn, u,
-                                                               state, alpha_n, trial, yield, w.plastic, plastic_count,
-                                                               w);
+    pre<<<pgrid, pepb * G, smem_pass, stream>>>(p, ne, r == 0, list, count, batch, coords, conn, u, state, alpha_n,
+                                                trial, yield, w.plastic, plastic_count, w);
     wave_return_kernel<<<rgrid, 128, 0, stream>>>(p, ne, w.plastic, plastic_count, state, trial, w);
     wave_post_kernel<G><<<grid, threads, smem_post, stream>>>(p, ne, list, count, yield, w);
     wave_control_kernel<G><<<grid, threads, smem_ctl, stream>>>(p, ne, r == 0, list, count, w, w.list[(r + 1) & 1],

@@ -491,9 +491,18 @@ __device__ __forceinline__ double kinematic_energy(const Params& p, const double
   return o;
 }
 
+// The loading window of the elastic branch (Plasticity.cpp:373): a point
+// loading at the last commit and within 1e-10 sigma_y of the surface keeps
+// loading, with the general tangent at dl = 0.
+__device__ __forceinline__ bool general_loading_window(const Params& p, const GTrial& T) {
+  return p.enabled && T.loading_n && T.f_trial > -1.0e-10 * T.sy_n && T.eq_trial > 0.0;
+}
+
 // The elastic branch: the trial stress, the elastic tangent (the general
 // tangent at dl = 0 inside the loading window), the committed state with
-// the loading flag.
+// the loading flag. WINDOW = false: for a point known to be outside the
+// window (the same result, without the window's code).
+template <bool WINDOW = true>
 __device__ __forceinline__ int general_elastic(const Params& p, const GTrial& T, const PointState& st, Response& out) {
   const double g = p.G, k = p.K;
   const int nt = p.nterms;
@@ -503,7 +512,7 @@ __device__ __forceinline__ int general_elastic(const Params& p, const GTrial& T,
   out.energy = 0.5 * k * T.vol * T.vol + g * dev_norm2(T.el) + isotropic_energy_of(p, T.a_n) + kinematic_energy(p, T.tn.a);
   out.yielding = false;
   bool loading = false;
-  if (p.enabled && T.loading_n && T.f_trial > -1.0e-10 * T.sy_n && T.eq_trial > 0.0) {
+  if (WINDOW && general_loading_window(p, T)) {
     loading = true;
     GPoint e;
     if (gr_evaluate(p, T.s_trial, T.tn, T.a_n, T.xi_tr, 0.0, e)) gr_tangent(p, e, T.a_n, 0.0, out.C);

@@ -200,3 +200,48 @@ def test_contact_blocks_into_the_system_tangent(pkg, orc, cuda):
     pat = orc.pattern(mesh.num_nodes, mesh.connectivity)
     ref = orc.add_node_blocks(pat, values.cpu().numpy(), cev.nodes.cpu().numpy(), cev.blocks.cpu().numpy())
     assert np.array_equal(ev.tangent.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("margin", [1.0e-6, 5.0e-4, 3.0e-3])
+def test_grid_search_finds_the_scans_candidates(pkg, orc, cuda, margin):
+    """The uniform-grid hash of the slave nodes (spherical tools) gives the
+    candidates of the reference's linear scan (RigidTool.cpp:345-393) - the
+    same count, and then the same active set, residual and blocks - over
+    increments whose swept segments are short, long, on cell boundaries and
+    far from the sheet, on a 60 x 60 x 2 sheet (3,721 top nodes) with a
+    deflected surface; and both equal the oracle's."""
+    mesh = sheet(pkg, n=60, h=0.25e-3)
+    nodes, area, kappa = top_slaves(mesh)
+    L = mesh.coords[:, 0].max()
+    ztop = mesh.coords[:, 2].max()
+    R = 2.0e-3
+    # Knots: a pass across the sheet, a jump along a cell boundary (x =
+    # k (R + margin)), a long diagonal and a leg high above the sheet.
+    h = R + margin
+    pts = [(0.2 * L, 0.3 * L, ztop + R - 1.0e-4), (0.8 * L, 0.35 * L, ztop + R - 1.5e-4),
+           (3 * h, 0.6 * L, ztop + R - 1.0e-4), (3 * h, 0.9 * L, ztop + R - 1.2e-4),
+           (0.9 * L, 0.1 * L, ztop + R - 0.8e-4), (0.9 * L, 0.1 * L, ztop + 0.05)]
+    times = [0.0, 0.2, 0.4, 0.6, 0.8, 1.0]
+    tool = dict(shape="sphere", times=times, points=pts, nodes=nodes, area=area, kappa=kappa, friction=0.1,
+                tangential_ratio=1.0, radius=R)
+    ref = orc.Contact(mesh.coords, [tool])
+    grid = pkg.ToolContact(mesh, [pkg.Tool(**tool)])
+    scan = pkg.ToolContact(mesh, [pkg.Tool(**tool)])
+    scan.set_search("scan")
+    u = displacements(mesh, 7, scale=1.0e-5)
+    steps = [(0.0, 0.1), (0.1, 0.3), (0.3, 0.45), (0.45, 0.7), (0.7, 0.9), (0.9, 1.0), (0.0, 1.0)]
+    seen = 0
+    for t0, t1 in steps:
+        counts = ref.begin_increment(u, t0, t1, [True], margin)
+        ud = torch.tensor(u, device=cuda)
+        grid.begin_increment(ud, t0, t1, [True], margin)
+        scan.begin_increment(ud, t0, t1, [True], margin)
+        assert grid.candidates(0) == scan.candidates(0) == counts[0], (t0, t1)
+        seen += counts[0]
+        r = ref.evaluate(u, t1, True)
+        eg = grid.evaluate(ud, t1, True)
+        es = scan.evaluate(ud, t1, True)
+        compare(eg, r, 1)
+        assert torch.equal(eg.nodes, es.nodes) and torch.equal(eg.residual, es.residual)
+        assert torch.equal(eg.blocks, es.blocks)
+    assert seen > 0
