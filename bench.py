@@ -515,6 +515,193 @@ def cpu_adjoint(pkg, n):
             "release_solve_ms": release_s * 1e3, "newton_iterations": iterations, "adjoint_ms": adjoint_s * 1e3}
 
 
+def run_cone(args, rank, world):
+    """The fine-mesh part: the truncated cone (18 mm footprint, 3 mm deep, 50
+    degree wall) in a 1 mm sheet of cone_n x cone_n x 4 IM Hex8 (224 x 224 x
+    4 = 200,704 elements by default), Hill48 + Chaboche, formed to 35 % of
+    its depth in committed increments, with the two tools of double-sided
+    forming on its wall. One step = one Newton iteration's device work:
+    NonlinearSystem.evaluate with the tangent, ToolContact.evaluate of both
+    tools with their blocks, and the blocks added into the tangent. Beside
+    it: the contact's share (K3), the candidate search of an increment by
+    the uniform-grid hash and by the flat scan, the candidate and active
+    counts."""
+    import torch
+
+    if world > 1 and rank != 0:
+        return 0
+    pkg = importlib.import_module(PKG)
+    wl = importlib.import_module(PKG + ".workload")
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = cone_cpu_baseline(args)
+    peaks = measured_peaks()
+    fp64_peak = fp64_peak_tflops(torch, dev)
+    t_setup = time.perf_counter()
+    sysm, prob = wl.make_cone_problem(args.cone_n, 4, device=dev)
+    mesh = prob.mesh
+    ne = mesh.num_elements
+    contact = pkg.ToolContact(mesh, [pkg.Tool(**t) for t in prob.tools], friction_tangent="exact")
+    u0 = torch.tensor(prob.u0, device=dev)
+    u = torch.tensor(prob.u, device=dev)
+    margin = 2.0e-3 + float(np.abs(prob.u - prob.u0).max()) + float(np.sqrt(prob.tools[0]["area"].min()))
+    contact.begin_increment(u0, 0.0, 1.0, [True, True], margin)
+    sysm.set_timing(True)
+    setup_s = time.perf_counter() - t_setup
+    stream = torch.cuda.current_stream()
+
+    def step():
+        ev = sysm.evaluate(u, 0.0, True)
+        cev = contact.evaluate(u, 1.0, True)
+        sysm.add_node_blocks(cev.nodes, cev.blocks)
+        return ev, cev
+
+    for _ in range(args.warmup):
+        ev, cev = step()
+    torch.cuda.synchronize()
+    elem_ms, k3_ms = [], []
+    with ClockSampler(0) as clocks:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("timed_steps")
+        e0.record(stream)
+        for _ in range(args.steps):
+            ev = sysm.evaluate(u, 0.0, True)
+            elem_ms.append(sysm.last_timings()["element"])
+            c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            c0.record(stream)
+            cev = contact.evaluate(u, 1.0, True)
+            c1.record(stream)
+            sysm.add_node_blocks(cev.nodes, cev.blocks)
+            c1.synchronize()
+            k3_ms.append(c0.elapsed_time(c1))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+    ms = e0.elapsed_time(e1) / args.steps
+
+    def begin_ms(mode, reps=10):
+        contact.set_search(mode)
+        contact.begin_increment(u0, 0.0, 1.0, [True, True], margin)
+        torch.cuda.synchronize()
+        b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        for _ in range(reps):
+            contact.begin_increment(u0, 0.0, 1.0, [True, True], margin)
+        b1.record(stream)
+        torch.cuda.synchronize()
+        return b0.elapsed_time(b1) / reps, [contact.candidates(k) for k in range(2)]
+
+    grid_ms, grid_cand = begin_ms("grid")
+    scan_ms, scan_cand = begin_ms("scan")
+    assert grid_cand == scan_cand, (grid_cand, scan_cand)
+    contact.set_search("grid")
+    # End to end through the public calls with host buffers.
+    u_host = u.cpu().pin_memory()
+    f_host = torch.empty(sysm.num_dofs, dtype=torch.float64).pin_memory()
+    v_host = torch.empty(sysm.nnz, dtype=torch.float64).pin_memory()
+    u_dev = torch.empty_like(u)
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    s0.record(stream)
+    for _ in range(args.steps):
+        u_dev.copy_(u_host, non_blocking=True)
+        ev = sysm.evaluate(u_dev, 0.0, True)
+        cev = contact.evaluate(u_dev, 1.0, True)
+        sysm.add_node_blocks(cev.nodes, cev.blocks)
+        f_host.copy_(ev.internal, non_blocking=True)
+        v_host.copy_(ev.tangent, non_blocking=True)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = s0.elapsed_time(s1) / args.steps
+    el_ms = statistics.mean(elem_ms)
+    flops = None
+    if not args.no_cpu_baseline:
+        flops = cone_flops_per_element(args)
+    roofline = None
+    if flops:
+        achieved = flops * ne / (el_ms / 1e3) / 1e12
+        roofline = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                    "frac": achieved / fp64_peak, "traffic": None, "kernel": "K1 (phase kernels)",
+                    "kernel_ms": el_ms, "flops_per_element": flops,
+                    "peak_source": "measured in this run: cuBLAS FP64 GEMM 8192^3 burst"}
+    line = {"metric": METRIC + " with two-tool contact", "value": ne / (ms / 1e3), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"fine-mesh part: truncated cone (18 mm footprint, 3 mm deep, 50 deg wall) in a "
+                                   f"1 mm sheet of {args.cone_n}x{args.cone_n}x4 IM Hex8 ({ne} elements), Hill48 + "
+                                   "Chaboche, formed to 35% of its depth; forming and support balls (R 2 mm) on the "
+                                   "wall; one step = evaluate with tangent + both tools' contact + their blocks",
+                       "l2": "inputs larger than L2"},
+            "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": {"value": ne / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 8 * sysm.num_dofs,
+                    "d2h_bytes_per_step": 8 * (sysm.num_dofs + sysm.nnz), "ms_per_step": e2e_ms},
+            "phases_ms": {"element": el_ms, "contact_evaluate": statistics.mean(k3_ms)},
+            "contact": {"begin_grid_ms": grid_ms, "begin_scan_ms": scan_ms, "candidates": grid_cand,
+                        "active": [int(cev.tools[k][6]) for k in range(2)],
+                        "slaves": [int(len(t["nodes"])) for t in prob.tools], "margin_m": margin},
+            "gpu_launches": None, "clocks": clocks.summary(), "yielding_fraction": ev.yielding_points / (8.0 * ne),
+            "setup_s": setup_s}
+    print(json.dumps(line), flush=True)
+    contact.close()
+    return 0
+
+
+def cone_sample(orc, n):
+    """A small cone part of the same construction on the CPU (the oracle's
+    element routines load its history)."""
+    wl = importlib.import_module(PKG + ".workload")
+    mesh = wl.cone_sheet(n, 4)
+    mat = importlib.import_module(PKG + ".material").hill_chaboche_sheet()
+    cone = wl.cone_part()
+    steps, s = 7, 0.35
+    committed = np.zeros((mesh.num_elements, 8, orc.NF))
+    alpha = np.zeros((mesh.num_elements, 9))
+    X = mesh.element_coordinates()
+    for k in range(1, steps + 1):
+        uk = (wl.formed_positions(mesh, cone, k * s / steps) - mesh.coords).reshape(-1)
+        r = orc.elements(mat.as_dict(), X, mesh.gather(uk), committed, alpha, want_tangent=False)
+        ok = r["status"] == 0
+        committed = np.where(ok[:, None, None], r["states"], committed)
+        alpha = np.where(ok[:, None], r["alpha"], alpha)
+    u = (wl.formed_positions(mesh, cone, s + 0.25 * s / steps) - mesh.coords).reshape(-1)
+    return mesh, mat, committed, alpha, u
+
+
+def cone_cpu_baseline(args):
+    """The oracle (-O3 -march=native, all host threads) on a cone_sample_n x
+    cone_sample_n x 4 part of the same construction: elements / s of its
+    NonlinearSystem::evaluate with the tangent."""
+    orc = oracle_module()
+    orc.use_variant("fast")
+    try:
+        mesh, mat, committed, alpha, u = cone_sample(orc, args.cone_sample_n)
+        cores = cpu_count()
+        pat = orc.pattern(mesh.num_nodes, mesh.connectivity)
+        orc.system_evaluate(mat.as_dict(), mesh.coords, mesh.connectivity, u, committed, alpha, threads=cores,
+                            pat=pat)
+        times = []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            r = orc.system_evaluate(mat.as_dict(), mesh.coords, mesh.connectivity, u, committed, alpha, threads=cores,
+                                    pat=pat)
+            times.append(time.perf_counter() - t0)
+        value = mesh.num_elements / statistics.median(times)
+        return {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "build": orc.FAST_FLAGS,
+                "sample": f"{mesh.num_elements} elements ({args.cone_sample_n}x{args.cone_sample_n}x4 cone part of the "
+                          f"same construction), median of 3 evaluations with the tangent (code {r['code']})"}
+    finally:
+        orc.use_variant("strict")
+
+
+def cone_flops_per_element(args):
+    orc = oracle_module()
+    mesh, mat, committed, alpha, u = cone_sample(orc, min(args.cone_sample_n, 24))
+    cnt = orc.count_flops(mat.as_dict(), mesh.element_coordinates(), mesh.gather(u), committed, alpha)
+    return cnt / mesh.num_elements
+
+
 def run_partition(args, rank, world):
     """The free-free block of a Dirichlet partition (PartitionedFactor,
     Forming.cpp:59-241): one step = the gather of the block's values from
@@ -663,12 +850,16 @@ def main():
                    help="the local iteration as phase kernels over the mesh (default) or one kernel per element")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
-    p.add_argument("--workload", default="microbench", choices=["microbench", "batched", "partition", "adjoint"],
+    p.add_argument("--cone-n", type=int, default=224)
+    p.add_argument("--cone-sample-n", type=int, default=48)
+    p.add_argument("--workload", default="microbench",
+                   choices=["microbench", "batched", "partition", "adjoint", "cone"],
                    help="batched: the design-sweep batch (64 parts of 20k-150k elements) in one launch against the "
                         "same parts evaluated one at a time; partition: the free-free block of a Dirichlet "
                         "partition gathered from the full tangent, and the factorisation it feeds; adjoint: the "
                         "springback gradient with respect to 400 commanded heights against one release solve and "
-                        "central differences")
+                        "central differences; cone: the fine-mesh truncated cone (200k elements) with the two tools "
+                        "of double-sided forming")
     p.add_argument("--element", default="incompatible_modes", choices=["incompatible_modes", "standard"],
                    help="standard: the standard Hex8 with mean dilatation on the same sheet and history")
     p.add_argument("--part-nx", type=int, default=200)
@@ -691,6 +882,8 @@ def main():
         return run_partition(args, rank, world)
     if args.workload == "adjoint":
         return run_adjoint(args, rank, world)
+    if args.workload == "cone":
+        return run_cone(args, rank, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

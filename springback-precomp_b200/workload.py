@@ -228,3 +228,157 @@ def gpu_evaluate(mesh, material, u, state, alpha, want_yield=False):
     return out_st, out_a, codes
 
 
+
+
+# ---- the fine-mesh part: a truncated cone formed in a 4-layer sheet ---------
+
+# The cone of the fine-mesh configuration: an 18 mm footprint, 3 mm deep, a
+# 50 degree wall (2 mm fillets at rim and floor), in a 1 mm sheet.
+CONE = dict(footprint_radius=9.0e-3, wall_angle_deg=50.0, depth=3.0e-3, top_fillet=2.0e-3, bottom_fillet=2.0e-3)
+CONE_BLANK = 24.0e-3    # m, the square blank the cone is formed in
+CONE_THICKNESS = 1.0e-3
+TOOL_RADIUS = 2.0e-3    # both tools: the forming ball above, the support ball below
+TOOL_TRAVEL = 5.0e-5    # m, the tools' travel in one increment (half the in-plane cell)
+
+
+@dataclasses.dataclass
+class ConeProblem:
+    mesh: HexMesh
+    material: Material
+    cone: object
+    s: float                 # the fraction of the cone's depth formed
+    u0: np.ndarray           # committed displacement (start of the increment)
+    u: np.ndarray            # evaluated displacement (end of the increment)
+    tools: list              # two dicts of Tool arguments: forming (top), support (bottom)
+    contact_radius: float    # m, where the tools act on the wall
+
+
+def cone_part():
+    from .parts import TruncatedCone
+
+    return TruncatedCone.with_footprint(**CONE)
+
+
+def cone_sheet(n: int = 224, layers: int = 4) -> HexMesh:
+    """The blank: n x n x layers Hex8 over CONE_BLANK square, 1 mm thick, its
+    top face at z = 0, centred on the cone's axis."""
+    return structured_hex_mesh(n, n, layers, CONE_BLANK, CONE_BLANK, CONE_THICKNESS, x0=-0.5 * CONE_BLANK,
+                               y0=-0.5 * CONE_BLANK, z0=-CONE_THICKNESS)
+
+
+def formed_positions(mesh: HexMesh, cone, s: float) -> np.ndarray:
+    """The sheet laid onto the surface z = s h(x, y) (s of the cone's depth):
+    each mid-surface point moves to the surface, each through-thickness
+    fibre follows the surface normal, shortened by the sine law (t cos of the
+    local wall angle), so that the wall thins as in incremental forming."""
+    x, y, z = mesh.coords[:, 0], mesh.coords[:, 1], mesh.coords[:, 2]
+    zm = -0.5 * CONE_THICKNESS
+    eps = 1.0e-7
+    h = s * cone.height(x, y)
+    hx = s * (cone.height(x + eps, y) - cone.height(x - eps, y)) / (2 * eps)
+    hy = s * (cone.height(x, y + eps) - cone.height(x, y - eps)) / (2 * eps)
+    norm = np.sqrt(1.0 + hx * hx + hy * hy)
+    n = np.stack([-hx, -hy, np.ones_like(hx)], axis=1) / norm[:, None]
+    off = (z - zm) / norm  # the fibre, thinned by cos = 1 / norm
+    return np.stack([x, y, zm + h], axis=1) + off[:, None] * n
+
+
+def slave_faces(mesh: HexMesh, top: bool, penalty: float = 10.0, young: float = 70.0e9):
+    """The nodes of the sheet's top (or bottom) face with their tributary
+    areas (a quarter of each adjacent cell) and penalties kappa = penalty E /
+    sqrt(area) (ToolContact's constructor, RigidTool.cpp:292-321)."""
+    z = mesh.coords[:, 2]
+    nodes = np.flatnonzero(np.isclose(z, z.max() if top else z.min()))
+    x, y = mesh.coords[nodes, 0], mesh.coords[nodes, 1]
+    hx = np.diff(np.unique(x)).min()
+    hy = np.diff(np.unique(y)).min()
+    wx = np.where(np.isclose(x, x.min()) | np.isclose(x, x.max()), 0.5, 1.0)
+    wy = np.where(np.isclose(y, y.min()) | np.isclose(y, y.max()), 0.5, 1.0)
+    area = wx * wy * hx * hy
+    return nodes.astype(np.int32), area, penalty * young / np.sqrt(area)
+
+
+def place_ball(faces: np.ndarray, point: np.ndarray, normal: np.ndarray, radius: float, penetration: float):
+    """The centre c = point + d normal of a ball of `radius` whose deepest
+    face node lies `penetration` inside it (min |x - c| = radius -
+    penetration), d found by bisection."""
+    near = faces[np.linalg.norm(faces - point, axis=1) < 3.0 * radius]
+
+    def gap(d):
+        return np.linalg.norm(near - (point + d * normal), axis=1).min() - (radius - penetration)
+
+    lo, hi = 0.0, 2.0 * radius
+    for _ in range(80):
+        mid = 0.5 * (lo + hi)
+        if gap(mid) < 0.0:
+            lo = mid
+        else:
+            hi = mid
+    return point + 0.5 * (lo + hi) * normal
+
+
+def make_cone_problem(n: int = 224, layers: int = 4, s: float = 0.35, steps: int = 7, device=None,
+                      material: Optional[Material] = None, penetration: float = 5.0e-5, friction: float = 0.1):
+    """The fine-mesh configuration a third of the way through forming: the
+    cone formed to s of its depth in `steps` committed increments (the
+    element kernel loading every element's history), the evaluated
+    increment a quarter step further, and the two tools of double-sided
+    forming - the forming ball on the top face and the support ball under
+    the bottom face, on the wall, moving along the spiral by TOOL_TRAVEL in
+    the increment, each `penetration` into its face at both ends of the
+    increment. Returns (system, ConeProblem)."""
+    import torch
+
+    from .system import NonlinearSystem, element_batch
+
+    dev = torch.device(device or "cuda")
+    mesh = cone_sheet(n, layers)
+    material = material or hill_chaboche_sheet()
+    cone = cone_part()
+    ds = s / steps
+    sysm = NonlinearSystem(mesh, material, kinematics="logarithmic")
+    cs, ca = sysm.committed_views()
+    cs.zero_()
+    ca.zero_()
+    conn_all = torch.tensor(mesh.connectivity, device=dev).long()
+    coords = torch.tensor(mesh.coords, device=dev)
+    chunk = 262144
+    for k in range(1, steps + 1):
+        uk = torch.tensor((formed_positions(mesh, cone, k * ds) - mesh.coords), device=dev)
+        for lo in range(0, mesh.num_elements, chunk):
+            hi = min(mesh.num_elements, lo + chunk)
+            cc = conn_all[lo:hi]
+            r = element_batch(material, coords[cc].reshape(-1, 24).contiguous(), uk[cc].reshape(-1, 24).contiguous(),
+                              cs[:, lo:hi].contiguous(), ca[lo:hi].contiguous(), want_tangent=False)
+            ok = r.code == 0
+            cs[:, lo:hi] = torch.where(ok[None, :, None], r.states, cs[:, lo:hi])
+            ca[lo:hi] = torch.where(ok[:, None], r.alpha, ca[lo:hi])
+    fracs = (s, s + 0.25 * ds)
+    pos = [formed_positions(mesh, cone, f) for f in fracs]
+    u0 = (pos[0] - mesh.coords).reshape(-1)
+    u1 = (pos[1] - mesh.coords).reshape(-1)
+    # The tools on the wall, where its slope is steepest.
+    prof_r = np.linspace(0.0, CONE["footprint_radius"], 4001)
+    hr = cone.height(prof_r, 0 * prof_r)
+    rc = float(prof_r[np.argmax(np.abs(np.gradient(hr, prof_r)))])
+    tools = []
+    for top in (True, False):
+        nodes, area, kappa = slave_faces(mesh, top)
+        pts = []
+        for t, frac, x_t in zip((0.0, 1.0), fracs, pos):
+            th = t * TOOL_TRAVEL / rc
+            x, y = rc * np.cos(th), rc * np.sin(th)
+            eps = 1.0e-7
+            hx = frac * (cone.height(np.array([x + eps]), np.array([y]))[0] -
+                         cone.height(np.array([x - eps]), np.array([y]))[0]) / (2 * eps)
+            hy = frac * (cone.height(np.array([x]), np.array([y + eps]))[0] -
+                         cone.height(np.array([x]), np.array([y - eps]))[0]) / (2 * eps)
+            nrm = np.array([-hx, -hy, 1.0]) / np.sqrt(1.0 + hx * hx + hy * hy)
+            mid = np.array([x, y, -0.5 * CONE_THICKNESS + frac * cone.height(np.array([x]), np.array([y]))[0]])
+            sign = 1.0 if top else -1.0
+            pts.append(tuple(place_ball(x_t[nodes], mid, sign * nrm, TOOL_RADIUS, penetration)))
+        tools.append(dict(shape="sphere", times=[0.0, 1.0], points=pts, nodes=nodes, area=area, kappa=kappa,
+                          radius=TOOL_RADIUS, friction=friction, tangential_ratio=1.0,
+                          name="forming" if top else "support"))
+    return sysm, ConeProblem(mesh=mesh, material=material, cone=cone, s=s, u0=u0, u=u1, tools=tools,
+                             contact_radius=rc)

@@ -25,6 +25,8 @@ backstresses and Voce hardening, a spherical tool on a 113-knot spiral
 path - the deck's parts in the JSON (the tool path read from its CSV), the
 mesh, the step-end displacements and element fields in the npz.
 
+parts.json: heights of the reference's part families at sample points.
+
 materials.json: the hardening parameters the reference's own Python
 (python/precomp/materials.py) derives - its built-in library (Hollomon
 fits) and the Swift law of the 40x40x2 forming sheet - plus the material
@@ -144,6 +146,45 @@ def challenge(ref_root: str, case: str = "kin_h0833") -> None:
                         eq_plastic_strain=np.array(eqps, dtype=np.float64), von_mises=np.array(vm, dtype=np.float64))
 
 
+def parts(ref_root: str) -> None:
+    """parts.json: heights of the reference's four part families
+    (python/precomp/geometry/parts.py) at seeded sample points, for a few
+    parameter sets each - the cone of the fine-mesh configuration (18 mm
+    footprint, 3 mm deep, 50 degree wall) among them."""
+    import numpy as np
+
+    sys.path.insert(0, os.path.join(ref_root, "python"))
+    from precomp.geometry import parts as P  # the reference's own module
+
+    cases = [
+        ("truncated_cone", dict(top_radius=0.0093, wall_angle_deg=50.0, depth=0.003, top_fillet=0.001,
+                                bottom_fillet=0.001)),
+        ("truncated_cone", dict(top_radius=0.05, wall_angle_deg=35.0, depth=0.02, top_fillet=0.005,
+                                bottom_fillet=0.004)),
+        ("elliptic_cone", dict(semi_axis_x=0.009, semi_axis_y=0.007, wall_angle_deg=45.0, depth=0.0025,
+                               top_fillet=0.001, bottom_fillet=0.001)),
+        ("elliptic_cone", dict(semi_axis_x=0.05, semi_axis_y=0.06, wall_angle_deg=55.0, depth=0.015,
+                               top_fillet=0.004, bottom_fillet=0.003)),
+        ("pyramid", dict(half_width_x=0.009, half_width_y=0.0075, wall_angle_deg=40.0, depth=0.0025,
+                         corner_radius=0.005, top_fillet=0.001, bottom_fillet=0.001)),
+        ("dome", dict(opening_radius=0.009, depth=0.003, rim_fillet=0.002, aspect=1.0)),
+        ("dome", dict(opening_radius=0.05, depth=0.02, rim_fillet=0.01, aspect=0.8)),
+    ]
+    rng = np.random.default_rng(1234)
+    out = []
+    for family, kw in cases:
+        part = P.families()[family](**kw)
+        r = 1.3 * part.footprint_radius()
+        xy = rng.uniform(-r, r, size=(400, 2))
+        xy[:8] = [[0, 0], [r / 2, 0], [0, r / 2], [r / 3, r / 4], [-r / 5, r / 7], [r, 0], [0, -r], [1e-6, 0]]
+        z = part.height(xy[:, 0], xy[:, 1])
+        out.append({"family": family, "params": kw, "footprint_radius": part.footprint_radius(),
+                    "xy": xy.tolist(), "z": [float(v) for v in z]})
+    with open(os.path.join(HERE, "parts.json"), "w") as f:
+        json.dump(out, f)
+        f.write("\n")
+
+
 if __name__ == "__main__":
     if len(sys.argv) != 2:
         sys.exit("usage: python tests/golden/make_golden.py <root of the reference's checkout>")
@@ -153,3 +194,4 @@ if __name__ == "__main__":
                  "plate_h2_std_mu0.1_drag3", "strip_h2_nobbar_mu0.1"):
         strip(root, case)
     challenge(root)
+    parts(root)
