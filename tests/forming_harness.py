@@ -10,7 +10,10 @@ What it restates of the driver, because the converged states depend on it:
 the step partition (prescribed DOFs held at their values, Forming.cpp:804-821),
 the start imbalance r0 ramped out over the step (:829-846, :890-897), the
 increment schedule (the tool travel per increment and the stations,
-:1149-1163) and the commit of every converged increment (:1208-1215). What
+:1149-1163), the cut of an increment whose Newton iteration fails - an
+element's SolverError from the GPU or no convergence - halved and retried,
+with the growth after a quick one (:1165-1247), and the commit of every
+converged increment (:1208-1215). What
 it does not restate, because it only changes the path to the same converged
 state: the predictor, the energy line search (a residual backtracking here),
 and the tolerances (the iteration here runs to a correction of 1e-13 m,
@@ -93,6 +96,20 @@ class StepResult:
     # (Forming.cpp:1266-1281).
     eq_plastic_strain: np.ndarray = None
     von_mises: np.ndarray = None
+    cuts: int = 0
+
+
+class NewtonFailure(RuntimeError):
+    """An increment's Newton iteration that did not converge."""
+
+
+# The increment control of the forming driver (Forming.cpp:37-39, 1149-1247):
+# a failed increment is halved, at most MAX_CUTS times in a row; an increment
+# that converged in at most QUICK_ITERATIONS lets the next grow by GROWTH, up
+# to the step's cap.
+MAX_CUTS = 10
+QUICK_ITERATIONS = 4
+GROWTH = 1.5
 
 
 class FormingRun:
@@ -150,6 +167,13 @@ class FormingRun:
         self.u = np.zeros(self.mesh.num_dofs)
         self.t = 0.0
         self.last_du = 0.0
+        # Host-side fault injection for tests: the numbers (1-based, counted
+        # over the run) of the increment attempts whose first evaluation
+        # raises the SolverError of an element's local iteration, as the GPU
+        # reports it.
+        self.inject_at = set()
+        self.attempts = 0
+        self.times = []
 
     # -- pieces of one Newton iteration -------------------------------------
     def _residual(self, u, t, active, tangent):
@@ -226,11 +250,13 @@ class FormingRun:
         if times is not None:
             for t1 in times:
                 s1 = 1.0 if t1 == te else (t1 - tb) / duration
-                fz_list.append(self._newton(t, t1, s1, free, r0, active))
+                fz_list.append(self._newton(t, t1, s1, free, r0, active)[0])
                 t = t1
             assert t == te, (t, te)
             self.t = te
             return self._step_end(StepResult(u=self.u.copy(), increments=len(times), tool_fz=fz_list))
+        cuts = cuts_in_a_row = 0
+        self.times = []
         while True:
             station = next(s for s in stations if s > t)
             h = min(dt, dt_max)
@@ -240,14 +266,28 @@ class FormingRun:
             reach = station - t <= h * (1.0 + 1.0e-6)
             t1 = station if reach else t + h
             s1 = 1.0 if (reach and station == te) else (t1 - tb) / duration
-            fz = self._newton(t, t1, s1, free, r0, active)
+            try:
+                fz, iterations = self._newton(t, t1, s1, free, r0, active)
+            except (self.pkg.SolverError, NewtonFailure) as err:
+                # The increment is cut: halved and retried from the last
+                # converged state (Forming.cpp:1173-1194).
+                cuts += 1
+                cuts_in_a_row += 1
+                if cuts_in_a_row > MAX_CUTS:
+                    raise NewtonFailure(f"an increment from t = {t} failed after {MAX_CUTS} halvings: {err}")
+                dt = 0.5 * (t1 - t)
+                continue
             fz_list.append(fz)
+            self.times.append(t1)
             count += 1
             t = t1
+            if iterations <= QUICK_ITERATIONS:
+                dt = min(GROWTH * dt, dt_max)
+            cuts_in_a_row = 0
             if s1 >= 1.0:
                 break
         self.t = te
-        return self._step_end(StepResult(u=self.u.copy(), increments=count, tool_fz=fz_list))
+        return self._step_end(StepResult(u=self.u.copy(), increments=count, tool_fz=fz_list, cuts=cuts))
 
     def _step_end(self, res: StepResult) -> StepResult:
         """The step-end stress recovery of every element at the converged
@@ -265,6 +305,12 @@ class FormingRun:
         a correction of 1e-13 m."""
         ramp = 1.0 - s1
         trial = self.u.copy()
+        self.attempts += 1
+        if self.attempts in self.inject_at:
+            # The GPU's report of an element whose local iteration did not
+            # converge (sbk_system_evaluate's SBK_ERR_SOLVER with the element
+            # and code 3), made on the host.
+            raise self.pkg.SolverError(4, "Hex8 element 0: SolverError (code 3), injected", 0, 3)
         any_tool = self.contact is not None and any(active)
         if self.contact is not None:
             self.contact.begin_increment(torch.tensor(self.u, device=self.dev), t0, t1, active,
@@ -341,7 +387,7 @@ class FormingRun:
             if (alpha == 1.0 and step <= 1e-13) or (it >= 40 and step <= 1e-11):
                 break
         else:
-            raise AssertionError(f"the increment to t = {t1} did not converge: (|R|, step, alpha) {history[-8:]}")
+            raise NewtonFailure(f"the increment to t = {t1} did not converge: (|R|, step, alpha) {history[-8:]}")
         # The accepted state's own evaluation makes its trial history the one committed.
         _, _, fz = self._residual(trial, t1, active, False)
         self.system.commit()
@@ -349,4 +395,4 @@ class FormingRun:
             self.contact.commit()
         self.last_du = float(np.abs((trial - self.u).reshape(-1, 3)).max())
         self.u = trial
-        return fz
+        return fz, it + 1
