@@ -353,8 +353,9 @@ __device__ __forceinline__ int point_kinematics(const Ctx<G, Rec>& c, int q, con
 
 // After the point's response r: its yield flag, the material block M and
 // stress S in the strain measure of the element (the logarithmic map, or
-// as they are), and its slot for the group sums.
-template <int G, class Rec>
+// as they are), and its slot for the group sums. MAPPED: r already holds
+// them in the element's strain measure (the logarithmic map was applied).
+template <int G, class Rec, bool MAPPED = false>
 __device__ __forceinline__ void point_slot(const Ctx<G, Rec>& c, int q, const Response& r, const LogKin& L,
                                            const double F[9], double w, double hmax, double M[36], double S[6]) {
   const Params& p = *c.p;
@@ -362,7 +363,7 @@ __device__ __forceinline__ void point_slot(const Ctx<G, Rec>& c, int q, const Re
   c.yield[c.e * p.nq + q] = r.yielding ? 1 : 0;
 #pragma unroll
   for (int i = 0; i < 36; ++i) M[i] = r.C[i];
-  if (p.kinematics == SBK_FINITE_LOGARITHMIC) {
+  if (!MAPPED && p.kinematics == SBK_FINITE_LOGARITHMIC) {
     log_transform(L, r.stress, S, M);
   } else {
 #pragma unroll
@@ -1772,9 +1773,43 @@ __global__ void __launch_bounds__(128, SBK_MINB_RETURN) wave_return_kernel(const
   }
 }
 
-// Pass, third kernel: per point the yield flag, the logarithmic map of the
-// response and the slot; per element the first failure, K_aa and the sums
-// (pass_sums) into the element's record.
+// Pass, third kernel (logarithmic kinematics): the logarithmic map of every
+// evaluated point's response (log_transform: S = P^T T, material = P^T C P
+// + T : L), a thread per point, in place in the point's record. On its own
+// its working set fits the registers of a thread; inside the sums kernel it
+// spilled.
+__global__ void __launch_bounds__(128, 2) wave_log_kernel(int64_t ne, int nq, const int32_t* __restrict__ list,
+                                                          const int32_t* __restrict__ count,
+                                                          const __grid_constant__ WaveBuffers w) {
+  const int64_t n = (count ? (int64_t)*count : ne) * 8;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int q = (int)(i & 7);
+    if (q >= nq) continue;
+    const int64_t e = list ? (int64_t)list[i >> 3] : (i >> 3);
+    if (w.pfail[e * 8 + q]) continue;
+    LogKin L;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) L.q[k] = *pw_at(w, e, kPwL + k, q);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) L.mu[k] = *pw_at(w, e, kPwL + 9 + k, q);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) L.first[k] = *pw_at(w, e, kPwL + 12 + k, q);
+    double t[6], S[6], M[36];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) t[k] = *pw_at(w, e, kPwStress + k, q);
+#pragma unroll
+    for (int k = 0; k < 36; ++k) M[k] = *pw_at(w, e, kPwC + k, q);
+    log_transform(L, t, S, M);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) *pw_at(w, e, kPwStress + k, q) = S[k];
+#pragma unroll
+    for (int k = 0; k < 36; ++k) *pw_at(w, e, kPwC + k, q) = M[k];
+  }
+}
+
+// Pass, fourth kernel: per point the yield flag and the slot; per element
+// the first failure, K_aa and the sums (pass_sums) into the element's
+// record.
 template <int G>
 __global__ void __launch_bounds__(128, SBK_MINB_POST) wave_post_kernel(const __grid_constant__ Params p, int64_t ne,
                                                         const int32_t* __restrict__ list,
@@ -1821,6 +1856,8 @@ __global__ void __launch_bounds__(128, SBK_MINB_POST) wave_post_kernel(const __g
 #pragma unroll
       for (int k = 0; k < 9; ++k) F[k] = *pw_at(w, e, kPwF + k, q);
       if (!fail) {
+        // The response in the element's strain measure (wave_log_kernel
+        // applied the logarithmic map).
         Response r;
         LogKin L;
 #pragma unroll
@@ -1829,14 +1866,8 @@ __global__ void __launch_bounds__(128, SBK_MINB_POST) wave_post_kernel(const __g
         for (int k = 0; k < 36; ++k) r.C[k] = *pw_at(w, e, kPwC + k, q);
         r.energy = *pw_at(w, e, kPwEnergy, q);
         r.yielding = *pw_at(w, e, kPwYield, q) != 0.0;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) L.q[k] = *pw_at(w, e, kPwL + k, q);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) L.mu[k] = *pw_at(w, e, kPwL + 9 + k, q);
-#pragma unroll
-        for (int k = 0; k < 6; ++k) L.first[k] = *pw_at(w, e, kPwL + 12 + k, q);
         const double hmax = *pw_at(w, e, kPwHmax, q);
-        point_slot(c, q, r, L, F, w_q, hmax, M, S);
+        point_slot<G, PassShared<G>, true>(c, q, r, L, F, w_q, hmax, M, S);
       }
     }
     // The sums read the point's M, S and F back from its slot in shared
@@ -3171,6 +3202,7 @@ int launch_elements_wave(const Params& p, int64_t ne, const double* coords, cons
   const unsigned pgrid = (unsigned)(pneed < cap ? pneed : cap);
   const int64_t rneed = (ne * 8 + 127) / 128;
   const unsigned rgrid = (unsigned)(rneed < 148 * 8 ? rneed : 148 * 8);
+  const unsigned lgrid = rgrid;
   cudaError_t err = cudaMemsetAsync(w.counts, 0, (2 * kWaveRounds + 3) * sizeof(int32_t), stream);
   if (err != cudaSuccess) return (int)err;
   for (int r = 0; r < kWaveRounds; ++r) {
@@ -3180,6 +3212,8 @@ int launch_elements_wave(const Params& p, int64_t ne, const double* coords, cons
     pre<<<pgrid, pepb * G, smem_pass, stream>>>(p, ne, r == 0, list, count, batch, coords, conn, u, state, alpha_n,
                                                 trial, yield, w.plastic, plastic_count, w);
     wave_return_kernel<<<rgrid, 128, 0, stream>>>(p, ne, w.plastic, plastic_count, state, trial, w);
+    if (p.kinematics == SBK_FINITE_LOGARITHMIC)
+      wave_log_kernel<<<lgrid, 128, 0, stream>>>(ne, p.nq, list, count, w);
     wave_post_kernel<G><<<grid, threads, smem_post, stream>>>(p, ne, list, count, yield, w);
     wave_control_kernel<G><<<grid, threads, smem_ctl, stream>>>(p, ne, r == 0, list, count, w, w.list[(r + 1) & 1],
                                                                 w.counts + r + 1, code, first_failure);
