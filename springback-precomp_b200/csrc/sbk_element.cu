@@ -1501,7 +1501,8 @@ struct __align__(16) PreShared {
 // to fit, which bounds the registers of a thread: 2 allows 255, 3 170, 4
 // 128. Measured on the 1M-element microbenchmark: the return kernel gains
 // 11 % at 4 (more warps hide its latency, its spills stay small); the other
-// three lose 15-65 % at 3 or 4 (their spills grow).
+// kernels lose 15-65 % at 3 or 4 (their spills grow), the logarithmic map
+// 33 % at 3.
 #ifndef SBK_MINB_PRE
 #define SBK_MINB_PRE 2
 #endif
@@ -1510,6 +1511,9 @@ struct __align__(16) PreShared {
 #endif
 #ifndef SBK_MINB_POST
 #define SBK_MINB_POST 2
+#endif
+#ifndef SBK_MINB_LOG
+#define SBK_MINB_LOG 2
 #endif
 #ifndef SBK_MINB_CONDENSE
 #define SBK_MINB_CONDENSE 2
@@ -1778,7 +1782,7 @@ __global__ void __launch_bounds__(128, SBK_MINB_RETURN) wave_return_kernel(const
 // + T : L), a thread per point, in place in the point's record. On its own
 // its working set fits the registers of a thread; inside the sums kernel it
 // spilled.
-__global__ void __launch_bounds__(128, 2) wave_log_kernel(int64_t ne, int nq, const int32_t* __restrict__ list,
+__global__ void __launch_bounds__(128, SBK_MINB_LOG) wave_log_kernel(int64_t ne, int nq, const int32_t* __restrict__ list,
                                                           const int32_t* __restrict__ count,
                                                           const __grid_constant__ WaveBuffers w) {
   const int64_t n = (count ? (int64_t)*count : ne) * 8;
