@@ -159,6 +159,15 @@ int sbk_system_set_element(sbk_system* sys, int element, int mean_dilatation);
 /* The formulation in use and whether it averages the dilatation. */
 int sbk_system_element(const sbk_system* sys, int* element, int* averaged);
 
+/* Where the evaluations with the tangent assemble its CSC values (nnz
+ * doubles, device, the caller's; NULL: the system's own buffer). No
+ * counterpart in the reference, whose Evaluation owns its matrix. A driver
+ * that alternates two buffers can read one back to the host, or hand it to
+ * its solver, while the next evaluation assembles into the other. The
+ * buffer must stay valid while evaluations use it; node blocks and
+ * stiffness_gross act on the current one. */
+int sbk_system_set_values_buffer(sbk_system* sys, double* values_dev);
+
 /* Launch shape of the element kernel: elements per thread block (0: the
  * default, 16 for rules of up to 8 points - four warps - and 8 for larger
  * rules - eight warps; at most what 227 KB of shared memory and 256 threads

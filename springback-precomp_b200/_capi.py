@@ -107,6 +107,7 @@ SIGNATURES = {
     "sbk_system_set_stream": (_I, [_P, _P]),
     "sbk_system_set_elements_per_block": (_I, [_P, _I]),
     "sbk_set_local_iteration": (_I, [_I]),
+    "sbk_system_set_values_buffer": (_I, [_P, _P]),
     "sbk_system_set_local_iteration": (_I, [_P, _I]),
     "sbk_system_set_element": (_I, [_P, _I, _I]),
     "sbk_system_element": (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(_I)]),

@@ -384,7 +384,8 @@ struct sbk_system {
   // assembly
   int32_t* outer = nullptr;
   int32_t* inner = nullptr;
-  double* values = nullptr;
+  double* values = nullptr;       // where the assembly writes the tangent values
+  double* own_values = nullptr;   // the system's own buffer (values unless the caller set one)
   double* internal = nullptr;
   double* scratch = nullptr;
   double* scalars = nullptr;
@@ -433,7 +434,7 @@ namespace {
 void free_system(sbk_system* s) {
   void* ptrs[] = {s->coords, s->conn, s->committed, s->trial, s->alpha_c, s->alpha_t, s->force,
                   s->tangent, s->energy_e, s->yield, s->iters, s->code, s->first_fail, s->outer,
-                  s->inner, s->values, s->internal, s->scratch, s->scalars, s->missing, s->block_col,
+                  s->inner, s->own_values, s->internal, s->scratch, s->scalars, s->missing, s->block_col,
                   s->block_value, s->block_ptr, s->block_src, s->node_ptr, s->node_src, s->product,
                   s->order, s->sched, s->wave_mem};
   for (void* p : ptrs)
@@ -617,7 +618,8 @@ int sbk_system_create(const sbk_mesh* mesh, const sbk_material* material, const 
   TRY(dalloc(&s->iters, static_cast<size_t>(s->ne)));
   TRY(dalloc(&s->code, static_cast<size_t>(s->ne)));
   TRY(dalloc(&s->first_fail, 1));
-  TRY(dalloc(&s->values, static_cast<size_t>(s->nnz)));
+  TRY(dalloc(&s->own_values, static_cast<size_t>(s->nnz)));
+  s->values = s->own_values;
   TRY(dalloc(&s->internal, static_cast<size_t>(s->nn) * 3));
   TRY(dalloc(&s->product, static_cast<size_t>(s->nn) * 3));
   TRY(dalloc(&s->order, static_cast<size_t>(s->ne)));
@@ -719,6 +721,13 @@ int sbk_system_set_local_iteration(sbk_system* sys, int mode) {
   if (mode != SBK_LOCAL_PHASES && mode != SBK_LOCAL_SINGLE_KERNEL) return fail(SBK_ERR_ARGUMENT, "unknown mode");
   sys->local_mode = mode;
   return mode == SBK_LOCAL_PHASES ? ensure_wave(sys) : SBK_OK;
+}
+
+int sbk_system_set_values_buffer(sbk_system* sys, double* values_dev) {
+  if (!sys) return fail(SBK_ERR_ARGUMENT, "null system");
+  sys->values = values_dev ? values_dev : sys->own_values;
+  sys->has_values = false;
+  return SBK_OK;
 }
 
 int sbk_system_set_elements_per_block(sbk_system* sys, int epb) {

@@ -309,6 +309,17 @@ class NonlinearSystem:
         depends on it."""
         _capi.check(_capi.lib().sbk_system_set_local_iteration(self._h, LOCAL_ITERATION[mode]))
 
+    def set_values_buffer(self, values: Optional[torch.Tensor] = None):
+        """Assemble the tangent of the next evaluations into `values` (nnz
+        float64 on the device, kept alive by the system meanwhile), or back
+        into the system's own buffer (None): a driver alternating two
+        buffers reads one back while the next evaluation fills the other."""
+        if values is not None and (values.dtype != torch.float64 or values.numel() != self.nnz or not values.is_cuda
+                                   or not values.is_contiguous()):
+            raise ValueError("values must be a contiguous CUDA float64 tensor of nnz entries")
+        self._values_buffer = values
+        _capi.check(_capi.lib().sbk_system_set_values_buffer(self._h, _ptr(values) if values is not None else None))
+
     def set_elements_per_block(self, epb: int):
         _capi.check(_capi.lib().sbk_system_set_elements_per_block(self._h, int(epb)))
 

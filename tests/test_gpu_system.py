@@ -261,3 +261,32 @@ def test_system_phase_kernels_match_the_single_kernel(pkg, cuda):
         assert abs(ena - enb) <= tol * abs(enb) and ya == yb
     assert np.abs(sa - sb).max() <= tol * np.abs(sb).max()
     assert np.abs(ma - mb).max() <= tol * np.abs(mb).max()
+
+
+def test_values_buffer_of_the_caller(pkg, cuda):
+    """sbk_system_set_values_buffer: evaluations with the tangent assemble
+    into the caller's buffer - alternating two, as a driver that reads one
+    back while the next evaluation fills the other - with the values of the
+    system's own buffer; node blocks go into the current buffer; None
+    returns to the own buffer."""
+    wl = importlib.import_module("springback-precomp_b200.workload")
+    prob = wl.make_problem(12, 8, 2, seed=4, sample=192)
+    sysm = pkg.NonlinearSystem(prob.mesh, prob.material, kinematics="logarithmic")
+    sysm.set_committed(prob.state)
+    sysm.set_internal(prob.alpha)
+    u = torch.tensor(prob.u, device=cuda)
+    own = sysm.evaluate(u, 0.0, True).tangent.clone()
+    bufs = [torch.full((sysm.nnz,), float("nan"), dtype=torch.float64, device=cuda) for _ in range(2)]
+    for k in range(4):
+        sysm.set_values_buffer(bufs[k % 2])
+        ev = sysm.evaluate(u, 0.0, True)
+        assert ev.tangent.data_ptr() == bufs[k % 2].data_ptr()
+        assert torch.equal(bufs[k % 2], own)
+    nodes = torch.tensor([0, 3], dtype=torch.int32, device=cuda)
+    blocks = torch.ones((2, 3, 3), dtype=torch.float64, device=cuda)
+    sysm.add_node_blocks(nodes, blocks)  # into bufs[1], the current one
+    assert not torch.equal(bufs[1], own) and torch.equal(bufs[0], own)
+    sysm.set_values_buffer(None)
+    ev = sysm.evaluate(u, 0.0, True)
+    assert ev.tangent.data_ptr() not in (bufs[0].data_ptr(), bufs[1].data_ptr())
+    assert torch.equal(ev.tangent, own)
