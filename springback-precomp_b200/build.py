@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libsbk.so")
 SOURCES = ["sbk_element.cu", "sbk_assembly.cu", "sbk_contact.cu", "sbk_capi.cu", "sbk_schedule.cu", "sbk_noalloc.cu",
-           "sbk_pattern.cu",
+           "sbk_pattern.cu", "sbk_return.cu",
            "sbk_partition.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -496,15 +496,36 @@ __global__ void resultant_kernel(const int32_t* __restrict__ list, const int32_t
   }
 }
 
-__global__ void norms_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
-                             const double* __restrict__ c, double* __restrict__ out) {
+// The Euclidean norms of three n-vectors in two fixed-shape stages (the
+// same sums in the same order every call): kNormBlocks blocks of partial
+// sums of squares, then one block over the partials.
+constexpr int kNormBlocks = 296;
+
+__global__ void norms_partial_kernel(int64_t n, const double* __restrict__ a, const double* __restrict__ b,
+                                     const double* __restrict__ c, double* __restrict__ partial) {
   __shared__ double sh[256][3];
   double s[3] = {0, 0, 0};
-  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     s[0] += a[i] * a[i];
     s[1] += b[i] * b[i];
     s[2] += c[i] * c[i];
   }
+  for (int k = 0; k < 3; ++k) sh[threadIdx.x][k] = s[k];
+  __syncthreads();
+  for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+    if (threadIdx.x < st)
+      for (int k = 0; k < 3; ++k) sh[threadIdx.x][k] += sh[threadIdx.x + st][k];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) partial[3 * blockIdx.x + k] = sh[0][k];
+}
+
+__global__ void norms_kernel(int nb, const double* __restrict__ partial, double* __restrict__ out) {
+  __shared__ double sh[256][3];
+  double s[3] = {0, 0, 0};
+  for (int i = threadIdx.x; i < nb; i += blockDim.x)
+    for (int k = 0; k < 3; ++k) s[k] += partial[3 * i + k];
   for (int k = 0; k < 3; ++k) sh[threadIdx.x][k] = s[k];
   __syncthreads();
   for (int st = blockDim.x / 2; st > 0; st >>= 1) {
@@ -654,6 +675,7 @@ struct sbk_contact {
   int num_blocks = 0;
   int32_t* flags = nullptr;  // [0] failed, [1] asym
   double* norms = nullptr;
+  double* norm_partial = nullptr;  // 3 per block of the norms' first stage
   double* res_dev = nullptr;  // 6 per tool
   std::vector<double> resultants;
   int search = SBK_SEARCH_GRID;
@@ -677,7 +699,7 @@ void free_contact(sbk_contact* c) {
       if (p) cudaFree(p);
   }
   void* ptrs[] = {c->coords, c->start, c->residual, c->gross, c->positions, c->block_nodes, c->blocks, c->flags,
-                  c->norms, c->res_dev};
+                  c->norms, c->norm_partial, c->res_dev};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   delete c;
@@ -720,6 +742,7 @@ int sbk_contact_create(const sbk_mesh* mesh, int32_t num_tools, const sbk_tool* 
   TRYC(calloc_dev(&c->positions, 3 * c->nn));
   TRYC(calloc_dev(&c->flags, 4));
   TRYC(calloc_dev(&c->norms, 4));
+  TRYC(calloc_dev(&c->norm_partial, 3 * kNormBlocks));
   int total = 0;
   for (int k = 0; k < num_tools; ++k) {
     const sbk_tool& s = tools[k];
@@ -972,7 +995,9 @@ int sbk_contact_evaluate(sbk_contact* c, const double* u_dev, double t, int want
     resultant_kernel<<<1, 256, 0, st>>>(h.alist, h.nalist, h.ev(), c->res_dev + 6 * k);
     if (want_tangent) base += counts[k];
   }
-  norms_kernel<<<1, 256, 0, st>>>(static_cast<int64_t>(nd), c->gross, c->positions, c->residual, c->norms);
+  norms_partial_kernel<<<kNormBlocks, 256, 0, st>>>(static_cast<int64_t>(nd), c->gross, c->positions, c->residual,
+                                                   c->norm_partial);
+  norms_kernel<<<1, 256, 0, st>>>(kNormBlocks, c->norm_partial, c->norms);
   SBK_C(cudaGetLastError());
   double norms[3];
   int32_t flags[2];

@@ -24,6 +24,7 @@
 
 #include "sbk_element.h"
 #include "sbk_material.cuh"
+#include "sbk_wave.h"
 
 namespace sbk {
 namespace {
@@ -1499,15 +1500,11 @@ struct __align__(16) PreShared {
 
 // Minimum resident blocks per SM (128 threads each) the compiler is told
 // to fit, which bounds the registers of a thread: 2 allows 255, 3 170, 4
-// 128. Measured on the 1M-element microbenchmark: the return kernel gains
-// 11 % at 4 (more warps hide its latency, its spills stay small); the other
-// kernels lose 15-65 % at 3 or 4 (their spills grow), the logarithmic map
-// 33 % at 3.
+// 128. Measured on the 1M-element microbenchmark: these kernels lose 15-65 %
+// at 3 or 4 (their spills grow), the logarithmic map 33 % at 3; the return
+// kernel (sbk_return.cu) is best at 4.
 #ifndef SBK_MINB_PRE
 #define SBK_MINB_PRE 2
-#endif
-#ifndef SBK_MINB_RETURN
-#define SBK_MINB_RETURN 4
 #endif
 #ifndef SBK_MINB_POST
 #define SBK_MINB_POST 2
@@ -1569,31 +1566,6 @@ __device__ __forceinline__ double abs_max9(const double* v) {
 __device__ __forceinline__ void append(int32_t* list, int32_t* count, int64_t e) {
   const int pos = atomicAdd(count, 1);
   list[pos] = (int32_t)e;
-}
-
-// Fields of a point's record between the three pass kernels (field f of
-// point q of element e at (e * kPw + f) * 8 + q).
-constexpr int kPwF = 0;        // F 9
-constexpr int kPwHmax = 9;     // the largest |H| entry
-constexpr int kPwL = 10;       // LogKin: axes 9, mu 3, first 6
-constexpr int kPwStrain = 28;  // the strain the return takes, 6
-constexpr int kPwStress = 34;  // the response: stress 6
-constexpr int kPwC = 40;       // C 36
-constexpr int kPwEnergy = 76;
-constexpr int kPwYield = 77;
-constexpr int kPw = 78;
-
-__device__ __forceinline__ double* pw_at(const WaveBuffers& w, int64_t e, int f, int q) {
-  return w.pw + (e * kPw + f) * 8 + q;
-}
-
-__device__ __forceinline__ void store_response(const WaveBuffers& w, int64_t e, int q, const Response& r) {
-#pragma unroll
-  for (int i = 0; i < 6; ++i) *pw_at(w, e, kPwStress + i, q) = r.stress[i];
-#pragma unroll
-  for (int i = 0; i < 36; ++i) *pw_at(w, e, kPwC + i, q) = r.C[i];
-  *pw_at(w, e, kPwEnergy, q) = r.energy;
-  *pw_at(w, e, kPwYield, q) = r.yielding ? 1.0 : 0.0;
 }
 
 // Pass, first kernel: per point the kinematics at the trial modes and the
@@ -1748,34 +1720,8 @@ __global__ void __launch_bounds__(128, SBK_MINB_PRE) wave_pre_kernel(const __gri
   }
 }
 
-// Pass, second kernel: the general return of every listed point, a thread
-// each, so that a warp's 32 lanes all run the closest-point iteration.
-__global__ void __launch_bounds__(128, SBK_MINB_RETURN) wave_return_kernel(const __grid_constant__ Params p, int64_t ne,
-                                                          const int32_t* __restrict__ plastic,
-                                                          const int32_t* __restrict__ plastic_count,
-                                                          const double* __restrict__ state,
-                                                          double* __restrict__ trial,
-                                                          const __grid_constant__ WaveBuffers w) {
-  const int64_t n = *plastic_count;
-  const int nq = p.nq;
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t pt = plastic[i];
-    const int64_t e = pt >> 3;
-    const int q = (int)(pt & 7);
-    double strain[6];
-#pragma unroll
-    for (int k = 0; k < 6; ++k) strain[k] = *pw_at(w, e, kPwStrain + k, q);
-    PointState st{state + e * nq + q, trial + e * nq + q, ne * nq};
-    Response r;
-    const int code = general_return(p, strain, st, r, w.warm + pt * 8);
-    if (code) {
-      w.pfail[pt] = (2 << 8) | q;
-      w.pcodes[pt] = code;
-    } else {
-      store_response(w, e, q, r);
-    }
-  }
-}
+// Pass, second kernel: the general return of every listed point, in
+// sbk_return.cu (launch_wave_returns).
 
 // Pass, third kernel (logarithmic kinematics): the logarithmic map of every
 // evaluated point's response (log_transform: S = P^T T, material = P^T C P
@@ -3215,7 +3161,7 @@ int launch_elements_wave(const Params& p, int64_t ne, const double* coords, cons
     int32_t* plastic_count = w.counts + kWaveRounds + 3 + r;
     pre<<<pgrid, pepb * G, smem_pass, stream>>>(p, ne, r == 0, list, count, batch, coords, conn, u, state, alpha_n,
                                                 trial, yield, w.plastic, plastic_count, w);
-    wave_return_kernel<<<rgrid, 128, 0, stream>>>(p, ne, w.plastic, plastic_count, state, trial, w);
+    launch_wave_returns(p, ne, w.plastic, plastic_count, state, trial, w, rgrid, stream);
     if (p.kinematics == SBK_FINITE_LOGARITHMIC)
       wave_log_kernel<<<lgrid, 128, 0, stream>>>(ne, p.nq, list, count, w);
     wave_post_kernel<G><<<grid, threads, smem_post, stream>>>(p, ne, list, count, yield, w);

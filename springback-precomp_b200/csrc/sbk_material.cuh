@@ -19,6 +19,14 @@ namespace sbk {
 
 constexpr double kEps = 2.220446049250313e-16;
 
+// How the closest-point return's helpers (the residual evaluation, the
+// consistent tangent, the backstress decay) are compiled: as calls (one
+// copy of their code for every caller) unless a translation unit asks for
+// them inlined.
+#ifndef SBK_RETURN_HELPER
+#define SBK_RETURN_HELPER __noinline__
+#endif
+
 // Point-failure codes (sbk_element_code).
 constexpr int kFailInverted = SBK_EL_INVERTED_POINT;
 constexpr int kFailReturn = SBK_EL_RETURN_NO_CONVERGE;
@@ -211,7 +219,7 @@ __device__ __forceinline__ int radial_return(const Params& p, const double strai
 struct Decay {
   double theta, chi, dtheta, dchi;
 };
-__device__ __noinline__ Decay decay_of(double gamma, double dl, int integration) {
+static __device__ SBK_RETURN_HELPER Decay decay_of(double gamma, double dl, int integration) {
   Decay d{1.0, 0.0, 0.0, 1.0};
   if (gamma == 0.0) {
     d.chi = dl;
@@ -245,7 +253,7 @@ struct Terms {
   double a[SBK_MAX_BACKSTRESSES][6];
 };
 
-__device__ __noinline__ bool gr_evaluate(const Params& p, const double s_trial[6], const Terms& tn,
+static __device__ SBK_RETURN_HELPER bool gr_evaluate(const Params& p, const double s_trial[6], const Terms& tn,
                                             double a_n, const double xi[6], double dl, GPoint& e) {
   double pxi[6];
 #pragma unroll
@@ -382,7 +390,7 @@ __device__ __forceinline__ void j_solve(const Params& p, const GPoint& e, const 
 
 // C_alg = C^e - 2G [m_t a^T + (dl / sigma_bar) S (P - m m^T) A] with
 // [A; a^T] = J^-1 [D_dev; 0] (Plasticity.cpp:299-311).
-__device__ __noinline__ void gr_tangent(const Params& p, const GPoint& e, double a_n, double dl, double C[36]) {
+static __device__ SBK_RETURN_HELPER void gr_tangent(const Params& p, const GPoint& e, double a_n, double dl, double C[36]) {
   JFactor jf;
   j_factor(p, e, a_n, dl, jf);
   const double g = p.G;
@@ -728,7 +736,7 @@ __device__ __forceinline__ void jacobi_rotate(double a[9], double v[9], int p, i
   }
 }
 
-__device__ __noinline__ double log_div(double mx, double my) {
+static __device__ __noinline__ double log_div(double mx, double my) {
   if (mx > my) {
     const double t = mx;
     mx = my;
@@ -747,7 +755,7 @@ __device__ __forceinline__ double first_of(const double f[6], int a, int b) {
   return (lo == 0 && hi == 1) ? f[3] : ((lo == 1 && hi == 2) ? f[4] : f[5]);
 }
 
-__device__ __noinline__ double log_div2(const LogKin& L, int a, int b, int c) {
+static __device__ __noinline__ double log_div2(const LogKin& L, int a, int b, int c) {
   int i = a, j = b, k = c;
   if (L.mu[i] < L.mu[j]) { const int t = i; i = j; j = t; }
   if (L.mu[j] < L.mu[k]) { const int t = j; j = k; k = t; }
@@ -853,7 +861,7 @@ __device__ __forceinline__ double rot_m(const double q[9], int r, int c) {
 // S = P^T T alone (LogarithmicStrain.cpp:144-149): the second
 // Piola-Kirchhoff stress of the Kirchhoff-like stress T work-conjugate to
 // E_log, for stress recovery.
-__device__ __noinline__ void log_stress(const LogKin& L, const double t[6], double s_out[6]) {
+static __device__ __noinline__ void log_stress(const LogKin& L, const double t[6], double s_out[6]) {
   const int kr[6] = {0, 1, 2, 0, 1, 2};
   const int kc[6] = {0, 1, 2, 1, 2, 0};
   double tpv[6];
