@@ -613,8 +613,8 @@ __device__ __noinline__ int pass(const Ctx<G, Rec>& c, const double at[9]) {
 // multiplied by its reciprocal, then the rank-one update. rowp / colp hold
 // the transpositions.
 template <int G, class CT>
-__device__ __noinline__ bool fullpiv_lu9_rows(const CT& c, const double* a, double* lu, int* rowp, int* colp,
-                                              double* maxpivot_out) {
+__device__ __forceinline__ bool fullpiv_lu9_rows_inline(const CT& c, const double* a, double* lu, int* rowp,
+                                                        int* colp, double* maxpivot_out) {
   const int lane = c.lane;
   _Pragma("unroll 1") for (int i = lane; i < 81; i += G) lu[i] = a[i];
   c.sync();
@@ -688,9 +688,15 @@ __device__ __noinline__ bool fullpiv_lu9_rows(const CT& c, const double* a, doub
   return ok;
 }
 
+template <int G, class CT>
+__device__ __noinline__ bool fullpiv_lu9_rows(const CT& c, const double* a, double* lu, int* rowp, int* colp,
+                                              double* maxpivot_out) {
+  return fullpiv_lu9_rows_inline<G>(c, a, lu, rowp, colp, maxpivot_out);
+}
+
 // x = A^-1 b with the FullPivLU factors (any lane; b and x may alias).
-__device__ __noinline__ void fullpiv_solve9(const double* lu, const int* rowp, const int* colp, const double* b,
-                                               double* x) {
+__device__ __forceinline__ void fullpiv_solve9_inline(const double* lu, const int* rowp, const int* colp,
+                                                      const double* b, double* x) {
   double y[9];
 #pragma unroll
   for (int i = 0; i < 9; ++i) y[i] = b[i];
@@ -730,6 +736,11 @@ __device__ __noinline__ void fullpiv_solve9(const double* lu, const int* rowp, c
   }
 #pragma unroll
   for (int i = 0; i < 9; ++i) x[i] = y[i];
+}
+
+__device__ __noinline__ void fullpiv_solve9(const double* lu, const int* rowp, const int* colp, const double* b,
+                                            double* x) {
+  fullpiv_solve9_inline(lu, rowp, colp, b, x);
 }
 
 // x = A^-T b with the FullPivLU factors of A (P A Q = L U, so
@@ -798,7 +809,7 @@ __device__ __noinline__ bool llt9(double* a) {
 // the same dot product in the same order - the same factor and the same
 // answer.
 template <int G, class CT>
-__device__ __noinline__ bool llt9_rows(const CT& c, double* a) {
+__device__ __forceinline__ bool llt9_rows_inline(const CT& c, double* a) {
   const int lane = c.lane;
   _Pragma("unroll 1") for (int k = 0; k < 9; ++k) {
     int bad = 0;
@@ -822,6 +833,11 @@ __device__ __noinline__ bool llt9_rows(const CT& c, double* a) {
     c.sync();
   }
   return true;
+}
+
+template <int G, class CT>
+__device__ __noinline__ bool llt9_rows(const CT& c, double* a) {
+  return llt9_rows_inline<G>(c, a);
 }
 
 __device__ __noinline__ void llt9_solve(const double* l, const double* b, double* x) {
@@ -1174,7 +1190,9 @@ struct Local {
 // the tangent, K* = K_uu - K_ua C, symmetrised for a symmetric tangent. Reads
 // the group's shared record: the last pass's slots and sums (slot, r), the
 // factors of its K_aa (lu, rowp, colp) and the geometry; kc is overwritten.
-template <int G, class Rec>
+// INLINE_SOLVE: the 9 x 9 solves compiled in place (their vectors stay in
+// registers) rather than called.
+template <int G, class Rec, bool INLINE_SOLVE = false>
 __device__ __forceinline__ void condense(const Ctx<G, Rec>& c, int want_tangent, double* __restrict__ force,
                                          double* __restrict__ tangent) {
   const Params& p = *c.p;
@@ -1226,7 +1244,8 @@ __device__ __forceinline__ void condense(const Ctx<G, Rec>& c, int want_tangent,
 #pragma unroll
       for (int j = 0; j < 9; ++j) b[j] = sym ? kua[k][j] : kau[k][j];
       double x[9];
-      fullpiv_solve9(s.lu, s.rowp, s.colp, b, x);
+      if (INLINE_SOLVE) fullpiv_solve9_inline(s.lu, s.rowp, s.colp, b, x);
+      else fullpiv_solve9(s.lu, s.rowp, s.colp, b, x);
 #pragma unroll
       for (int j = 0; j < 9; ++j) C[(3 * a + k) * 9 + j] = x[j];
     }
@@ -1236,7 +1255,8 @@ __device__ __forceinline__ void condense(const Ctx<G, Rec>& c, int want_tangent,
     const int a = lane;
     // f* = f_u - K_ua K_aa^-1 r_alpha.
     double corr[9];
-    fullpiv_solve9(s.lu, s.rowp, s.colp, s.r + 24, corr);
+    if (INLINE_SOLVE) fullpiv_solve9_inline(s.lu, s.rowp, s.colp, s.r + 24, corr);
+    else fullpiv_solve9(s.lu, s.rowp, s.colp, s.r + 24, corr);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       double v = 0.0;
@@ -1916,7 +1936,7 @@ __global__ void __launch_bounds__(128) wave_control_kernel(const __grid_constant
     const double largest = modes_inf(s.r);
     const double scale = abs_max9(s.scale);
     const double floor_ = kLocalRoundOff * abs_max9(s.flo);
-    const bool invertible = fullpiv_lu9_rows<G>(c, s.kc, s.lu, s.rowp, s.colp, &s.maxpivot);
+    const bool invertible = fullpiv_lu9_rows_inline<G>(c, s.kc, s.lu, s.rowp, s.colp, &s.maxpivot);
     for (int k = lane; k < 81; k += G) s.work[k] = s.kc[k];
     for (int k = lane; k < 9; k += G) s.r0[k] = s.r[24 + k];
     c.sync();
@@ -1952,10 +1972,10 @@ __global__ void __launch_bounds__(128) wave_control_kernel(const __grid_constant
     c.sync();
     if (lane == 0) {
       double nw[9];
-      fullpiv_solve9(s.lu, s.rowp, s.colp, s.r0, nw);
+      fullpiv_solve9_inline(s.lu, s.rowp, s.colp, s.r0, nw);
       for (int k = 0; k < 9; ++k) s.dir[k] = -nw[k];
     }
-    const bool positive = llt9_rows<G>(c, s.work + 162);
+    const bool positive = llt9_rows_inline<G>(c, s.work + 162);
     c.sync();
     if (!positive) {
       if (lane == 0) append(fallback_list, fallback_count, e);
@@ -2010,7 +2030,7 @@ __global__ void __launch_bounds__(128, SBK_MINB_CONDENSE) wave_condense_kernel(c
     for (int k = lane; k < 9; k += G) s.r[24 + k] = w.r[e * 33 + 24 + k];
     c.sync();
     force_sums(c);  // f_u and the energy of the last pass
-    condense<G>(c, want_tangent, force, tangent);
+    condense<G, CondenseShared<G>, true>(c, want_tangent, force, tangent);
     if (lane == 0) {
       energy[e] = s.energy;
       iterations[e] = w.iters[e];
