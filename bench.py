@@ -278,80 +278,85 @@ def cpu_baseline_subprocess(args):
 
 
 def run_batched(args, rank, world):
-    """The batched design sweep (the 64 uneven parts of the sweep
-    configuration: 20k-150k elements each, material of the microbenchmark):
-    one evaluation of all parts as one system, plain and as a replayed CUDA
-    graph, against the same parts evaluated one system at a time (each
-    evaluate followed by its host read, as a per-part driver does). Parts are
-    seeded sheets of 2 layers with aspect ratios 1.0-1.6 under a bending
-    field; their points start virgin."""
+    """The batched design sweep: the parts of the sweep configuration - a
+    scrambled Sobol sequence over four families (dome, truncated cone,
+    elliptic cone of axis ratio 1.0-1.6, pyramid), footprint 15-20 mm, depth
+    2-4 mm, wall 30-55 degrees, 20k-150k Hex8 each in two layers - with the
+    microbenchmark's material. One sweep = `sweep_increments` forming
+    increments of every part towards its shape (to 15 % of its depth, the
+    sheet laid on the scaled surface): each increment two Newton iterations'
+    evaluations with the tangent, then the commit - the element loop's work
+    of the parts' forming runs; the solves are the reference's own and stay
+    out. Timed one part at a time (each part's system made, its increments
+    timed on the device, released), against all parts as one batched system
+    whose thread mapping the autotuner picks first. Reported: parts per hour
+    of both."""
     import torch
 
     if world > 1 and rank != 0:
         return 0
     pkg = importlib.import_module(PKG)
     batch_mod = importlib.import_module(PKG + ".batch")
+    wl = importlib.import_module(PKG + ".workload")
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    rng = np.random.default_rng(20260)
     mat = pkg.material.hill_chaboche_sheet()
-    meshes, us = [], []
-    for _ in range(args.parts):
-        ne = int(rng.uniform(20000, 150000))
-        aspect = rng.uniform(1.0, 1.6)
-        ny = max(1, int(round(np.sqrt(ne / 2 / aspect))))
-        nx = max(1, int(round(ne / 2 / ny)))
-        m = pkg.structured_hex_mesh(nx, ny, 2, nx * 4e-5, ny * 4e-5, 1e-3)
-        x = m.coords
-        u = np.zeros_like(x)
-        span = x[:, 0].max() - x[:, 0].min()
-        u[:, 2] = -0.02 * (x[:, 0] - x[:, 0].mean()) ** 2 / span
-        u[:, 0] = 0.002 * (x[:, 2] - x[:, 2].mean()) * (x[:, 0] - x[:, 0].mean()) / span
-        meshes.append(m)
-        us.append(u.reshape(-1))
+    parts = wl.sweep_parts(args.parts)
+    meshes = [m for _, m in parts]
+    K, depth = args.sweep_increments, 0.15
     total = sum(m.num_elements for m in meshes)
+    stream = torch.cuda.current_stream()
 
-    def timed(fn, reps):
-        fn()
+    # The increments' displacements, once for both runs (host memory).
+    disps = [[(wl.formed_positions(m, part, (k + 1) * depth / K) - m.coords).reshape(-1) for k in range(K)]
+             for part, m in parts]
+
+    def run_increments(system, us):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        yielding = 0
+        for k in range(K):
+            for _ in range(2):
+                ev = system.evaluate(us[k], 0.0, True)
+            yielding = ev.yielding_points
+            system.commit()
+        e1.record(stream)
         torch.cuda.synchronize()
-        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s0.record()
-        for _ in range(reps):
-            fn()
-        s1.record()
-        torch.cuda.synchronize()
-        return s0.elapsed_time(s1) / reps
+        return e0.elapsed_time(e1), yielding
 
     # One part at a time.
-    systems = [pkg.NonlinearSystem(m, mat) for m in meshes]
-    u_dev = [torch.tensor(u, device=dev) for u in us]
-
-    def sequential():
-        for sy, u in zip(systems, u_dev):
-            sy.evaluate(u, 0.0, True)
-
-    seq_ms = timed(sequential, max(1, args.steps // 4))
-    yielding = sum(sy.evaluate(u, 0.0, True).yielding_points for sy, u in zip(systems, u_dev))
-    del systems
+    seq_ms, per_part = 0.0, []
+    for (part, mesh), dp in zip(parts, disps):
+        sy = pkg.NonlinearSystem(mesh, mat)
+        us = [torch.tensor(d, device=dev) for d in dp]
+        ms, _ = run_increments(sy, us)
+        seq_ms += ms
+        per_part.append(ms)
+        sy.close()
+        del us
     torch.cuda.empty_cache()
+    # All parts as one system.
+    t0 = time.perf_counter()
     batch = batch_mod.PartBatch(meshes, mat)
-    ub = torch.tensor(np.concatenate(us), device=dev)
-    tune = batch.autotune(ub, candidates=(4, 8, 16))
-    bat_ms = timed(lambda: batch.evaluate(ub, True), max(1, args.steps // 4))
-    graph = batch_mod.GraphedEvaluation(batch.system, ub)
-    gr_ms = timed(graph.replay, max(1, args.steps // 4))
-    line = {"metric": "batched design sweep: part evaluations/s (FP64)", "value": args.parts / (gr_ms / 1e3),
-            "unit": "parts/s", "n_gpus": 1, "steps": max(1, args.steps // 4), "warmup": 1,
-            "ms_per_step": gr_ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic",
-            "config": {"workload": f"{args.parts} sheet parts of 20k-150k IM Hex8 ({total} elements), Hill48 + "
-                                   f"Chaboche + Voce, logarithmic strain, bending from virgin points; one step = "
-                                   f"one evaluation of every part with its tangent"},
-            "sequential_ms": seq_ms, "batched_ms": bat_ms, "graph_ms": gr_ms,
-            "speedup_batched": seq_ms / bat_ms, "speedup_graph": seq_ms / gr_ms,
-            "elements_per_s_graph": total / (gr_ms / 1e3), "autotune_ms": tune,
-            "chosen_elements_per_block": batch.chosen_elements_per_block,
-            "yielding_fraction": yielding / (8.0 * total)}
+    ub = [torch.tensor(np.concatenate([dp[k] for dp in disps]), device=dev) for k in range(K)]
+    build_s = time.perf_counter() - t0
+    tune = batch.autotune(ub[0])
+    bat_ms, yielding = run_increments(batch.system, ub)
+    line = {"metric": "batched design sweep: parts/h of the element loop (FP64)", "value": args.parts / (bat_ms / 1e3) * 3600.0,
+            "unit": "parts/h", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": bat_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.parts} parts (Sobol over dome, truncated cone, elliptic cone, pyramid; "
+                                   f"footprint 15-20 mm, depth 2-4 mm, wall 30-55 deg), {total} IM Hex8 in all "
+                                   f"(20k-150k each, 2 layers), Hill48 + Chaboche + Voce, logarithmic strain; one "
+                                   f"step = {K} forming increments of every part, each 2 evaluations with the "
+                                   "tangent and a commit"},
+            "sequential_parts_per_hour": args.parts / (seq_ms / 1e3) * 3600.0,
+            "sequential_ms": seq_ms, "batched_ms": bat_ms, "speedup": seq_ms / bat_ms,
+            "elements_per_s_batched": 2 * K * total / (bat_ms / 1e3),
+            "elements_per_s_sequential": 2 * K * total / (seq_ms / 1e3),
+            "autotune_ms": {f"{m}/{e}": t for (m, e), t in tune.items()}, "chosen": list(batch.chosen),
+            "batch_build_s": build_s, "yielding_fraction": yielding / (8.0 * total),
+            "part_ms_min_max": [min(per_part), max(per_part)]}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -394,16 +399,34 @@ def run_adjoint(args, rank, world):
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     nx, ny = args.adj_nx, args.adj_ny
-    prob = wl.make_problem(nx, ny, 2, seed=5, sample=min(4096, nx * ny * 2))
-    mesh = prob.mesh
+    if args.adj_part == "cone":
+        # The fine-mesh part: the truncated cone formed to 35 % of its depth,
+        # its committed history from the element kernel; the grid over the
+        # cone's footprint.
+        csys, cprob = wl.make_cone_problem(args.adj_cone_n, 4, device=dev)
+        mesh, material = cprob.mesh, cprob.material
+        committed, modes = csys.committed_all(), csys.internal_all()
+        csys.close()
+        u_np = cprob.u0
+        r = wl.CONE["footprint_radius"]
+        box = (-r, r, -r, r)
+        part_desc = (f"truncated cone (18 mm footprint, 3 mm deep, 50 deg wall) formed to 35 % in a "
+                     f"{args.adj_cone_n}x{args.adj_cone_n}x4 IM Hex8 sheet")
+    else:
+        prob = wl.make_problem(nx, ny, 2, seed=5, sample=min(4096, nx * ny * 2))
+        mesh, material, committed, modes, u_np = prob.mesh, prob.material, prob.state, prob.alpha, prob.u
+        lo, hi = mesh.coords.min(axis=0), mesh.coords.max(axis=0)
+        box = (lo[0], hi[0], lo[1], hi[1])
+        part_desc = (f"{nx}x{ny}x2 IM Hex8 sheet part carrying the microbenchmark's committed Hill48 + Chaboche "
+                     f"history")
     x0 = torch.tensor(mesh.coords, device=dev)
-    lo, hi = mesh.coords.min(axis=0), mesh.coords.max(axis=0)
-    grid = pkg.BicubicHeights(lo[0], hi[0], lo[1], hi[1], n=20)
+    zmax = mesh.coords[:, 2].max()
+    grid = pkg.BicubicHeights(box[0], box[1], box[2], box[3], n=20)
     stencil = grid.stencil(mesh.coords[:, :2], device=dev)
-    top = torch.tensor(np.flatnonzero(np.isclose(mesh.coords[:, 2], hi[2])), device=dev)
-    u_formed = torch.tensor(prob.u, device=dev)
+    top = torch.tensor(np.flatnonzero(np.isclose(mesh.coords[:, 2], zmax)), device=dev)
+    u_formed = torch.tensor(u_np, device=dev)
     target = x0[top, 2] + u_formed.reshape(-1, 3)[top, 2]
-    release = pkg.Release(mesh, prob.material, prob.state, prob.alpha, pkg.supports_321(mesh))
+    release = pkg.Release(mesh, material, committed, modes, pkg.supports_321(mesh))
 
     def coords_of(p):
         lift = torch.zeros_like(x0)
@@ -465,9 +488,8 @@ def run_adjoint(args, rank, world):
             "value": g_ms / rel_ms, "unit": "x", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": g_ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"frozen release of a {nx}x{ny}x2 IM Hex8 sheet part ({mesh.num_elements} "
-                                   f"elements, {len(release.free)} free DOFs) carrying the microbenchmark's "
-                                   "committed Hill48 + Chaboche history, 3-2-1 supports; J = RMS springback of "
+            "config": {"workload": f"frozen release of a {part_desc} ({mesh.num_elements} elements, "
+                                   f"{len(release.free)} free DOFs), 3-2-1 supports; J = RMS springback of "
                                    "the top face; p = 20x20 bicubic height grid; one step = dJ/dp by "
                                    "torch.autograd (release solve + adjoint)"},
             "release_solve_ms": rel_ms, "newton_iterations": iterations, "gradient_ms": g_ms,
@@ -878,10 +900,15 @@ def main():
     p.add_argument("--part-nx", type=int, default=200)
     p.add_argument("--part-ny", type=int, default=200)
     p.add_argument("--parts", type=int, default=64)
+    p.add_argument("--sweep-increments", type=int, default=4)
     p.add_argument("--adj-nx", type=int, default=100)
     p.add_argument("--adj-ny", type=int, default=100)
     p.add_argument("--directions", type=int, default=32)
     p.add_argument("--adj-sample", type=int, default=40)
+    p.add_argument("--adj-part", default="sheet", choices=["sheet", "cone"],
+                   help="the part of the adjoint workload: a flat sheet with the microbenchmark's history, or the "
+                        "fine-mesh cone")
+    p.add_argument("--adj-cone-n", type=int, default=112)
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
 

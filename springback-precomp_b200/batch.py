@@ -75,24 +75,36 @@ class PartBatch:
         """The batch's displacement from the parts' ones."""
         return torch.cat([u.reshape(-1) for u in parts_u])
 
-    def autotune(self, u: torch.Tensor, candidates=(1, 2, 4, 8, 16), repeats: int = 2, want_tangent: bool = True):
-        """Time the element kernel at each elements-per-block candidate on
-        this batch (CUDA events on the system's stream, after one warm-up),
-        keep the fastest, and return {candidate: ms}. No result depends on
-        the choice."""
+    def autotune(self, u: torch.Tensor, candidates=(("phases", 0), ("phases", 8), ("single", 16), ("single", 8)),
+                 repeats: int = 2, want_tangent: bool = True):
+        """Time the element loop at each candidate mapping on this batch -
+        (local iteration, elements per block): the phase kernels (a thread
+        per point in the point kernels, an 8-lane group per element in the
+        others) or the single kernel (an 8-lane group per element, a point
+        per lane, start to finish), each at a block shape - with CUDA events
+        on the system's stream after one warm-up; keep the fastest and
+        return {candidate: ms}. No result depends on the choice. A bare
+        integer candidate is an elements-per-block of the current mode."""
         self.system.set_timing(True)
         times = {}
-        for epb in candidates:
+        for cand in candidates:
+            mode, epb = cand if isinstance(cand, tuple) else (None, cand)
+            if mode is not None:
+                self.system.set_local_iteration(mode)
             self.system.set_elements_per_block(epb)
             self.system.evaluate(u, 0.0, want_tangent)
             best = float("inf")
             for _ in range(repeats):
                 self.system.evaluate(u, 0.0, want_tangent)
                 best = min(best, self.system.last_timings()["element"])
-            times[epb] = best
+            times[cand] = best
         choice = min(times, key=times.get)
-        self.system.set_elements_per_block(choice)
-        self.chosen_elements_per_block = choice
+        mode, epb = choice if isinstance(choice, tuple) else (None, choice)
+        if mode is not None:
+            self.system.set_local_iteration(mode)
+        self.system.set_elements_per_block(epb)
+        self.chosen = choice
+        self.chosen_elements_per_block = epb
         return times
 
 

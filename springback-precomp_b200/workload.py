@@ -15,6 +15,7 @@ the element kernel itself (the GPU by default).
 from __future__ import annotations
 
 import dataclasses
+import math
 from typing import Callable, Optional
 
 import numpy as np
@@ -382,3 +383,55 @@ def make_cone_problem(n: int = 224, layers: int = 4, s: float = 0.35, steps: int
                           name="forming" if top else "support"))
     return sysm, ConeProblem(mesh=mesh, material=material, cone=cone, s=s, u0=u0, u=u1, tools=tools,
                              contact_radius=rc)
+
+
+# ---- the design sweep: parts of four families from a Sobol sequence ----------
+
+SWEEP_BOUNDS = dict(footprint_radius=(7.5e-3, 10.0e-3), depth=(2.0e-3, 4.0e-3), wall_angle_deg=(30.0, 55.0),
+                    axis_ratio=(1.0, 1.6), elements=(20000, 150000))
+SWEEP_FAMILIES = ("dome", "truncated_cone", "elliptic_cone", "pyramid")
+
+
+def sweep_parts(count: int = 64, seed: int = 20260, layers: int = 2):
+    """The design sweep's parts: a scrambled Sobol sequence (scipy's, seeded)
+    over the family, footprint radius 7.5-10 mm, depth 2-4 mm, wall angle
+    30-55 degrees, elliptic axis ratio 1.0-1.6 and the mesh size, 20k-150k
+    Hex8 in `layers` layers over a square blank 2.6 footprint radii wide, 1
+    mm thick. Fillets are 2 mm at rim and floor. Returns a list of (part,
+    mesh)."""
+    from scipy.stats import qmc
+
+    from .parts import Dome, EllipticCone, Pyramid, TruncatedCone
+
+    pts = qmc.Sobol(d=6, scramble=True, seed=seed).random(count)
+    b = SWEEP_BOUNDS
+
+    def lerp(u, k):
+        lo, hi = b[k]
+        return lo + u * (hi - lo)
+
+    out = []
+    for u in pts:
+        family = SWEEP_FAMILIES[min(int(u[0] * 4), 3)]
+        r, d, ang = lerp(u[1], "footprint_radius"), lerp(u[2], "depth"), lerp(u[3], "wall_angle_deg")
+        ratio = lerp(u[4], "axis_ratio")
+        f = 2.0e-3
+        if family == "truncated_cone":
+            part = TruncatedCone.with_footprint(r, ang, d, f, f)
+        elif family == "elliptic_cone":
+            t = -TruncatedCone.with_footprint(r, ang, d, f, f).profile.w_first
+            part = EllipticCone(r - t, (r - t) / ratio, ang, d, f, f)
+        elif family == "pyramid":
+            t = -TruncatedCone.with_footprint(r, ang, d, f, f).profile.w_first
+            half = (r - t) / math.sqrt(2.0)
+            run = TruncatedCone(1.0, ang, d, f, f).profile.w_last
+            part = Pyramid(half, half / ratio ** 0.5, ang, d, min(half / ratio ** 0.5, max(run, 0.5 * half)), f, f)
+        else:
+            part = Dome(r, min(d, 0.9 * r), f, 1.0 / ratio)
+        ne = int(lerp(u[5], "elements"))
+        n = max(8, int(round(math.sqrt(ne / layers))))
+        blank = 2.6 * r
+        mesh = structured_hex_mesh(n, n, layers, blank, blank, CONE_THICKNESS, x0=-0.5 * blank, y0=-0.5 * blank,
+                                   z0=-CONE_THICKNESS)
+        out.append((part, mesh))
+    return out

@@ -113,3 +113,21 @@ def test_autotune_picks_a_shape_and_changes_no_result(pkg, cuda, batch_setup):
     assert set(times) == {1, 2, 4, 8} and all(t > 0 for t in times.values())
     assert batch.chosen_elements_per_block == min(times, key=times.get)
     assert torch.equal(batch.evaluate(u).internal, before)
+
+
+def test_autotune_over_the_thread_mappings(pkg, cuda, batch_setup):
+    """The autotuner's search over the mapping of points to threads - the
+    phase kernels or the single kernel, at two block shapes each - keeps the
+    fastest; the results stay those of the default mapping (to the last bits
+    the two compiled paths may differ in)."""
+    batch_mod, meshes, mat, us = batch_setup
+    batch = batch_mod.PartBatch(meshes, mat)
+    u = torch.tensor(np.concatenate(us), device=cuda)
+    before = batch.evaluate(u)
+    f0, k0 = before.internal.clone(), before.tangent.clone()
+    cands = (("phases", 0), ("phases", 8), ("single", 16), ("single", 8))
+    times = batch.autotune(u, candidates=cands)
+    assert set(times) == set(cands) and batch.chosen == min(times, key=times.get)
+    after = batch.evaluate(u)
+    assert (after.internal - f0).abs().max().item() <= 1e-13 * f0.abs().max().item()
+    assert (after.tangent - k0).abs().max().item() <= 1e-13 * k0.abs().max().item()
