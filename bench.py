@@ -676,7 +676,13 @@ def run_cone(args, rank, world):
             "contact": {"begin_grid_ms": grid_ms, "begin_scan_ms": scan_ms, "candidates": grid_cand,
                         "active": [int(cev.tools[k][6]) for k in range(2)],
                         "slaves": [int(len(t["nodes"])) for t in prob.tools], "margin_m": margin},
-            "gpu_launches": None, "clocks": clocks.summary(), "yielding_fraction": ev.yielding_points / (8.0 * ne),
+            # K1's phase kernels (26 rounds of 5, the condensation, the
+            # single kernel's list), K2b + finish, K2a, the schedule (3); per
+            # tool 7 contact kernels (moved points, evaluate, the ordered
+            # compaction's 3, scatter, resultants), the norms' two stages over
+            # both tools, and the blocks' add.
+            "gpu_launches": args.steps * ((26 * 5 + 2) + 6 + 2 * 7 + 2 + 1), "clocks": clocks.summary(),
+            "yielding_fraction": ev.yielding_points / (8.0 * ne),
             "setup_s": setup_s}
     print(json.dumps(line), flush=True)
     contact.close()
@@ -1034,14 +1040,14 @@ def main():
                                       prob.mesh.gather(prob.u), committed, prob.alpha)
             flops_per_element = cnt / prob.mesh.num_elements
         el_ms = statistics.mean(elem_ms)
-        # Kernels of one step: K1 (the phase kernels: 26 rounds of 4 launches,
+        # Kernels of one step: K1 (the phase kernels: 26 rounds of 5 launches,
         # the condensation, the single kernel for the elements it takes; or
-        # one launch), then the force gather (2), the value gather, the
-        # summary and the schedule (2).
+        # one launch), then the force gather and its finish (2), the value
+        # gather and the schedule (3).
         phases = args.element == "incompatible_modes" and args.local_iteration == "phases"
-        launches_per_step = (26 * 4 + 2 if phases else 1) + 6
-        k1_name = ("K1: the local iteration as phase kernels (wave_pre / wave_return / wave_post / wave_control "
-                   "x 26 rounds, wave_condense, element_list)" if phases else
+        launches_per_step = (26 * 5 + 2 if phases else 1) + 6
+        k1_name = ("K1: the local iteration as phase kernels (wave_pre / wave_return / wave_log / wave_post / "
+                   "wave_control x 26 rounds, wave_condense, element_list)" if phases else
                    "element_kernel (K1)" if args.element == "incompatible_modes" else "standard_kernel (K1s)")
         roofline = None
         if flops_per_element:
