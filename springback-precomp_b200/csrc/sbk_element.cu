@@ -1536,17 +1536,19 @@ struct __align__(16) PreShared {
 #define SBK_MINB_CONDENSE 2
 #endif
 
+// The control kernel's record: K_aa (then, once the LU has copied it, its
+// symmetric part in place for the Cholesky test), the LU, the pass's sums.
+// 1.9 KB per element, so that six 4-warp blocks fit an SM (the kernel's
+// registers allow six).
 template <int G>
 struct __align__(16) ControlShared {
-  double kc[kKcStride];
+  double kc[81];
   double lu[81];
-  double work[243];
   double r[33];
   double scale[9];
   double flo[9];
   double alpha[9];
   double dir[9];
-  double r0[9];
   double maxpivot;
   int rowp[9], colp[9];
 };
@@ -1937,8 +1939,6 @@ __global__ void __launch_bounds__(128) wave_control_kernel(const __grid_constant
     const double scale = abs_max9(s.scale);
     const double floor_ = kLocalRoundOff * abs_max9(s.flo);
     const bool invertible = fullpiv_lu9_rows_inline<G>(c, s.kc, s.lu, s.rowp, s.colp, &s.maxpivot);
-    for (int k = lane; k < 81; k += G) s.work[k] = s.kc[k];
-    for (int k = lane; k < 9; k += G) s.r0[k] = s.r[24 + k];
     c.sync();
     if (!invertible) {
       if (lane == 0) wave_fail(code, first_failure, e, SBK_EL_LOCAL_SINGULAR);
@@ -1963,19 +1963,26 @@ __global__ void __launch_bounds__(128) wave_control_kernel(const __grid_constant
       continue;
     }
     ++iterations;
-    for (int idx = lane; idx < 81; idx += G) {
-      const int a = idx / 9, b = idx % 9;
-      const double v = 0.5 * (s.work[a * 9 + b] + s.work[b * 9 + a]);
-      s.work[81 + idx] = v;
-      s.work[162 + idx] = v;
+    // The symmetric part (K + K^T) / 2 in place: each lane owns the pairs
+    // (a, b), a <= b, it writes, and reads nothing another lane writes.
+    for (int idx = lane; idx < 45; idx += G) {
+      int a = 0, rest = idx;
+      while (rest >= 9 - a) {
+        rest -= 9 - a;
+        ++a;
+      }
+      const int b = a + rest;
+      const double v = 0.5 * (s.kc[a * 9 + b] + s.kc[b * 9 + a]);
+      s.kc[a * 9 + b] = v;
+      s.kc[b * 9 + a] = v;
     }
     c.sync();
     if (lane == 0) {
       double nw[9];
-      fullpiv_solve9_inline(s.lu, s.rowp, s.colp, s.r0, nw);
+      fullpiv_solve9_inline(s.lu, s.rowp, s.colp, s.r + 24, nw);
       for (int k = 0; k < 9; ++k) s.dir[k] = -nw[k];
     }
-    const bool positive = llt9_rows_inline<G>(c, s.work + 162);
+    const bool positive = llt9_rows_inline<G>(c, s.kc);
     c.sync();
     if (!positive) {
       if (lane == 0) append(fallback_list, fallback_count, e);

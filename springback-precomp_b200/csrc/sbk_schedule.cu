@@ -16,6 +16,8 @@
 // assembly sums in element order.
 #include <cuda_runtime.h>
 
+#include <cub/device/device_scan.cuh>
+
 #include "sbk_element.h"
 
 namespace sbk {
@@ -53,33 +55,8 @@ __global__ void __launch_bounds__(256) schedule_count_kernel(int64_t ne, int nq,
   for (int i = threadIdx.x; i < kBuckets; i += blockDim.x) count[(int64_t)i * nb + b] = h[i];
 }
 
-// Pass 2: exclusive prefix sum of the counts in bucket-major order, by one
-// block: each thread sums a contiguous stretch, then the stretches' totals
-// are scanned.
-__global__ void __launch_bounds__(1024) schedule_scan_kernel(int64_t n, int32_t* __restrict__ count) {
-  __shared__ int32_t part[1024];
-  const int64_t per = (n + blockDim.x - 1) / blockDim.x;
-  const int64_t lo = threadIdx.x * per, hi = lo + per < n ? lo + per : n;
-  int32_t s = 0;
-  for (int64_t i = lo; i < hi; ++i) s += count[i];
-  part[threadIdx.x] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int32_t run = 0;
-    for (int i = 0; i < (int)blockDim.x; ++i) {
-      const int32_t v = part[i];
-      part[i] = run;
-      run += v;
-    }
-  }
-  __syncthreads();
-  int32_t run = part[threadIdx.x];
-  for (int64_t i = lo; i < hi; ++i) {
-    const int32_t v = count[i];
-    count[i] = run;
-    run += v;
-  }
-}
+// Pass 2: exclusive prefix sum of the counts in bucket-major order into the
+// starts, by CUB's device-wide scan (its temporary storage after the keys).
 
 // Pass 3: each chunk places its elements in mesh order at its buckets'
 // offsets (one thread walks the chunk, so the order within a bucket is the
@@ -99,19 +76,40 @@ __global__ void schedule_place_kernel(int64_t ne, int64_t nb, const int16_t* __r
 
 }  // namespace
 
-size_t schedule_scratch_ints(int64_t ne) {
+namespace {
+// The counts (kBuckets per chunk), their scan (the starts), the int16 keys,
+// then the scan's temporary storage at a 256-byte boundary: offsets in ints.
+int64_t counts_of(int64_t ne) {
   const int64_t nb = (ne + kChunk - 1) / kChunk;
-  return (size_t)(kBuckets * (nb > 0 ? nb : 1)) + (size_t)(ne + 1) / 2;  // the counts, then int16 keys
+  return (int64_t)kBuckets * (nb > 0 ? nb : 1);
+}
+int64_t temp_offset(int64_t ne) {
+  const int64_t ints = 2 * counts_of(ne) + (ne + 1) / 2;
+  return (ints + 63) / 64 * 64;
+}
+size_t scan_temp_bytes(int64_t n) {
+  size_t bytes = 0;
+  cub::DeviceScan::ExclusiveSum(nullptr, bytes, (int32_t*)nullptr, (int32_t*)nullptr, (int)n);
+  return bytes;
+}
+}  // namespace
+
+size_t schedule_scratch_ints(int64_t ne) {
+  return (size_t)temp_offset(ne) + (scan_temp_bytes(counts_of(ne)) + 3) / 4;
 }
 
 int launch_schedule(int64_t ne, int nq, const int32_t* iterations, const uint8_t* yield, int32_t* scratch,
                     int32_t* order, cudaStream_t stream) {
   if (ne <= 0) return 0;
   const int64_t nb = (ne + kChunk - 1) / kChunk;
-  int16_t* keys = reinterpret_cast<int16_t*>(scratch + (int64_t)kBuckets * nb);
+  const int64_t n = (int64_t)kBuckets * nb;
+  int32_t* starts = scratch + n;
+  int16_t* keys = reinterpret_cast<int16_t*>(scratch + 2 * n);
   schedule_count_kernel<<<(unsigned)nb, 256, 0, stream>>>(ne, nq, nb, iterations, yield, scratch, keys);
-  schedule_scan_kernel<<<1, 1024, 0, stream>>>((int64_t)kBuckets * nb, scratch);
-  schedule_place_kernel<<<(unsigned)nb, 32, 0, stream>>>(ne, nb, keys, scratch, order);
+  size_t bytes = scan_temp_bytes(n);
+  cudaError_t err = cub::DeviceScan::ExclusiveSum(scratch + temp_offset(ne), bytes, scratch, starts, (int)n, stream);
+  if (err != cudaSuccess) return (int)err;
+  schedule_place_kernel<<<(unsigned)nb, 32, 0, stream>>>(ne, nb, keys, starts, order);
   return (int)cudaGetLastError();
 }
 

@@ -392,16 +392,47 @@ SWEEP_BOUNDS = dict(footprint_radius=(7.5e-3, 10.0e-3), depth=(2.0e-3, 4.0e-3), 
 SWEEP_FAMILIES = ("dome", "truncated_cone", "elliptic_cone", "pyramid")
 
 
+SWEEP_FLOOR_MARGIN = 0.5e-3
+
+
+def sweep_part(family: str, r: float, d: float, ang: float, ratio: float, f: float = 2.0e-3):
+    """One part of the sweep and the room its walls leave: (part, inner - w),
+    with w the inward distance from the rim at which the floor fillet ends
+    and inner the least inward distance of the footprint's medial axis (the
+    truncated cone's top radius; the ellipse's b^2 / a, where the axis'
+    ridge ends; the rounded rectangle's smaller half-width or corner
+    radius). Where that room is negative the walls meet in a crease instead
+    of a floor; a dome has none."""
+    from .parts import Dome, EllipticCone, Pyramid, TruncatedCone
+
+    if family == "dome":
+        return Dome(r, min(d, 0.9 * r), f, 1.0 / ratio), math.inf
+    cone = TruncatedCone.with_footprint(r, ang, d, f, f)
+    w = cone.profile.w_last
+    if family == "truncated_cone":
+        return cone, cone.top_radius - w
+    t = -cone.profile.w_first
+    if family == "elliptic_cone":
+        a, b = r - t, (r - t) / ratio
+        return EllipticCone(a, b, ang, d, f, f), b * b / a - w
+    half = (r - t) / math.sqrt(2.0)
+    hy = half / ratio ** 0.5
+    rc = min(hy, max(w + SWEEP_FLOOR_MARGIN, 0.5 * half))
+    return Pyramid(half, hy, ang, d, rc, f, f), min(hy, rc) - w
+
+
 def sweep_parts(count: int = 64, seed: int = 20260, layers: int = 2):
     """The design sweep's parts: a scrambled Sobol sequence (scipy's, seeded)
     over the family, footprint radius 7.5-10 mm, depth 2-4 mm, wall angle
     30-55 degrees, elliptic axis ratio 1.0-1.6 and the mesh size, 20k-150k
     Hex8 in `layers` layers over a square blank 2.6 footprint radii wide, 1
-    mm thick. Fillets are 2 mm at rim and floor. Returns a list of (part,
-    mesh)."""
+    mm thick. Fillets are 2 mm at rim and floor. A shallow wall does not fit
+    a narrow footprint at full depth (a 30 degree wall 4 mm deep runs 6.9
+    mm): where the walls would meet in a crease, the part takes the largest
+    depth that leaves its floor SWEEP_FLOOR_MARGIN clear of the medial axis
+    (a sheet laid on a crease folds within one element). Returns a list of
+    (part, mesh)."""
     from scipy.stats import qmc
-
-    from .parts import Dome, EllipticCone, Pyramid, TruncatedCone
 
     pts = qmc.Sobol(d=6, scramble=True, seed=seed).random(count)
     b = SWEEP_BOUNDS
@@ -415,19 +446,26 @@ def sweep_parts(count: int = 64, seed: int = 20260, layers: int = 2):
         family = SWEEP_FAMILIES[min(int(u[0] * 4), 3)]
         r, d, ang = lerp(u[1], "footprint_radius"), lerp(u[2], "depth"), lerp(u[3], "wall_angle_deg")
         ratio = lerp(u[4], "axis_ratio")
-        f = 2.0e-3
-        if family == "truncated_cone":
-            part = TruncatedCone.with_footprint(r, ang, d, f, f)
-        elif family == "elliptic_cone":
-            t = -TruncatedCone.with_footprint(r, ang, d, f, f).profile.w_first
-            part = EllipticCone(r - t, (r - t) / ratio, ang, d, f, f)
-        elif family == "pyramid":
-            t = -TruncatedCone.with_footprint(r, ang, d, f, f).profile.w_first
-            half = (r - t) / math.sqrt(2.0)
-            run = TruncatedCone(1.0, ang, d, f, f).profile.w_last
-            part = Pyramid(half, half / ratio ** 0.5, ang, d, min(half / ratio ** 0.5, max(run, 0.5 * half)), f, f)
-        else:
-            part = Dome(r, min(d, 0.9 * r), f, 1.0 / ratio)
+        part, room = sweep_part(family, r, d, ang, ratio)
+        if room < SWEEP_FLOOR_MARGIN:
+            # The shallowest depth whose fillets fit the wall (below it they
+            # overlap), then the deepest above it with a clear floor.
+            lo, hi = 0.0, d
+            for _ in range(50):
+                mid = 0.5 * (lo + hi)
+                try:
+                    sweep_part(family, r, mid, ang, ratio)
+                    hi = mid
+                except ValueError:
+                    lo = mid
+            lo, hi = hi, d
+            for _ in range(50):
+                mid = 0.5 * (lo + hi)
+                if sweep_part(family, r, mid, ang, ratio)[1] >= SWEEP_FLOOR_MARGIN:
+                    lo = mid
+                else:
+                    hi = mid
+            part, room = sweep_part(family, r, lo, ang, ratio)
         ne = int(lerp(u[5], "elements"))
         n = max(8, int(round(math.sqrt(ne / layers))))
         blank = 2.6 * r
