@@ -40,3 +40,39 @@ def test_fine_mesh_cone_has_the_configured_footprint():
     slope = np.diff(z) / np.diff(r)
     assert abs(slope.max() - np.tan(np.radians(50.0))) < 1e-3
     assert z[r >= 9.0e-3].max() == 0.0 and z[r < 9.0e-3 - 1e-6].max() < 0.0
+
+
+def test_sweep_parts_keep_a_floor():
+    """The design sweep's 64 parts: four families, 16 each, within the
+    footprint and wall-angle ranges, meshes of 20k-150k elements; every part
+    leaves its floor clear of the footprint's medial axis (a sheet laid on
+    a crease where two walls meet folds inside one element, which no
+    forming run survives), the depth capped where the sampled one would
+    not (the capped parts at the largest depth that does)."""
+    wl = importlib.import_module("springback-precomp_b200.workload")
+    parts = wl.sweep_parts(64)
+    families = [type(p).family for p, _ in parts]
+    assert {f: families.count(f) for f in set(families)} == {f: 16 for f in wl.SWEEP_FAMILIES}
+    capped = 0
+    for p, m in parts:
+        assert 20000 * 0.95 <= m.num_elements <= 150000 * 1.05
+        if p.family == "dome":
+            continue
+        assert 30.0 <= p.wall_angle_deg <= 55.0
+        r = p.footprint_radius()
+        # A pyramid's rounded square is inscribed in the sampled footprint.
+        lo = 0.0 if p.family == "pyramid" else 7.5e-3 * (1 - 1e-9)
+        assert lo <= r <= 10.0e-3 * (1 + 1e-9), r
+        if p.family == "truncated_cone":
+            inner = p.top_radius
+        elif p.family == "elliptic_cone":
+            a, b = max(p.semi_axis_x, p.semi_axis_y), min(p.semi_axis_x, p.semi_axis_y)
+            inner = b * b / a
+        else:
+            inner = min(p.half_width_x, p.half_width_y, p.corner_radius)
+        room = inner - p.profile.w_last
+        assert room >= wl.SWEEP_FLOOR_MARGIN * (1 - 1e-6), (p, room)
+        if p.depth < 2.0e-3 - 1e-12 or room < wl.SWEEP_FLOOR_MARGIN * 1.01:
+            capped += 1
+        assert p.depth <= 4.0e-3
+    assert capped < 32
