@@ -411,7 +411,11 @@ def run_adjoint(args, rank, world):
         r = wl.CONE["footprint_radius"]
         box = (-r, r, -r, r)
         part_desc = (f"truncated cone (18 mm footprint, 3 mm deep, 50 deg wall) formed to 35 % in a "
-                     f"{args.adj_cone_n}x{args.adj_cone_n}x4 IM Hex8 sheet")
+                     f"{args.adj_cone_n}x{args.adj_cone_n}x4 IM Hex8 sheet, its imbalance released in 8 increments")
+        # Its history is loaded by imposed displacements, far from
+        # equilibrium: full Newton steps from it overshoot onto another
+        # equilibrium of the supported sheet or invert elements.
+        increments = 8
     else:
         prob = wl.make_problem(nx, ny, 2, seed=5, sample=min(4096, nx * ny * 2))
         mesh, material, committed, modes, u_np = prob.mesh, prob.material, prob.state, prob.alpha, prob.u
@@ -419,6 +423,7 @@ def run_adjoint(args, rank, world):
         box = (lo[0], hi[0], lo[1], hi[1])
         part_desc = (f"{nx}x{ny}x2 IM Hex8 sheet part carrying the microbenchmark's committed Hill48 + Chaboche "
                      f"history")
+        increments = 1
     x0 = torch.tensor(mesh.coords, device=dev)
     zmax = mesh.coords[:, 2].max()
     grid = pkg.BicubicHeights(box[0], box[1], box[2], box[3], n=20)
@@ -426,7 +431,7 @@ def run_adjoint(args, rank, world):
     top = torch.tensor(np.flatnonzero(np.isclose(mesh.coords[:, 2], zmax)), device=dev)
     u_formed = torch.tensor(u_np, device=dev)
     target = x0[top, 2] + u_formed.reshape(-1, 3)[top, 2]
-    release = pkg.Release(mesh, material, committed, modes, pkg.supports_321(mesh))
+    release = pkg.Release(mesh, material, committed, modes, pkg.supports_321(mesh), increments=increments)
 
     def coords_of(p):
         lift = torch.zeros_like(x0)
@@ -480,7 +485,7 @@ def run_adjoint(args, rank, world):
         jd = []
         for sign in (1.0, -1.0):
             c = coords_of(torch.tensor(sign * h * d, device=dev))
-            jd.append(float(pkg.springback_rms(c, release.solve(c, u_star), top, target)))
+            jd.append(float(pkg.springback_rms(c, release.solve(c, u_star, increments=1), top, target)))
         fd = (jd[0] - jd[1]) / (2.0 * h)
         errors.append(abs(float((g * d).sum()) - fd) / abs(fd))
     fd_s = time.perf_counter() - t0
@@ -504,37 +509,46 @@ def run_adjoint(args, rank, world):
                                     "seconds": fd_s},
             "factor_kind": release.part.kind, "clocks": clocks.summary()}
     if not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_adjoint(pkg, args.adj_sample)
+        line["cpu_baseline"] = (cpu_adjoint(pkg, 16, "cone") if args.adj_part == "cone"
+                                else cpu_adjoint(pkg, args.adj_sample))
     print(json.dumps(line))
     release.close()
     return 0
 
 
-def cpu_adjoint(pkg, n):
+def cpu_adjoint(pkg, n, part="sheet"):
     """The same release and gradient with the oracle on the host cores (the
     oracle's release Newton with scipy's sparse LU, its adjoint with the
     transposed block and its per-element shape derivative) on an n x n x 2
-    sample part whose history the oracle loads."""
+    sample part whose history the oracle loads, or an n x n x 4 cone part of
+    the fine-mesh construction (released in 8 increments, as on the GPU)."""
     orc = oracle_module()
-    prob, committed = oracle_problem(orc, n, n, 2, 5)
-    mesh, mat = prob.mesh, prob.material
+    if part == "cone":
+        wl = importlib.import_module(PKG + ".workload")
+        mesh, mat, committed, alpha, _ = cone_sample(orc, n)
+        u0 = (wl.formed_positions(mesh, wl.cone_part(), 0.35) - mesh.coords).reshape(-1)
+        increments, desc = 8, f"{n}x{n}x4 cone part ({mesh.num_elements} elements) released in 8 increments"
+    else:
+        prob, committed = oracle_problem(orc, n, n, 2, 5)
+        mesh, mat, alpha, u0 = prob.mesh, prob.material, prob.alpha, prob.u
+        increments, desc = 1, f"{n}x{n}x2 part ({mesh.num_elements} elements)"
     m = mat.as_dict()
     m["yield_stress"] = 1e300  # frozen
     free = pkg.supports_321(mesh)
     top = np.flatnonzero(np.isclose(mesh.coords[:, 2], mesh.coords[:, 2].max()))
     t0 = time.perf_counter()
-    u, iterations = orc.release_solve(m, mesh.coords, mesh.connectivity, committed, prob.alpha, free, prob.u)
+    u, iterations = orc.release_solve(m, mesh.coords, mesh.connectivity, committed, alpha, free, u0,
+                                      increments=increments)
     release_s = time.perf_counter() - t0
-    d = u.reshape(-1, 3)[top, 2] - prob.u.reshape(-1, 3)[top, 2]
+    d = u.reshape(-1, 3)[top, 2] - u0.reshape(-1, 3)[top, 2]
     j = float(np.sqrt(np.mean(d * d)))
     dj = np.zeros(mesh.num_dofs)
     dj[3 * top + 2] = d / (len(top) * j)
     t0 = time.perf_counter()
-    orc.release_adjoint(m, mesh.coords, mesh.connectivity, committed, prob.alpha, free, u, dj)
+    orc.release_adjoint(m, mesh.coords, mesh.connectivity, committed, alpha, free, u, dj)
     adjoint_s = time.perf_counter() - t0
     return {"value": (release_s + adjoint_s) / release_s, "unit": "x", "cores": os.cpu_count(), "kind": "port",
-            "sample": f"{n}x{n}x2 part ({mesh.num_elements} elements), the oracle's history, one release and one "
-                      "gradient",
+            "sample": f"{desc}, the oracle's history, one release and one gradient",
             "release_solve_ms": release_s * 1e3, "newton_iterations": iterations, "adjoint_ms": adjoint_s * 1e3}
 
 
@@ -677,11 +691,11 @@ def run_cone(args, rank, world):
                         "active": [int(cev.tools[k][6]) for k in range(2)],
                         "slaves": [int(len(t["nodes"])) for t in prob.tools], "margin_m": margin},
             # K1's phase kernels (26 rounds of 5, the condensation, the
-            # single kernel's list), K2b + finish, K2a, the schedule (3); per
-            # tool 7 contact kernels (moved points, evaluate, the ordered
-            # compaction's 3, scatter, resultants), the norms' two stages over
-            # both tools, and the blocks' add.
-            "gpu_launches": args.steps * ((26 * 5 + 2) + 6 + 2 * 7 + 2 + 1), "clocks": clocks.summary(),
+            # single kernel's list), K2b + finish, K2a; per tool 7 contact
+            # kernels (moved points, evaluate, the ordered compaction's 3,
+            # scatter, resultants), the norms' two stages over both tools,
+            # and the blocks' add.
+            "gpu_launches": args.steps * ((26 * 5 + 2) + 3 + 2 * 7 + 2 + 1), "clocks": clocks.summary(),
             "yielding_fraction": ev.yielding_points / (8.0 * ne),
             "setup_s": setup_s}
     print(json.dumps(line), flush=True)
@@ -1043,9 +1057,10 @@ def main():
         # Kernels of one step: K1 (the phase kernels: 26 rounds of 5 launches,
         # the condensation, the single kernel for the elements it takes; or
         # one launch), then the force gather and its finish (2), the value
-        # gather and the schedule (3).
+        # gather, and for the single kernel the schedule (count, CUB's scan,
+        # place).
         phases = args.element == "incompatible_modes" and args.local_iteration == "phases"
-        launches_per_step = (26 * 5 + 2 if phases else 1) + 6
+        launches_per_step = (26 * 5 + 2 if phases else 1 + 3) + 3
         k1_name = ("K1: the local iteration as phase kernels (wave_pre / wave_return / wave_log / wave_post / "
                    "wave_control x 26 rounds, wave_condense, element_list)" if phases else
                    "element_kernel (K1)" if args.element == "incompatible_modes" else "standard_kernel (K1s)")

@@ -447,13 +447,16 @@ def add_to(full, free, part, factor) -> np.ndarray:
 
 
 def release_solve(m: dict, coords, conn, committed, alpha_n, free, u0, kinematics="logarithmic", tol=1e-10,
-                  max_iterations=40, threads=0):
+                  max_iterations=40, threads=0, increments=1):
     """The released equilibrium on the CPU: Newton on the free rows of
     f_int(u) = 0 from u0 (its held DOFs kept), every tangent the oracle's
     assembled CSC (NonlinearSystem::evaluate restated) and every correction
-    a scipy sparse solve of its free-free block, until a full step is below
-    `tol` of u, then one step more. The frozen release passes a material
-    whose yield stress no point reaches. Returns (u, iterations)."""
+    a scipy sparse solve of its free-free block, a step halved while an
+    element refuses it, until a full step is below `tol` of u, then one step
+    more. `increments` > 1 takes the start's imbalance r0 off in equal
+    steps (equilibrium of f_int(u) = (1 - k / increments) r0 at each k), as
+    the device Release does. The frozen release passes a material whose
+    yield stress no point reaches. Returns (u, Newton iterations)."""
     import scipy.sparse
     import scipy.sparse.linalg
 
@@ -462,18 +465,42 @@ def release_solve(m: dict, coords, conn, committed, alpha_n, free, u0, kinematic
     pat = pattern(nn, conn)
     free = np.asarray(free, dtype=np.int64)
     u = np.array(u0, dtype=np.float64, copy=True)
-    converged = False
-    for it in range(max_iterations):
-        r = system_evaluate(m, coords, conn, u, committed, alpha_n, kinematics=kinematics, threads=threads, pat=pat)
-        if r["code"] != 0:
-            raise RuntimeError(f"the oracle's element {r['failed_element']} failed in the release")
-        if converged:
-            return u, it
-        k = scipy.sparse.csc_matrix((r["values"], pat["inner"], pat["outer"]), shape=(3 * nn, 3 * nn))
-        du = scipy.sparse.linalg.spsolve(k[free][:, free].tocsc(), -r["internal"][free])
-        u[free] += du
-        converged = np.linalg.norm(du) <= tol * np.linalg.norm(u)
-    raise RuntimeError("the oracle's release did not converge")
+
+    def evaluate(x):
+        return system_evaluate(m, coords, conn, x, committed, alpha_n, kinematics=kinematics, threads=threads, pat=pat)
+
+    r = evaluate(u)
+    if r["code"] != 0:
+        raise RuntimeError(f"the oracle's element {r['failed_element']} failed in the release")
+    r0 = r["internal"][free].copy()
+    total = 0
+    for k in range(1, increments + 1):
+        left = 1.0 - k / increments
+        last = k == increments
+        converged = False
+        for _ in range(max_iterations):
+            kk = scipy.sparse.csc_matrix((r["values"], pat["inner"], pat["outer"]), shape=(3 * nn, 3 * nn))
+            du = scipy.sparse.linalg.spsolve(kk[free][:, free].tocsc(), -(r["internal"][free] - left * r0))
+            step = 1.0
+            while True:
+                trial = u.copy()
+                trial[free] += step * du
+                rt = evaluate(trial)
+                if rt["code"] == 0:
+                    break
+                step *= 0.5
+                if step < 1.0 / 1024:
+                    raise RuntimeError(f"the oracle's element {rt['failed_element']} failed in the release")
+            u, r = trial, rt
+            total += 1
+            if converged:
+                break
+            converged = step == 1.0 and np.linalg.norm(du) <= tol * np.linalg.norm(u)
+            if converged and not last:
+                break
+        else:
+            raise RuntimeError("the oracle's release did not converge")
+    return u, total
 
 
 def release_adjoint(m: dict, coords, conn, committed, alpha_n, free, u, dj_du, kinematics="logarithmic",

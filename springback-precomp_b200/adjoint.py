@@ -109,7 +109,8 @@ class Release:
     the partition of its supports (`free`: the DOFs not held)."""
 
     def __init__(self, mesh: HexMesh, material, committed: np.ndarray, modes: np.ndarray, free: Sequence[int],
-                 kinematics: str = "logarithmic", tolerance: float = 1e-10, max_iterations: int = 40):
+                 kinematics: str = "logarithmic", tolerance: float = 1e-10, max_iterations: int = 40,
+                 increments: int = 1):
         self.mesh = mesh
         self.system = NonlinearSystem(mesh, material, kinematics=kinematics)
         self.system.set_committed(committed)
@@ -119,6 +120,7 @@ class Release:
         self.part = PartitionedFactor.for_system(self.system, self.free)
         self.tolerance = tolerance
         self.max_iterations = max_iterations
+        self.increments = increments
         self.iterations = 0
         self.factorizations = 0
         self._factored = None
@@ -145,36 +147,56 @@ class Release:
         f = getattr(self, "_factored", None)
         return f is not None and torch.equal(f[0], u) and torch.equal(f[1], coords.reshape(-1, 3))
 
-    def solve(self, coords: torch.Tensor, u0: torch.Tensor) -> torch.Tensor:
+    def solve(self, coords: torch.Tensor, u0: torch.Tensor, increments: Optional[int] = None) -> torch.Tensor:
         """The released displacement u* at the reference coordinates coords
         (num_nodes x 3, device) from u0 (its held DOFs kept): Newton, a step
         halved while an element refuses it, until a full step is below
         `tolerance` of u, then one step more. SolverError when it does not
-        converge."""
+        converge.
+
+        `increments` > 1 takes the imbalance of the start, r0 = f_int(u0) on
+        the free rows, off in that many equal steps - Newton to equilibrium
+        of f_int(u) = (1 - k / increments) r0 at each k - for a start far
+        from equilibrium (a history loaded by imposed displacements), where
+        full Newton steps from u0 overshoot. The material is frozen, so the
+        end state solves f_int(u*) = 0 whatever the path that reached it.
+        None: the release's own `increments`."""
+        increments = self.increments if increments is None else int(increments)
         self.system.set_coordinates(coords.reshape(-1, 3))
         u = u0.detach().clone()
         ev = self._tangent(u, coords)
-        r = self.part.restrict(ev.internal)
-        converged = False
-        for it in range(self.max_iterations):
-            du = self.part.solve(-r)
-            step = 1.0
-            while True:
-                trial = self.part.add_to(u.clone(), du, step)
-                try:
-                    ev = self._tangent(trial, coords)
+        r_start = self.part.restrict(ev.internal)
+        total = 0
+        for k in range(1, increments + 1):
+            left = 1.0 - k / increments
+            last = k == increments
+            r = self.part.restrict(ev.internal) - left * r_start
+            converged = False
+            for it in range(self.max_iterations):
+                du = self.part.solve(-r)
+                step = 1.0
+                while True:
+                    trial = self.part.add_to(u.clone(), du, step)
+                    try:
+                        ev = self._tangent(trial, coords)
+                        break
+                    except _capi.SolverError:
+                        step *= 0.5
+                        if step < 1.0 / 1024:
+                            raise
+                u = trial
+                total += 1
+                r = self.part.restrict(ev.internal) - left * r_start
+                if converged:
                     break
-                except _capi.SolverError:
-                    step *= 0.5
-                    if step < 1.0 / 1024:
-                        raise
-            u = trial
-            r = self.part.restrict(ev.internal)
-            if converged:
-                self.iterations = it + 1
-                return u
-            converged = step == 1.0 and float(torch.linalg.norm(du)) <= self.tolerance * float(torch.linalg.norm(u))
-        raise _capi.SolverError(4, f"the release did not converge in {self.max_iterations} Newton iterations")
+                converged = step == 1.0 and float(torch.linalg.norm(du)) <= self.tolerance * float(torch.linalg.norm(u))
+                if converged and not last:
+                    break
+            else:
+                raise _capi.SolverError(4, f"the release did not converge in {self.max_iterations} Newton "
+                                           f"iterations (increment {k} of {increments})")
+        self.iterations = total
+        return u
 
     def adjoint(self, coords: torch.Tensor, u: torch.Tensor, grad_u: torch.Tensor) -> torch.Tensor:
         """dJ/dX (num_nodes x 3) from dJ/du at the released u: K_ff^T

@@ -460,13 +460,24 @@ int ensure_wave(sbk_system* s) {
   return SBK_OK;
 }
 
+// Whether K1 of the system runs as the phase kernels.
+bool uses_phases(const sbk_system* sys) {
+  return sys->local_mode == SBK_LOCAL_PHASES && sys->wave_mem && sbk::wave_applies(sys->p);
+}
+
+// Whether the element schedule runs after an evaluation: for the single
+// kernel only. The phase kernels take the elements in mesh order (on the
+// 1M-element microbenchmark the schedule's order was 0.5 % slower there:
+// every phase is a short body of code that all warps share anyway).
+bool schedules(const sbk_system* sys) { return sys->schedule && !uses_phases(sys); }
+
 // K1 of a system: the phase kernels where they apply, else the single kernel.
 int system_elements(sbk_system* sys, const double* u_dev, int want_tangent, cudaStream_t st) {
   const int32_t* order = sys->schedule && sys->order_valid ? sys->order : nullptr;
-  if (sys->local_mode == SBK_LOCAL_PHASES && sys->wave_mem && sbk::wave_applies(sys->p))
+  if (uses_phases(sys))
     return sbk::launch_elements_wave(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c,
                                      want_tangent, sys->force, sys->tangent, sys->energy_e, sys->trial, sys->alpha_t,
-                                     sys->yield, sys->iters, sys->code, sys->first_fail, false, order, sys->wave,
+                                     sys->yield, sys->iters, sys->code, sys->first_fail, false, nullptr, sys->wave,
                                      sys->elements_per_block, st);
   return sbk::launch_elements(sys->p, sys->ne, sys->coords, sys->conn, u_dev, sys->committed, sys->alpha_c,
                               want_tangent, sys->force, sys->tangent, sys->energy_e, sys->trial, sys->alpha_t,
@@ -769,7 +780,7 @@ int sbk_system_evaluate(sbk_system* sys, const double* u_dev, double lambda, int
     if (rc) return fail(SBK_ERR_CUDA, std::string("assembly: ") + cudaGetErrorString((cudaError_t)rc));
   }
   if (sys->timing) SBK_CUDA(cudaEventRecord(sys->ev[3], st));
-  if (sys->schedule) {
+  if (schedules(sys)) {
     rc = sbk::launch_schedule(sys->ne, sys->p.nq, sys->iters, sys->yield, sys->sched, sys->order, st);
     if (rc) return fail(SBK_ERR_CUDA, std::string("schedule: ") + cudaGetErrorString((cudaError_t)rc));
     sys->order_valid = true;
@@ -855,7 +866,7 @@ int sbk_system_enqueue(sbk_system* sys, const double* u_dev, int want_tangent, d
   rc = sbk::launch_assemble_forces(sys->maps(), sys->force, sys->energy_e, sys->yield, sys->p.nq, sys->internal,
                                    sys->scratch, sys->scalars, st);
   if (!rc && want_tangent) rc = sbk::launch_assemble_values(sys->maps(), sys->tangent, sys->values, st);
-  if (!rc && sys->schedule && sys->order_valid)
+  if (!rc && schedules(sys) && sys->order_valid)
     rc = sbk::launch_schedule(sys->ne, sys->p.nq, sys->iters, sys->yield, sys->sched, sys->order, st);
   if (!rc) rc = sbk::launch_summary(sys->scalars, sys->first_fail, sys->code, summary_dev, st);
   if (rc) return fail(SBK_ERR_CUDA, std::string("enqueue: ") + cudaGetErrorString((cudaError_t)rc));

@@ -64,3 +64,34 @@ def test_two_tool_contact_matches_the_oracle(pkg, orc, cuda, cone, search):
     assert np.abs(ev.residual.cpu().numpy() - r["residual"]).max() <= 1e-12 * r["gross"]
     assert np.abs(ev.blocks.cpu().numpy() - r["blocks"]).max() <= 1e-12 * np.abs(r["blocks"]).max()
     gpu.close()
+
+
+def test_cone_release_in_increments_is_the_oracles(pkg, orc, cuda):
+    """The frozen release of a 16 x 16 x 4 cone part whose history was
+    loaded by imposed displacements: its start is far from equilibrium, and
+    full Newton steps from it reach another equilibrium of the supported
+    sheet or invert elements, so the release takes the start's imbalance off
+    in 8 increments. The device's u* against the oracle's release with the
+    same increments (scipy solves of the oracle's tangents) within 1e-9; the
+    springback is a fraction of a millimetre."""
+    wl = importlib.import_module("springback-precomp_b200.workload")
+    sysm, prob = wl.make_cone_problem(16, 4, device=cuda)
+    mesh, mat = prob.mesh, prob.material
+    committed_dev, modes = sysm.committed_all(), sysm.internal_all()
+    sysm.close()
+    free = pkg.supports_321(mesh)
+    release = pkg.Release(mesh, mat, committed_dev, modes, free, increments=8)
+    x0 = torch.tensor(mesh.coords, device=cuda)
+    u_star = release.solve(x0, torch.tensor(prob.u0, device=cuda)).cpu().numpy()
+    release.close()
+    m = mat.as_dict()
+    m["yield_stress"] = 1e300  # frozen
+    committed = device_to_oracle(committed_dev, mat.kinematic_terms)
+    u_ref, iterations = orc.release_solve(m, mesh.coords, mesh.connectivity, committed, modes, free, prob.u0,
+                                          increments=8)
+    rel = np.linalg.norm(u_star - u_ref) / np.linalg.norm(u_ref)
+    spring = np.abs(u_ref - prob.u0).max()
+    print(f"cone release: {iterations} Newton iterations, springback {spring * 1e3:.3f} mm, device against "
+          f"oracle {rel:.2e}")
+    assert rel <= 1e-9
+    assert 0.1e-3 < spring < 2.0e-3
