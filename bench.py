@@ -457,8 +457,11 @@ def run_adjoint(args, rank, world):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), out
 
-    for _ in range(args.warmup):
+    for w in range(args.warmup):
+        t0 = time.perf_counter()
         j, grad, u_star = gradient()
+        print(f"adjoint warm-up {w}: {time.perf_counter() - t0:.1f} s, {release.iterations} Newton iterations",
+              file=sys.stderr, flush=True)
     # The backward alone: the adjoint at the released state, dJ/du of the RMS.
     c0 = coords_of(torch.zeros((20, 20), dtype=torch.float64, device=dev))
     dj = torch.zeros_like(u_star)
@@ -928,7 +931,9 @@ def main():
     p.add_argument("--adj-part", default="sheet", choices=["sheet", "cone"],
                    help="the part of the adjoint workload: a flat sheet with the microbenchmark's history, or the "
                         "fine-mesh cone")
-    p.add_argument("--adj-cone-n", type=int, default=112)
+    p.add_argument("--adj-cone-n", type=int, default=64,
+                   help="the adjoint's cone part: adj-cone-n x adj-cone-n x 4 (each release is ~43 factorisations "
+                        "of its free-free block, 63k DOFs at 64)")
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
 
