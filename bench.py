@@ -931,9 +931,11 @@ def main():
     p.add_argument("--adj-part", default="sheet", choices=["sheet", "cone"],
                    help="the part of the adjoint workload: a flat sheet with the microbenchmark's history, or the "
                         "fine-mesh cone")
-    p.add_argument("--adj-cone-n", type=int, default=64,
-                   help="the adjoint's cone part: adj-cone-n x adj-cone-n x 4 (each release is ~43 factorisations "
-                        "of its free-free block, 63k DOFs at 64)")
+    p.add_argument("--adj-cone-n", type=int, default=32,
+                   help="the adjoint's cone part: adj-cone-n x adj-cone-n x 4. Each release is ~43 factorisations "
+                        "of its free-free block, which the residual stress of the imposed history leaves "
+                        "indefinite: the dense device LU takes it up to 20,000 rows (16,329 at 32); above, "
+                        "GMRES and the sparse QR take ~14 s per factorisation at 64")
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
 
