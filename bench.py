@@ -52,11 +52,11 @@ METRIC = "Hex8 tangent+residual+assembly elem/s (FP64)"
 # DRAM bytes (read + write) per element of one evaluation's K1: ncu's
 # dram__bytes_read.sum + dram__bytes_write.sum summed over the phase kernels
 # of one evaluation of the same construction at 80,000 elements (200 x 200 x
-# 2): 17.80 GB (pre 5.18, return 5.76, log map 2.11, post 3.04, control
-# 0.49, condense 0.83, the single kernel's share 0.39); the traffic grows
+# 2): 16.57 GB (pre 4.48, return 5.41, log map 2.09, post 2.94, control
+# 0.48, condense 0.81, the single kernel's share 0.36); the traffic grows
 # with the elements, so an evaluation of ne elements moves about ne times
 # this.
-K1_DRAM_BYTES_PER_ELEMENT = 17.80e9 / 80000
+K1_DRAM_BYTES_PER_ELEMENT = 16.57e9 / 80000
 # The single kernel (--local-iteration single): 0.69 + 5.28 GB in one launch
 # at 80,000 elements.
 K1_SINGLE_DRAM_BYTES_PER_ELEMENT = (0.692594688e9 + 5.275133e9) / 80000
