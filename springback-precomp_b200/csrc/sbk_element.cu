@@ -1308,10 +1308,7 @@ __device__ __forceinline__ void condense(const Ctx<G, Rec>& c, int want_tangent,
   }
   if (want_tangent && sym) {
     // K* = (K* + K*^T) / 2: the unordered pair {(i, j), (j, i)} by the lane
-    // that owns row min(i, j). Eight pairs of a row are loaded before any
-    // of them is stored: a store may alias the next pair's loads as far as
-    // the compiler knows, so pair by pair every pair waited for its own
-    // round trip to L2.
+    // that owns row min(i, j).
     __threadfence_block();
     c.sync();
     if (lane < 8) {
@@ -1319,25 +1316,12 @@ __device__ __forceinline__ void condense(const Ctx<G, Rec>& c, int want_tangent,
       auto at = [&](int i, int j) -> double* { return Ke + (8 * (i / 3) + j / 3) * 9 + 3 * (i % 3) + (j % 3); };
       for (int k = 0; k < 3; ++k) {
         const int i = 3 * lane + k;
-        for (int j0 = i + 1; j0 < 24; j0 += 8) {
-          double x[8], y[8];
-#pragma unroll
-          for (int t = 0; t < 8; ++t) {
-            const int j = j0 + t;
-            if (j < 24) {
-              x[t] = *at(i, j);
-              y[t] = *at(j, i);
-            }
-          }
-#pragma unroll
-          for (int t = 0; t < 8; ++t) {
-            const int j = j0 + t;
-            if (j < 24) {
-              const double v = 0.5 * (x[t] + y[t]);
-              *at(i, j) = v;
-              *at(j, i) = v;
-            }
-          }
+        for (int j = i + 1; j < 24; ++j) {
+          double* x = at(i, j);
+          double* y = at(j, i);
+          const double v = 0.5 * (*x + *y);
+          *x = v;
+          *y = v;
         }
       }
     }
