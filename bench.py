@@ -932,10 +932,9 @@ def main():
                    help="the part of the adjoint workload: a flat sheet with the microbenchmark's history, or the "
                         "fine-mesh cone")
     p.add_argument("--adj-cone-n", type=int, default=32,
-                   help="the adjoint's cone part: adj-cone-n x adj-cone-n x 4. Each release is ~43 factorisations "
-                        "of its free-free block, which the residual stress of the imposed history leaves "
-                        "indefinite: the dense device LU takes it up to 20,000 rows (16,329 at 32); above, "
-                        "GMRES and the sparse QR take ~14 s per factorisation at 64")
+                   help="the adjoint's cone part: adj-cone-n x adj-cone-n x 4. Each release is ~43 Newton "
+                        "iterations, each a factorisation of its free-free block: ~0.24 s at 32 (16,329 DOFs), "
+                        "~14 s at 64 (63k DOFs)")
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
 
