@@ -82,3 +82,33 @@ def test_oracle_height_gradient_matches_central_differences(pkg, orc, problem):
         fd = (j_of(h * d) - j_of(-h * d)) / (2.0 * h)
         adj = float((grad * d).sum())
         assert abs(adj - fd) <= GRADIENT_TOL * abs(fd), (adj, fd, abs(adj - fd) / abs(fd))
+
+
+def test_incremental_release_reaches_equilibrium(pkg, orc):
+    """The oracle's release in increments (the start's imbalance r0 taken
+    off in equal steps) on a 16 x 16 x 4 cone part whose history was loaded
+    by imposed displacements: the end state is an equilibrium of the free
+    rows (f_int(u*) within 1e-8 of r0), every increment's equilibrium was
+    reached, and the sheet sprang back by a fraction of a millimetre."""
+    wl = importlib.import_module("springback-precomp_b200.workload")
+    mesh = wl.cone_sheet(16, 4)
+    mat = pkg.material.hill_chaboche_sheet()
+    cone = wl.cone_part()
+    X = mesh.element_coordinates()
+    committed = np.zeros((mesh.num_elements, 8, orc.NF))
+    alpha = np.zeros((mesh.num_elements, 9))
+    for k in range(1, 8):
+        uk = (wl.formed_positions(mesh, cone, k * 0.35 / 7) - mesh.coords).reshape(-1)
+        r = orc.elements(mat.as_dict(), X, mesh.gather(uk), committed, alpha, want_tangent=False)
+        assert (r["status"] == 0).all()
+        committed, alpha = r["states"], r["alpha"]
+    u0 = (wl.formed_positions(mesh, cone, 0.35) - mesh.coords).reshape(-1)
+    m = mat.as_dict()
+    m["yield_stress"] = 1e300  # frozen
+    free = pkg.supports_321(mesh)
+    r0 = orc.system_evaluate(m, mesh.coords, mesh.connectivity, u0, committed, alpha)["internal"][free]
+    u, iterations = orc.release_solve(m, mesh.coords, mesh.connectivity, committed, alpha, free, u0, increments=8)
+    r = orc.system_evaluate(m, mesh.coords, mesh.connectivity, u, committed, alpha)["internal"][free]
+    assert np.linalg.norm(r) <= 1e-8 * np.linalg.norm(r0)
+    assert iterations >= 8 * 2
+    assert 0.05e-3 < np.abs(u - u0).max() < 2.0e-3
