@@ -519,6 +519,59 @@ def run_adjoint(args, rank, world):
     return 0
 
 
+def run_forming(args, rank, world):
+    """The CPU-runnable forming run on one GPU, start to finish: the 40 x 40
+    x 2 IM sheet (Swift J2, logarithmic strain) clamped in its outer band,
+    one 3 mm sphere on the spiral to a 10 mm, 2 mm deep dome in 0.5 mm
+    step-downs, then the unload in the clamp and the release onto 3-2-1
+    supports (workload.cfg1_deck). The Newton driver around this package's
+    element loop, contact and device factorisations is the test harness's
+    restatement of the reference's forming driver (tests/forming_harness.py:
+    its increment schedule, cuts, contact anticipation and line search). A
+    throughput and robustness run: the reference committed no output for
+    it. Reported: wall time per step, increments, cuts, the formed and
+    released heights."""
+    import torch
+
+    if world > 1 and rank != 0:
+        return 0
+    pkg = importlib.import_module(PKG)
+    wl = importlib.import_module(PKG + ".workload")
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests"))
+    from forming_harness import FormingRun
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    deck = wl.cfg1_deck()
+    run = FormingRun(pkg, deck, dev)
+    top = np.flatnonzero(np.isclose(run.nodes[:, 2], run.nodes[:, 2].max()))
+    steps = []
+    with ClockSampler(0) as clocks:
+        for k, st in enumerate(deck["steps"]):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = run.run_step(k, None)
+            torch.cuda.synchronize()
+            z = run.nodes[top, 2] + res.u.reshape(-1, 3)[top, 2]
+            steps.append({"name": st["deck"]["name"], "seconds": time.perf_counter() - t0,
+                          "increments": res.increments, "cuts": res.cuts, "pole_height_m": float(z.min()),
+                          "max_eq_plastic_strain": float(res.eq_plastic_strain.max()),
+                          "max_tool_force_n": float(max((abs(f) for f in res.tool_fz), default=0.0))})
+            print(json.dumps(steps[-1]), file=sys.stderr, flush=True)
+    total = sum(s["seconds"] for s in steps)
+    line = {"metric": "CPU-runnable forming run: wall time on one GPU", "value": total, "unit": "s", "n_gpus": 1,
+            "steps": 1, "warmup": 0, "ms_per_step": total * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "20x20x1 mm sheet, 40x40x2 IM Hex8, outer 1 mm clamped; J2 + Swift (E 70 GPa, "
+                                   "nu 0.33, K 425 MPa, eps0 0.003, n 0.29) through from_swift; sphere R 3 mm, "
+                                   "penalty 10, mu 0.1, spiral to a 10 mm x 2 mm dome in 0.5 mm step-downs; "
+                                   "unload; 3-2-1 release; logarithmic strain"},
+            "per_step": steps, "tool_path_points": len(deck["tools"][0]["trajectory"]["points"]),
+            "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def cpu_adjoint(pkg, n, part="sheet"):
     """The same release and gradient with the oracle on the host cores (the
     oracle's release Newton with scipy's sparse LU, its adjoint with the
@@ -911,13 +964,14 @@ def main():
     p.add_argument("--cone-n", type=int, default=224)
     p.add_argument("--cone-sample-n", type=int, default=48)
     p.add_argument("--workload", default="microbench",
-                   choices=["microbench", "batched", "partition", "adjoint", "cone"],
+                   choices=["microbench", "batched", "partition", "adjoint", "cone", "forming"],
                    help="batched: the design-sweep batch (64 parts of 20k-150k elements) in one launch against the "
                         "same parts evaluated one at a time; partition: the free-free block of a Dirichlet "
                         "partition gathered from the full tangent, and the factorisation it feeds; adjoint: the "
                         "springback gradient with respect to 400 commanded heights against one release solve and "
                         "central differences; cone: the fine-mesh truncated cone (200k elements) with the two tools "
-                        "of double-sided forming")
+                        "of double-sided forming; forming: the CPU-runnable forming run (a 40x40x2 sheet, a spiral "
+                        "to a dome, unload, release) start to finish")
     p.add_argument("--element", default="incompatible_modes", choices=["incompatible_modes", "standard"],
                    help="standard: the standard Hex8 with mean dilatation on the same sheet and history")
     p.add_argument("--part-nx", type=int, default=200)
@@ -950,6 +1004,8 @@ def main():
         return run_adjoint(args, rank, world)
     if args.workload == "cone":
         return run_cone(args, rank, world)
+    if args.workload == "forming":
+        return run_forming(args, rank, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

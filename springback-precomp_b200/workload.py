@@ -473,3 +473,150 @@ def sweep_parts(count: int = 64, seed: int = 20260, layers: int = 2):
                                    z0=-CONE_THICKNESS)
         out.append((part, mesh))
     return out
+
+
+# ---- the CPU-runnable forming run: a dome by a spiral ------------------------
+
+def revolution_spiral(height: Callable, r_max: float, tool_radius: float, step_down: float,
+                      spacing: float = 1.0e-3, clearance: float = 2.0e-3, samples: int = 4001):
+    """The reference's continuous spiral tool path (spiral_toolpath,
+    python/precomp/toolpath.py:395-470) restated for a target of revolution
+    z = height(r) (the reference extracts its loops with contourpy, which
+    this image lacks; for a surface of revolution every loop is a circle):
+
+    - the drop-cutter centre height c(r) = max over |s - r| <= R of
+      height(|s|) + sqrt(R^2 - (s - r)^2), in the meridian plane (a ball
+      touches a surface of revolution in the plane through the axis and its
+      centre);
+    - the levels R - k step_down above the deepest centre height, then one
+      step_down / 1000 above it (toolpath.py:288-303), the deepest raised
+      until its loop is at least two point spacings long;
+    - revolution k falls linearly with its arc length from level k - 1 to
+      level k (level 0 is level 1's loop at the sheet plane, where the tip
+      touches z = 0), at the radius where c equals the height, starting at
+      angle 0 counter-clockwise; a last revolution at the deepest level
+      closes the path; approach and retract `clearance` above R.
+
+    Returns (points (n, 3), pseudo-times t = s / total (n,), the pseudo-time
+    of the last point on the part)."""
+    R = float(tool_radius)
+    r = np.linspace(0.0, r_max, samples)
+    h = r[1] - r[0]
+    offsets = np.arange(-int(R / h), int(R / h) + 1) * h
+    cap = np.sqrt(np.maximum(R * R - offsets ** 2, 0.0))
+    c = np.empty_like(r)
+    for i in range(0, samples, 512):
+        s = r[i:i + 512, None] + offsets[None, :]
+        c[i:i + 512] = (np.asarray(height(np.abs(s))) + cap[None, :]).max(axis=1)
+    c = np.maximum.accumulate(c)  # a bowl: the centre rises outward
+    cmin, delta = float(c[0]), 1.0e-3 * step_down
+    levels, k = [], 1
+    while R - k * step_down > cmin + delta:
+        levels.append(R - k * step_down)
+        k += 1
+    if not levels or levels[-1] - (cmin + delta) > delta:
+        levels.append(cmin + delta)
+
+    def radius_at(z):
+        return np.interp(z, c, r)
+
+    # A loop shorter than two point spacings cannot be followed; the deepest
+    # levels whose loops are that short give way to the lowest height with
+    # a followable loop, searched in 64 steps up to the deepest followable
+    # level (toolpath.py:306-336, 389-392).
+    def followable(z):
+        return 2.0 * math.pi * float(radius_at(z)) >= 2.0 * spacing
+
+    j = len(levels) - 1
+    while j >= 0 and not followable(levels[j]):
+        j -= 1
+    if j < len(levels) - 1:
+        last = levels[-1]
+        above = levels[j] if j >= 0 else R
+        dz = (above - last) / 64
+        for q in range(64):
+            if followable(last + q * dz):
+                levels = levels[:j + 1] + [last + q * dz]
+                break
+        else:
+            levels = levels[:j + 1]
+
+    heights = [R] + levels
+    radii = [float(radius_at(levels[0]))] + [float(radius_at(z)) for z in levels]
+    pts = []
+    for k in range(1, len(heights)):
+        n = max(3, int(math.ceil(2.0 * math.pi * max(radii[k - 1], radii[k]) / spacing)))
+        lam = np.arange(n) / n
+        z = heights[k - 1] + lam * (heights[k] - heights[k - 1])
+        rad = np.full(n, radii[1]) if k == 1 else radius_at(z)
+        pts.append(np.column_stack([rad * np.cos(2 * np.pi * lam), rad * np.sin(2 * np.pi * lam), z]))
+    n = max(3, int(math.ceil(2.0 * math.pi * radii[-1] / spacing)))
+    lam = np.arange(n + 1) / n
+    pts.append(np.column_stack([radii[-1] * np.cos(2 * np.pi * lam), radii[-1] * np.sin(2 * np.pi * lam),
+                                np.full(n + 1, heights[-1])]))
+    body = np.vstack(pts)
+    safe = R + clearance
+    points = np.vstack([[body[0, 0], body[0, 1], safe], body, [body[-1, 0], body[-1, 1], safe]])
+    step = np.linalg.norm(np.diff(points, axis=0), axis=1)
+    keep = np.concatenate([[True], step > 1e-15])
+    points = points[keep]
+    s = np.concatenate([[0.0], np.cumsum(np.linalg.norm(np.diff(points, axis=0), axis=1))])
+    t = s / s[-1]
+    return points, t, float(t[-2])
+
+
+CFG1 = dict(blank=20.0e-3, thickness=1.0e-3, nx=40, nz=2, clamp=1.0e-3, tool_radius=3.0e-3, friction=0.1,
+            dome_radius=5.0e-3, dome_depth=2.0e-3, dome_fillet=2.0e-3, step_down=0.5e-3, spacing=1.0e-3,
+            max_tool_travel=1.0e-3, swift=(70.0e9, 0.33, 425.0e6, 0.003, 0.29))
+
+
+def cfg1_deck(**overrides) -> dict:
+    """The CPU-runnable forming run as a forming deck (the form the test
+    harness's forming driver reads): a 20 x 20 x 1 mm sheet of 40 x 40 x 2
+    IM Hex8, its top face at z = 0, clamped in its outer 1 mm band; J2 with
+    the Swift law (E 70 GPa, nu 0.33, K 425 MPa, eps0 0.003, n 0.29) through
+    from_swift; logarithmic strain; one sphere of radius 3 mm, penalty 10,
+    Coulomb 0.1, on the spiral (revolution_spiral, 0.5 mm step-downs, 1 mm
+    spacing) to a 10 mm, 2 mm deep dome with a 2 mm rim fillet; then the
+    unload in the clamp and the release onto 3-2-1 supports, as the
+    reference's deck writer builds them (python/precomp/fea/deck.py:107-179:
+    the tool surface inside the clamp, the supports half the clamp margin
+    from the blank's corners). No reference output exists for this run."""
+    from .material import Material
+    from .parts import Dome
+
+    p = dict(CFG1, **overrides)
+    b, th, nx, nz, e = p["blank"], p["thickness"], p["nx"], p["nz"], p["clamp"]
+    mesh = structured_hex_mesh(nx, nx, nz, b, b, th, x0=-0.5 * b, y0=-0.5 * b, z0=-th)
+    E, nu, K, eps0, n = p["swift"]
+    mat = Material.from_swift("swift-j2", E, nu, K, eps0, n)
+    dome = Dome(p["dome_radius"], p["dome_depth"], p["dome_fillet"])
+    points, t, t_form = revolution_spiral(lambda r: dome.height(r, 0 * r), 0.5 * b, p["tool_radius"],
+                                          p["step_down"], p["spacing"])
+    half = 0.5 * b - e
+    clamp = {"name": "clamp", "fix": ["x", "y", "z"], "mode": "hold",
+             "region": {"any_of": [{"box": {"xmax": -half}}, {"box": {"xmin": half}}, {"box": {"ymax": -half}},
+                                   {"box": {"ymin": half}}]}}
+    a = 0.5 * b - 0.5 * e
+    supports = [{"name": "support_xyz", "fix": ["x", "y", "z"], "mode": "hold", "region": {"nearest_node": [-a, -a, 0.0]}},
+                {"name": "support_yz", "fix": ["y", "z"], "mode": "hold", "region": {"nearest_node": [a, -a, 0.0]}},
+                {"name": "support_z", "fix": ["z"], "mode": "hold", "region": {"nearest_node": [-a, a, 0.0]}}]
+    return {
+        "nodes": mesh.coords.tolist(), "elements": mesh.connectivity.tolist(),
+        "material": {"name": mat.name, "youngs_modulus": mat.youngs_modulus, "poisson_ratio": mat.poisson_ratio,
+                     "plasticity": {"yield_stress": mat.yield_stress, "hardening_modulus": mat.hardening_modulus,
+                                    "saturation_stress": mat.saturation_stress,
+                                    "saturation_rate": mat.saturation_rate}},
+        "model": {"element_formulation": "incompatible_modes"}, "kinematics": "finite_logarithmic",
+        "tools": [{"name": "tool", "shape": "sphere", "radius": p["tool_radius"], "friction": p["friction"],
+                   "penalty": 10.0,
+                   "surface": {"box": {"zmin": 0.0, "xmin": -half, "xmax": half, "ymin": -half, "ymax": half}},
+                   "trajectory": {"times": t.tolist(), "points": points.tolist()}}],
+        "steps": [
+            {"deck": {"name": "form", "type": "form", "tools": ["tool"], "time": [0.0, t_form],
+                      "max_tool_travel": p["max_tool_travel"], "boundary_conditions": [clamp]}},
+            {"deck": {"name": "unload", "type": "release", "tools": [], "boundary_conditions": [clamp]}},
+            {"deck": {"name": "release", "type": "release", "tools": [], "boundary_conditions": supports}},
+        ],
+        "dome": dome,
+    }
