@@ -76,3 +76,34 @@ def test_sweep_parts_keep_a_floor():
             capped += 1
         assert p.depth <= 4.0e-3
     assert capped < 32
+
+
+def test_spiral_follows_the_dome_without_gouging():
+    """The spiral tool path of the CPU-runnable forming run (the reference's
+    spiral_toolpath restated for a target of revolution): it starts and
+    ends in the air above the sheet, its height never rises on the part,
+    each revolution drops one step-down until the deepest level, the ball
+    never cuts into the target (its lowest point along the contact normal
+    stays on or above the dome everywhere), and it reaches the dome's
+    depth within a step-down."""
+    wl = importlib.import_module("springback-precomp_b200.workload")
+    parts = importlib.import_module("springback-precomp_b200.parts")
+    dome = parts.Dome(5e-3, 2e-3, 2e-3)
+    R, step = 3e-3, 0.5e-3
+    pts, t, t_form = wl.revolution_spiral(lambda r: dome.height(r, 0 * r), 10e-3, R, step, 1e-3)
+    assert pts[0, 2] > R and pts[-1, 2] > R  # approach and retract in the air
+    assert np.all(np.diff(t) > 0) and t[0] == 0.0 and t[-1] == 1.0 and 0.8 < t_form < 1.0
+    body = pts[1:-1]
+    assert np.all(np.diff(body[:, 2]) <= 1e-15)
+    assert body[0, 2] == R  # the tip at the sheet plane
+    # No gouge: the ball's centre is at least R from every point of the
+    # target's surface of revolution (sampled densely in the meridian plane
+    # through the centre).
+    s = np.linspace(-10e-3, 10e-3, 20001)
+    zs = dome.height(np.abs(s), 0 * s)
+    for p in body[::3]:
+        rho = np.hypot(p[0], p[1])
+        d = np.sqrt((s - rho) ** 2 + (zs - p[2]) ** 2).min()
+        assert d >= R * (1 - 1e-6), (p, d)
+    # The deepest tip within a step-down of the dome's depth.
+    assert -2e-3 <= body[:, 2].min() - R <= -2e-3 + step
