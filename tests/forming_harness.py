@@ -113,9 +113,22 @@ GROWTH = 1.5
 
 
 class FormingRun:
-    def __init__(self, pkg, fixture: dict, device, solver: str = "device"):
+    def __init__(self, pkg, fixture: dict, device, solver: str = "device", growth_test: str = "own"):
+        """growth_test: which Newton iteration count decides the growth of
+        the next increment after a quick one - "own", the iterations to this
+        harness's correction of 1e-13 m (the replays of the reference's runs
+        use it), or "reference", the iterations until a full step's
+        correction is within the reference's displacement tolerance, 1e-6 of
+        the increment (Forming.cpp:914-921, 1112; displacement_tolerance,
+        include/sparlab/fem/Forming.hpp:184): the iterations the reference
+        counts, so that a run on the harness's own schedule grows back
+        after a cut as the reference's does."""
         self.pkg = pkg
         self.solver = solver
+        if growth_test not in ("own", "reference"):
+            raise ValueError("growth_test must be 'own' or 'reference'")
+        self.growth_test = growth_test
+        self.reference_iterations = 0
         self.part = None
         self.contact_symmetric = True
         self.fx = fixture
@@ -281,7 +294,8 @@ class FormingRun:
             self.times.append(t1)
             count += 1
             t = t1
-            if iterations <= QUICK_ITERATIONS:
+            counted = iterations if self.growth_test == "own" else self.reference_iterations
+            if counted <= QUICK_ITERATIONS:
                 dt = min(GROWTH * dt, dt_max)
             cuts_in_a_row = 0
             if s1 >= 1.0:
@@ -324,6 +338,7 @@ class FormingRun:
             return ev, r, float(du @ (r[free] - ramp * r0))
 
         history = []
+        self.reference_iterations = 0
         have = None  # the full step's evaluation with its tangent, when kept
         for it in range(300):
             if have is None:
@@ -384,10 +399,15 @@ class FormingRun:
             trial[free] += alpha * du
             step = alpha * np.abs(du).max()
             history.append((float(np.linalg.norm(rf)), float(step), alpha))
+            if not self.reference_iterations and alpha == 1.0 and \
+                    np.linalg.norm(du) <= 1.0e-6 * np.linalg.norm(trial[free] - self.u[free]):
+                self.reference_iterations = it + 1
             if (alpha == 1.0 and step <= 1e-13) or (it >= 40 and step <= 1e-11):
                 break
         else:
             raise NewtonFailure(f"the increment to t = {t1} did not converge: (|R|, step, alpha) {history[-8:]}")
+        if not self.reference_iterations:
+            self.reference_iterations = it + 1
         # The accepted state's own evaluation makes its trial history the one committed.
         _, _, fz = self._residual(trial, t1, active, False)
         self.system.commit()
