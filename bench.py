@@ -543,6 +543,12 @@ def run_forming(args, rank, world):
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
     deck = wl.cfg1_deck()
+    times = deck["tools"][0]["trajectory"]["times"]
+    if args.forming_stations > 0:
+        # The form step cut short after that many points of the path (then
+        # the unload and the release as usual).
+        deck["steps"][0]["deck"]["time"][1] = min(deck["steps"][0]["deck"]["time"][1],
+                                                  times[min(args.forming_stations, len(times) - 1)])
     # The increments grow back after a cut as the reference's driver lets
     # them: by the iterations to its own tolerance.
     run = FormingRun(pkg, deck, dev, growth_test="reference")
@@ -561,6 +567,7 @@ def run_forming(args, rank, world):
                           "max_tool_force_n": float(max((abs(f) for f in res.tool_fz), default=0.0))})
             print(json.dumps(steps[-1]), file=sys.stderr, flush=True)
     total = sum(s["seconds"] for s in steps)
+    form = steps[0]
     line = {"metric": "CPU-runnable forming run: wall time on one GPU", "value": total, "unit": "s", "n_gpus": 1,
             "steps": 1, "warmup": 0, "ms_per_step": total * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -569,9 +576,32 @@ def run_forming(args, rank, world):
                                    "penalty 10, mu 0.1, spiral to a 10 mm x 2 mm dome in 0.5 mm step-downs; "
                                    "unload; 3-2-1 release; logarithmic strain"},
             "per_step": steps, "tool_path_points": len(deck["tools"][0]["trajectory"]["points"]),
-            "clocks": clocks.summary()}
+            "form_end_time": deck["steps"][0]["deck"]["time"][1],
+            "form_seconds_per_increment": form["seconds"] / max(form["increments"], 1), "clocks": clocks.summary()}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = forming_cpu_baseline(pkg, wl, FormingRun)
     print(json.dumps(line), flush=True)
     return 0
+
+
+def forming_cpu_baseline(pkg, wl, FormingRun, stations=5):
+    """The same deck's first `stations` path points through the same
+    harness on the host cores, the oracle's system and contact in place of
+    the package's and scipy's solves: seconds per converged increment."""
+    from oracle_backend import OracleBackend
+
+    orc = oracle_module()
+    orc.use_variant("fast")
+    deck = wl.cfg1_deck()
+    deck["steps"][0]["deck"]["time"][1] = deck["tools"][0]["trajectory"]["times"][stations]
+    run = FormingRun(OracleBackend(pkg, orc), deck, "cpu", solver="host", growth_test="reference")
+    t0 = time.perf_counter()
+    res = run.run_step(0, None)
+    seconds = time.perf_counter() - t0
+    return {"value": seconds / max(res.increments, 1), "unit": "s per increment", "cores": cpu_count(),
+            "kind": "port", "sample": f"the form step to the path's point {stations} ({res.increments} increments, "
+                                      f"{res.cuts} cuts), the oracle through the harness, scipy's solves",
+            "seconds": seconds}
 
 
 def cpu_adjoint(pkg, n, part="sheet"):
@@ -984,6 +1014,8 @@ def main():
     p.add_argument("--adj-ny", type=int, default=100)
     p.add_argument("--directions", type=int, default=32)
     p.add_argument("--adj-sample", type=int, default=40)
+    p.add_argument("--forming-stations", type=int, default=0,
+                   help="forming: end the form step at this point of the tool path (0: the whole path)")
     p.add_argument("--adj-part", default="sheet", choices=["sheet", "cone"],
                    help="the part of the adjoint workload: a flat sheet with the microbenchmark's history, or the "
                         "fine-mesh cone")
