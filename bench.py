@@ -342,7 +342,8 @@ def run_batched(args, rank, world):
     build_s = time.perf_counter() - t0
     tune = batch.autotune(ub[0])
     bat_ms, yielding = run_increments(batch.system, ub)
-    line = {"metric": "batched design sweep: parts/h of the element loop (FP64)", "value": args.parts / (bat_ms / 1e3) * 3600.0,
+    line = {"metric": "batched design sweep: parts/h of the element loop (FP64)",
+            "value": args.parts / (bat_ms / 1e3) * 3600.0,
             "unit": "parts/h", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": bat_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"{args.parts} parts (Sobol over dome, truncated cone, elliptic cone, pyramid; "
@@ -551,7 +552,7 @@ def run_forming(args, rank, world):
                                                   times[min(args.forming_stations, len(times) - 1)])
     # The increments grow back after a cut as the reference's driver lets
     # them: by the iterations to its own tolerance.
-    run = FormingRun(pkg, deck, dev, growth_test="reference")
+    run = FormingRun(pkg, deck, dev, growth_test="reference", tolerance="reference")
     top = np.flatnonzero(np.isclose(run.nodes[:, 2], run.nodes[:, 2].max()))
     steps = []
     with ClockSampler(0) as clocks:
@@ -594,7 +595,8 @@ def forming_cpu_baseline(pkg, wl, FormingRun, stations=5):
     orc.use_variant("fast")
     deck = wl.cfg1_deck()
     deck["steps"][0]["deck"]["time"][1] = deck["tools"][0]["trajectory"]["times"][stations]
-    run = FormingRun(OracleBackend(pkg, orc), deck, "cpu", solver="host", growth_test="reference")
+    run = FormingRun(OracleBackend(pkg, orc), deck, "cpu", solver="host", growth_test="reference",
+                     tolerance="reference")
     t0 = time.perf_counter()
     res = run.run_step(0, None)
     seconds = time.perf_counter() - t0

@@ -598,7 +598,8 @@ def cfg1_deck(**overrides) -> dict:
              "region": {"any_of": [{"box": {"xmax": -half}}, {"box": {"xmin": half}}, {"box": {"ymax": -half}},
                                    {"box": {"ymin": half}}]}}
     a = 0.5 * b - 0.5 * e
-    supports = [{"name": "support_xyz", "fix": ["x", "y", "z"], "mode": "hold", "region": {"nearest_node": [-a, -a, 0.0]}},
+    supports = [{"name": "support_xyz", "fix": ["x", "y", "z"], "mode": "hold",
+                 "region": {"nearest_node": [-a, -a, 0.0]}},
                 {"name": "support_yz", "fix": ["y", "z"], "mode": "hold", "region": {"nearest_node": [a, -a, 0.0]}},
                 {"name": "support_z", "fix": ["z"], "mode": "hold", "region": {"nearest_node": [-a, a, 0.0]}}]
     return {

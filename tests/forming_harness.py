@@ -113,7 +113,8 @@ GROWTH = 1.5
 
 
 class FormingRun:
-    def __init__(self, pkg, fixture: dict, device, solver: str = "device", growth_test: str = "own"):
+    def __init__(self, pkg, fixture: dict, device, solver: str = "device", growth_test: str = "own",
+                 tolerance: str = "own"):
         """growth_test: which Newton iteration count decides the growth of
         the next increment after a quick one - "own", the iterations to this
         harness's correction of 1e-13 m (the replays of the reference's runs
@@ -122,12 +123,23 @@ class FormingRun:
         the increment (Forming.cpp:914-921, 1112; displacement_tolerance,
         include/sparlab/fem/Forming.hpp:184): the iterations the reference
         counts, so that a run on the harness's own schedule grows back
-        after a cut as the reference's does."""
+        after a cut as the reference's does.
+
+        tolerance: where an increment's Newton iteration stops - "own", a
+        full step's correction of 1e-13 m (1e-11 m after 40 iterations),
+        which the replays of the reference's committed runs need to meet its
+        states to 1e-8 m; or "reference", the first full step whose
+        correction is within the reference's displacement tolerance (1e-6 of
+        the increment), for a run that no reference output is compared with
+        and whose cost should be the reference driver's."""
         self.pkg = pkg
         self.solver = solver
         if growth_test not in ("own", "reference"):
             raise ValueError("growth_test must be 'own' or 'reference'")
         self.growth_test = growth_test
+        if tolerance not in ("own", "reference"):
+            raise ValueError("tolerance must be 'own' or 'reference'")
+        self.tolerance = tolerance
         self.reference_iterations = 0
         self.part = None
         self.contact_symmetric = True
@@ -402,6 +414,8 @@ class FormingRun:
             if not self.reference_iterations and alpha == 1.0 and \
                     np.linalg.norm(du) <= 1.0e-6 * np.linalg.norm(trial[free] - self.u[free]):
                 self.reference_iterations = it + 1
+                if self.tolerance == "reference":
+                    break
             if (alpha == 1.0 and step <= 1e-13) or (it >= 40 and step <= 1e-11):
                 break
         else:

@@ -23,7 +23,8 @@ def test_first_revolution_of_the_spiral(pkg, orc):
     # The form step cut short after the path's fourth point on the part.
     t_end = times[5]
     deck["steps"][0]["deck"]["time"] = [0.0, t_end]
-    run = FormingRun(OracleBackend(pkg, orc), deck, "cpu", solver="host", growth_test="reference")
+    run = FormingRun(OracleBackend(pkg, orc), deck, "cpu", solver="host", growth_test="reference",
+                     tolerance="reference")
     res = run.run_step(0, None)
     assert res.increments >= 4
     assert res.tool_fz[-1] > 0.0  # the sheet pushes the tool up
